@@ -1,0 +1,317 @@
+"""Benchmark of the DF guiding hot path (guided queries/s) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload full|small]
+
+A step is one gdf_infer over one bounce wavefront of synthetic query records
+(default: 1920x1080 = 2,073,600 queries, 16-level 2^19 hash grids, 64x4
+theta/phi MLPs, 64 bins each). `value` times the kernel with inputs resident
+in HBM; `e2e` times the same call with host buffers, including the
+host->device copy of the queries, guided mask and guiding data and the
+device->host read of the guiding data. L2 is flushed (256 MiB write) between
+timed steps, outside the timed events.
+
+With --impl reference the CPU implementation of the same path runs on the
+host cores (the restated reference path) on a bounded sample
+of the workload per step.
+
+Multi-GPU: the path has no exchange step; each rank runs an independent
+replica of the full workload (weak scaling), timed on the device, max over
+ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "guiding-df_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+import numpy as np  # noqa: E402
+
+FLOP_PER_QUERY = {  # 2 * sum(fan_in * fan_out), unpadded encoded widths, theta + phi
+    "full": 2 * ((60 * 64 + 3 * 64 * 64 + 64 * 64) + (72 * 64 + 3 * 64 * 64 + 64 * 64)),
+    "small": 2 * ((44 * 64 + 2 * 64 * 64 + 64 * 32) + (56 * 64 + 2 * 64 * 64 + 64 * 32)),
+}
+N_QUERIES = {"full": 1920 * 1080, "small": 65536}
+METRIC = "guided queries/s"
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return {"hbm_gbs": d["hbm_gbs"], "bf16_tflops": d["bf16_tflops"],
+                "bf16_tflops_sustained": d.get("bf16_tflops_sustained"), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0, "source": "fallback"}
+
+
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi during timing."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sms, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sms.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sms) if sms else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sms)}
+
+
+def make_context(workload: str, seed: int):
+    import pygdf
+    preset = pygdf.PRESET_FULL if workload == "full" else pygdf.PRESET_SMALL
+    cfg = pygdf.default_config(preset)
+    ctx = pygdf.Context(cfg)
+    rng = np.random.default_rng(seed)
+    import oracle as O
+    d = O.df_cfg_from(cfg)
+    params = []
+    for net in (0, 1):
+        p = ctx.get_params(net)
+        n_mlp = O.df_mlp_params(d, net)
+        p[:n_mlp] *= 2.5
+        p[n_mlp:] = rng.uniform(-0.5, 0.5, p.size - n_mlp).astype(np.float32)
+        ctx.set_params(net, p)
+        params.append(p)
+    return ctx, cfg, params
+
+
+def cpu_reference(workload: str, cfg, params, seconds: float, threads: int):
+    """Times the CPU restatement (fp32 forward + reference epilogue) on the host."""
+    import oracle as O
+    from pygdf import workload as W
+    d = O.df_cfg_from(cfg)
+    p16 = [O.round_f16(p) for p in params]
+    chunk = 16384
+    q = W.queries(chunk, 99)
+    wi, guided = W.wi_init(chunk, 99, 1.0, 0.0)
+    u = W.uniforms(chunk, 99)
+    O.infer_fp32(d, p16[0], p16[1], q[:256], wi[:256], guided[:256], u[:256], threads)  # warm
+    done, t0 = 0, time.perf_counter()
+    while True:
+        O.infer_fp32(d, p16[0], p16[1], q, wi, guided, u, threads)
+        done += chunk
+        el = time.perf_counter() - t0
+        if el >= seconds:
+            break
+    return done / el, done, el
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="full", choices=["full", "small"])
+    ap.add_argument("--cpu-seconds", type=float, default=12.0,
+                    help="CPU-baseline sample length; 0 skips it (profiling runs)")
+    ap.add_argument("--skip-e2e", action="store_true", help="profiling runs: kernel timing only")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    n = N_QUERIES[args.workload]
+    workload_name = ("DF guided inference, 1920x1080 wavefront: hash grid 16 levels x 2 features, "
+                     "2^19 entries/level, theta/phi MLP 64x4, 64 bins, linear interpolation"
+                     if args.workload == "full" else
+                     "DF guided inference, 65,536 queries: hash grid 8x2, 2^16, MLP 64x3, 32 bins")
+    threads = os.cpu_count() or 1
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        import pygdf
+        cfg = pygdf.default_config(pygdf.PRESET_FULL if args.workload == "full" else pygdf.PRESET_SMALL)
+        import oracle as O
+        d = O.df_cfg_from(cfg)
+        rng = np.random.default_rng(0)
+        params = []
+        for net in (0, 1):
+            p = rng.uniform(-0.1, 0.1, O.df_n_params(d, net)).astype(np.float32)
+            params.append(p)
+        per_step = max(1.0, args.cpu_seconds / max(1, args.steps + args.warmup))
+        for _ in range(args.warmup):
+            cpu_reference(args.workload, cfg, params, per_step, threads)
+        vals = [cpu_reference(args.workload, cfg, params, per_step, threads) for _ in range(args.steps)]
+        v = statistics.median(x[0] for x in vals)
+        sample = f"{vals[0][1]} queries per step of the {n}-query workload, {threads} threads"
+        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "queries/s", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": n / v * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic", "config": {"workload": workload_name, "queries": n},
+                "cpu_baseline": {"value": v, "unit": "queries/s", "cores": threads, "kind": "port",
+                                 "sample": sample},
+                "e2e": {"value": v, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from pygdf import workload as W
+    ctx, cfg, params = make_context(args.workload, seed=1234 + rank)
+    dev = torch.device("cuda", local_rank)
+    q_h = W.queries(n, 42 + rank)
+    wi_h, guided_h = W.wi_init(n, 42 + rank, guided_frac=0.7, one_sided_frac=0.1)
+    q = torch.from_numpy(q_h).to(dev)
+    wi0 = torch.from_numpy(wi_h).to(dev)
+    guided = torch.from_numpy(guided_h).to(dev)
+    wi = wi0.clone()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def step(offset):
+        ctx.infer(q, wi, guided=guided, seed=7, offset=offset, n=n, stream=stream)
+
+    for i in range(args.warmup):
+        wi.copy_(wi0)
+        step(i)
+    torch.cuda.synchronize()
+    ctx.sync(stream)
+
+    # ---- device-resident timing (kernel only, L2 flushed between steps)
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    times = []
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    for i in range(args.steps):
+        wi.copy_(wi0)
+        flush.zero_()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        step(1000 + i)
+        e.record(stream)
+        e.synchronize()
+        times.append(s.elapsed_time(e))
+    torch.cuda.synchronize()
+    ctx.sync(stream)
+    if dist:
+        dist.barrier()
+
+    # ---- end to end through the C ABI with host buffers
+    q_pin = torch.from_numpy(q_h).pin_memory()
+    wi_pin = torch.from_numpy(wi_h).pin_memory()
+    g_pin = torch.from_numpy(guided_h).pin_memory()
+    out_pin = torch.empty_like(wi_pin).pin_memory()
+    e2e_times = []
+    for i in range(0 if args.skip_e2e else args.warmup + args.steps):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        q.copy_(q_pin, non_blocking=True)
+        wi.copy_(wi_pin, non_blocking=True)
+        guided.copy_(g_pin, non_blocking=True)
+        step(5000 + i)
+        out_pin.copy_(wi, non_blocking=True)
+        e.record(stream)
+        e.synchronize()
+        if i >= args.warmup:
+            e2e_times.append(s.elapsed_time(e))
+    clk = clocks.stop()
+    ctx.sync(stream)
+
+    ms = statistics.mean(times)
+    ms_e2e = statistics.mean(e2e_times) if e2e_times else float("nan")
+    if dist:
+        t = torch.tensor([ms, ms_e2e], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, ms_e2e = float(t[0]), float(t[1])
+    value = n * world / (ms * 1e-3)
+    e2e_value = n * world / (ms_e2e * 1e-3)
+    h2d = q_h.nbytes + wi_h.nbytes + guided_h.nbytes
+    d2h = wi_h.nbytes
+
+    if rank == 0:
+        peaks = load_peaks()
+        flops = FLOP_PER_QUERY[args.workload] * n
+        achieved = flops / (min(times) * 1e-3) / 1e12
+        traffic = None
+        prof = os.path.join(ROOT, "profiles", f"df_fused_{args.workload}.json")
+        if os.path.exists(prof):
+            traffic = json.load(open(prof)).get("dram_bytes_per_launch")
+        if args.cpu_seconds > 0:
+            cpu_v, cpu_n, cpu_s = cpu_reference(args.workload, cfg, params, args.cpu_seconds, threads)
+        else:
+            cpu_v, cpu_n, cpu_s = None, 0, 0.0
+        line = {
+            "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "fp16 (fp32 accumulate)", "data": "synthetic",
+            "config": {"workload": workload_name, "queries": n, "l2": "flushed (256 MiB) between steps",
+                       "parallelism": f"replicas x{world}"},
+            "e2e": {"value": e2e_value, "unit": "queries/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e},
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peaks["bf16_tflops"],
+                         "unit": "TFLOP/s", "frac": achieved / peaks["bf16_tflops"], "traffic": traffic,
+                         "peak_source": peaks["source"], "kernel": "df_fused_kernel",
+                         "flop_per_query": FLOP_PER_QUERY[args.workload]},
+            "cpu_baseline": {"value": cpu_v, "unit": "queries/s", "cores": threads, "kind": "port",
+                             "sample": f"{cpu_n} queries ({cpu_s:.1f} s) of the same workload"},
+            "clocks": clk,
+            "gpu_launches": args.steps,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

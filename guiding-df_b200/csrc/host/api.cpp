@@ -1,0 +1,604 @@
+// api.cpp -- implementation of the gdf C ABI (include/gdf.h).
+//
+// Host-side orchestration of the guiding module: configuration presets and
+// validation, parameter layout and initialisation, checkpoint files, and the
+// launches of the fused kernels. Nothing here computes a query on the CPU;
+// every compute entry point launches a CUDA kernel or fails.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../kernels/df_kernels.h"
+#include "context.h"
+
+using gdf::Context;
+using gdf::Net;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+gdf_status fail(gdf_status s, const std::string& msg) {
+  g_last_error = msg;
+  return s;
+}
+
+gdf_status cuda_fail(cudaError_t e, const char* what) {
+  return fail(GDF_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define GDF_CUDA(call)                                        \
+  do {                                                        \
+    cudaError_t e_ = (call);                                  \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call);       \
+  } while (0)
+
+int32_t pad16(int32_t v) { return (v + 15) / 16 * 16; }
+
+// PCG32 (M. E. O'Neill, "PCG: a family of simple fast space-efficient
+// statistically good algorithms for random number generation", 2014).
+struct Pcg32 {
+  uint64_t state = 0, inc = 1;
+  explicit Pcg32(uint64_t seed, uint64_t seq = 0xda3e39cb94b95bdbULL) {
+    inc = (seq << 1u) | 1u;
+    next();
+    state += seed;
+    next();
+  }
+  uint32_t next() {
+    const uint64_t old = state;
+    state = old * 6364136223846793005ULL + inc;
+    const uint32_t xs = static_cast<uint32_t>(((old >> 18u) ^ old) >> 27u);
+    const uint32_t rot = static_cast<uint32_t>(old >> 59u);
+    return (xs >> rot) | (xs << ((~rot + 1u) & 31));
+  }
+  float uniform() { return static_cast<float>(next() >> 8) * (1.0f / 16777216.0f); }
+};
+
+bool valid_grid(const gdf_grid_config& g) {
+  return g.n_levels > 0 && g.n_levels <= GDF_MAX_GRID_LEVELS &&
+         (g.n_features_per_level == 2 || g.n_features_per_level == 4) &&
+         g.log2_hashmap_size > 0 && g.log2_hashmap_size <= 26 && g.base_resolution > 0 &&
+         g.per_level_scale >= 1.0f && g.type >= 0 && g.type <= 2 && g.interpolation >= 0 &&
+         g.interpolation <= 2;
+}
+
+gdf_status validate(const gdf_config& c) {
+  if (c.abi_version != GDF_ABI_VERSION) return fail(GDF_ERR_INVALID_ARG, "abi_version mismatch");
+  auto bins_ok = [](int b) { return b == 16 || b == 32 || b == 64; };
+  if (!bins_ok(c.n_bins_theta) || !bins_ok(c.n_bins_phi))
+    return fail(GDF_ERR_INVALID_ARG, "n_bins must be 16, 32 or 64");
+  if (c.pdf_interp != GDF_PDF_LINEAR && c.pdf_interp != GDF_PDF_NEAREST)
+    return fail(GDF_ERR_INVALID_ARG, "pdf_interp");
+  if (!valid_grid(c.grid_theta) || !valid_grid(c.grid_phi))
+    return fail(GDF_ERR_INVALID_ARG, "grid config out of range");
+  if (c.grid_theta.n_levels != c.grid_phi.n_levels ||
+      c.grid_theta.n_features_per_level != c.grid_phi.n_features_per_level)
+    return fail(GDF_ERR_UNSUPPORTED, "theta and phi grids must share levels and features");
+  if (c.sh_degree != 4 || c.oneblob_bins != 4 || c.tw_frequencies != 12)
+    return fail(GDF_ERR_UNSUPPORTED, "built encodings: SH degree 4, OneBlob 4 bins, TriangleWave 12");
+  if (c.mlp_theta.n_neurons != 64 || c.mlp_phi.n_neurons != 64)
+    return fail(GDF_ERR_UNSUPPORTED, "only 64-neuron MLPs are built");
+  if (c.mlp_theta.n_hidden_layers < 1 || c.mlp_theta.n_hidden_layers > 8 ||
+      c.mlp_phi.n_hidden_layers < 1 || c.mlp_phi.n_hidden_layers > 8)
+    return fail(GDF_ERR_INVALID_ARG, "n_hidden_layers must be in [1, 8]");
+  if (c.nrc_enable) {
+    if (c.mlp_nrc.n_neurons != 64 || c.mlp_nrc.n_hidden_layers < 1 || c.mlp_nrc.n_hidden_layers > 8)
+      return fail(GDF_ERR_UNSUPPORTED, "NRC MLP must be 64 wide with 1..8 hidden layers");
+    if (c.nrc_frequencies != 12 || c.nrc_oneblob_bins != 4)
+      return fail(GDF_ERR_UNSUPPORTED, "built NRC encoding: Frequency 12, OneBlob 4");
+  }
+  if (c.precision < GDF_PREC_FP16 || c.precision > GDF_PREC_FP8)
+    return fail(GDF_ERR_INVALID_ARG, "precision");
+  if (c.max_queries < 0 || c.max_train_batch < 0)
+    return fail(GDF_ERR_INVALID_ARG, "negative capacity");
+  gdf::DfShape s{c.grid_theta.n_levels, c.grid_theta.n_features_per_level, c.n_bins_theta,
+                 c.n_bins_phi, c.pdf_interp == GDF_PDF_LINEAR};
+  if (!gdf::df_shape_supported(s))
+    return fail(GDF_ERR_UNSUPPORTED, "no fused kernel is built for this (levels, features, bins) shape");
+  return GDF_OK;
+}
+
+template <typename T>
+gdf_status dalloc(T** p, size_t n) {
+  if (n == 0) { *p = nullptr; return GDF_OK; }
+  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), n * sizeof(T));
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    cudaGetLastError();
+    return fail(GDF_ERR_OOM_BUDGET, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
+  }
+  return GDF_OK;
+}
+
+void free_net(Net& n) {
+  cudaFree(n.master); cudaFree(n.w16); cudaFree(n.ema16); cudaFree(n.adam_m);
+  cudaFree(n.adam_v); cudaFree(n.adam_step); cudaFree(n.grad); cudaFree(n.blob_ema);
+  cudaFree(n.blob_w16);
+  n = Net{};
+}
+
+// DF network layout: composite encoding widths (composite.h:187-199) padded
+// to 16 (network_with_input_encoding.h:44), FullyFusedMLP matrices
+// (fully_fused_mlp.cu:630-668).
+gdf_status layout_df_net(const gdf_config& c, int id, Net& n) {
+  const gdf_grid_config& g = id == 0 ? c.grid_theta : c.grid_phi;
+  const gdf_mlp_config& m = id == 0 ? c.mlp_theta : c.mlp_phi;
+  n.present = true;
+  n.levels = g.n_levels;
+  n.features = g.n_features_per_level;
+  int32_t enc = g.n_levels * g.n_features_per_level + c.sh_degree * c.sh_degree + 3 * c.oneblob_bins;
+  if (id == 1) enc += c.tw_frequencies;
+  n.k0 = pad16(enc);
+  n.width = m.n_neurons;
+  n.hidden = m.n_hidden_layers;
+  n.n_out = id == 0 ? c.n_bins_theta : c.n_bins_phi;
+  n.n_out_pad = pad16(n.n_out);
+  if (!gdf::build_grid_levels(g, &n.gl, &n.n_grid)) return fail(GDF_ERR_INVALID_ARG, "grid tables");
+  n.rows.clear(); n.cols.clear();
+  n.rows.push_back(n.width); n.cols.push_back(n.k0);
+  for (int l = 1; l < n.hidden; ++l) { n.rows.push_back(n.width); n.cols.push_back(n.width); }
+  n.rows.push_back(n.n_out_pad); n.cols.push_back(n.width);
+  n.n_mlp = 0;
+  for (size_t i = 0; i < n.rows.size(); ++i) n.n_mlp += static_cast<int64_t>(n.rows[i]) * n.cols[i];
+  n.n_params = n.n_mlp + n.n_grid;
+  n.blob_bytes = static_cast<uint32_t>(n.n_mlp * 2);
+  return GDF_OK;
+}
+
+// NRC: [Frequency(3 dims x 12 x sin/cos) | OneBlob(6 dims x 4) | Identity(6)]
+// padded with ones to 112 (common/configs/nn/base_hashgrid_nrc_df.json).
+gdf_status layout_nrc_net(const gdf_config& c, Net& n) {
+  n.present = true;
+  n.levels = 0; n.features = 0; n.n_grid = 0;
+  n.k0 = pad16(3 * c.nrc_frequencies * 2 + 6 * c.nrc_oneblob_bins + 6);
+  n.width = c.mlp_nrc.n_neurons;
+  n.hidden = c.mlp_nrc.n_hidden_layers;
+  n.n_out = 3;
+  n.n_out_pad = 16;
+  n.rows.clear(); n.cols.clear();
+  n.rows.push_back(n.width); n.cols.push_back(n.k0);
+  for (int l = 1; l < n.hidden; ++l) { n.rows.push_back(n.width); n.cols.push_back(n.width); }
+  n.rows.push_back(n.n_out_pad); n.cols.push_back(n.width);
+  n.n_mlp = 0;
+  for (size_t i = 0; i < n.rows.size(); ++i) n.n_mlp += static_cast<int64_t>(n.rows[i]) * n.cols[i];
+  n.n_params = n.n_mlp;
+  n.blob_bytes = static_cast<uint32_t>(n.n_mlp * 2);
+  return GDF_OK;
+}
+
+gdf_status alloc_net(Net& n) {
+  gdf_status s;
+  const size_t np = static_cast<size_t>(n.n_params);
+  if ((s = dalloc(&n.master, np)) || (s = dalloc(&n.w16, np)) || (s = dalloc(&n.ema16, np)) ||
+      (s = dalloc(&n.adam_m, np)) || (s = dalloc(&n.adam_v, np)) ||
+      (s = dalloc(&n.adam_step, np)) || (s = dalloc(&n.grad, np)) ||
+      (s = dalloc(&n.blob_ema, static_cast<size_t>(n.n_mlp))) ||
+      (s = dalloc(&n.blob_w16, static_cast<size_t>(n.n_mlp))))
+    return s;
+  return GDF_OK;
+}
+
+// Re-packs the tensor-core weight blobs from the fp16 copies.
+gdf_status repack(Net& n, cudaStream_t st) {
+  cudaError_t e = gdf::launch_pack_mlp(n.ema16, n.blob_ema, n.rows.data(), n.cols.data(),
+                                       static_cast<int>(n.rows.size()), st);
+  if (e != cudaSuccess) return cuda_fail(e, "pack ema");
+  e = gdf::launch_pack_mlp(n.w16, n.blob_w16, n.rows.data(), n.cols.data(),
+                           static_cast<int>(n.rows.size()), st);
+  if (e != cudaSuccess) return cuda_fail(e, "pack w16");
+  return GDF_OK;
+}
+
+// Uploads fp32 master weights; fp16 and EMA copies become fp16(master)
+// (Trainer::set_params_full_precision, trainer.h:238-250); optimizer state
+// is left untouched.
+gdf_status upload_params(Net& n, const std::vector<float>& host) {
+  std::vector<__half> h16(host.size());
+  for (size_t i = 0; i < host.size(); ++i) h16[i] = __float2half_rn(host[i]);
+  GDF_CUDA(cudaMemcpy(n.master, host.data(), host.size() * 4, cudaMemcpyHostToDevice));
+  GDF_CUDA(cudaMemcpy(n.w16, h16.data(), h16.size() * 2, cudaMemcpyHostToDevice));
+  GDF_CUDA(cudaMemcpy(n.ema16, h16.data(), h16.size() * 2, cudaMemcpyHostToDevice));
+  gdf_status s = repack(n, nullptr);
+  if (s) return s;
+  GDF_CUDA(cudaDeviceSynchronize());
+  return GDF_OK;
+}
+
+// Xavier-uniform MLP matrices (gpu_matrix.h initialize_xavier_uniform,
+// fully_fused_mlp.cu:885-904) and U(-1e-4, 1e-4) grid tables
+// (grid.h:1364-1369), drawn from PCG32 seeded with `seed`.
+gdf_status init_params(Net& n, uint32_t seed, uint32_t stream_id) {
+  Pcg32 rng(seed, 0x9e3779b97f4a7c15ULL + stream_id);
+  std::vector<float> h(static_cast<size_t>(n.n_params));
+  size_t o = 0;
+  for (size_t l = 0; l < n.rows.size(); ++l) {
+    const float scale = std::sqrt(6.0f / static_cast<float>(n.rows[l] + n.cols[l]));
+    const size_t cnt = static_cast<size_t>(n.rows[l]) * n.cols[l];
+    for (size_t i = 0; i < cnt; ++i) h[o++] = rng.uniform() * 2.0f * scale - scale;
+  }
+  for (; o < h.size(); ++o) h[o] = rng.uniform() * 2e-4f - 1e-4f;
+  GDF_CUDA(cudaMemset(n.adam_m, 0, h.size() * 4));
+  GDF_CUDA(cudaMemset(n.adam_v, 0, h.size() * 4));
+  GDF_CUDA(cudaMemset(n.adam_step, 0, h.size() * 4));
+  GDF_CUDA(cudaMemset(n.grad, 0, h.size() * 4));
+  n.opt_step = 0;
+  return upload_params(n, h);
+}
+
+Net* net_of(Context* c, int32_t id) {
+  if (!c || id < 0 || id > 2 || !c->net[id].present) return nullptr;
+  return &c->net[id];
+}
+
+gdf_status check_ptr(const void* p, const char* name) {
+  if (!p) return fail(GDF_ERR_INVALID_ARG, std::string(name) + " is null");
+  return GDF_OK;
+}
+
+}  // namespace
+
+namespace gdf {
+
+bool build_grid_levels(const gdf_grid_config& c, GridLevels* gl, int64_t* n_params) {
+  std::memset(gl, 0, sizeof(*gl));
+  if (c.n_levels > 24) return false;
+  gl->n_levels = c.n_levels;
+  gl->interp = c.interpolation;
+  const float log2_scale = std::log2(c.per_level_scale);
+  uint32_t offset = 0;
+  for (int i = 0; i < c.n_levels; ++i) {
+    const float scale = std::exp2(static_cast<float>(i) * log2_scale) *
+                        static_cast<float>(c.base_resolution) - 1.0f;
+    const uint32_t res = static_cast<uint32_t>(std::ceil(scale)) + 1u;
+    const uint32_t max_params = 0xffffffffu / 2u;
+    uint32_t params = std::pow(static_cast<float>(res), 3.0f) > static_cast<float>(max_params)
+                          ? max_params
+                          : res * res * res;
+    params = (params + 7u) / 8u * 8u;
+    if (c.type == GDF_GRID_TILED) {
+      const uint32_t b = static_cast<uint32_t>(c.base_resolution);
+      if (b * b * b < params) params = b * b * b;
+    } else if (c.type == GDF_GRID_HASH) {
+      const uint32_t t = 1u << c.log2_hashmap_size;
+      if (t < params) params = t;
+    }
+    uint32_t stride = 1, nd = 0;
+    for (int d = 0; d < 3 && stride <= params; ++d) {
+      ++nd;
+      stride *= res;
+    }
+    gl->scale[i] = scale;
+    gl->offset[i] = offset;
+    gl->hsize[i] = params;
+    gl->res[i] = res;
+    gl->ndims[i] = nd;
+    gl->hashed[i] = (c.type == GDF_GRID_HASH && params < stride) ? 1u : 0u;
+    gl->pow2[i] = (params & (params - 1u)) == 0u ? 1u : 0u;
+    offset += params;
+  }
+  *n_params = static_cast<int64_t>(offset) * c.n_features_per_level;
+  return true;
+}
+
+}  // namespace gdf
+
+struct gdf_ctx {
+  Context c;
+};
+
+extern "C" {
+
+const char* gdf_last_error(void) { return g_last_error.c_str(); }
+
+const char* gdf_status_string(gdf_status s) {
+  switch (s) {
+    case GDF_OK: return "ok";
+    case GDF_ERR_INVALID_ARG: return "invalid argument";
+    case GDF_ERR_OOM_BUDGET: return "out of memory / budget";
+    case GDF_ERR_CUDA: return "cuda error";
+    case GDF_ERR_TIMEOUT: return "device wait timed out";
+    case GDF_ERR_NUMERIC: return "numeric error";
+    case GDF_ERR_UNSUPPORTED: return "unsupported configuration";
+    case GDF_ERR_STATE: return "invalid state";
+  }
+  return "unknown";
+}
+
+gdf_status gdf_default_config(int32_t preset, gdf_config* cfg) {
+  if (!cfg) return fail(GDF_ERR_INVALID_ARG, "cfg is null");
+  gdf_config c;
+  std::memset(&c, 0, sizeof(c));
+  c.abi_version = GDF_ABI_VERSION;
+  c.pdf_interp = GDF_PDF_LINEAR;
+  c.sh_degree = 4;
+  c.oneblob_bins = 4;
+  c.tw_frequencies = 12;
+  // base_product_df.json optimizer: EMA 0.95 over Adam(3e-2, 0.9, 0.99, 1e-15, l2 1e-6).
+  c.adam_df = gdf_adam_config{3e-2f, 0.9f, 0.99f, 1e-15f, 1e-6f, 0.95f};
+  c.loss_scale = 1024.f;
+  // base_hashgrid_nrc_df.json optimizer: EMA 0.99 over Adam(8e-3, 0.9, 0.99, 1e-8, l2 1e-6).
+  c.adam_nrc = gdf_adam_config{8e-3f, 0.9f, 0.99f, 1e-8f, 1e-6f, 0.99f};
+  c.nrc_loss_scale = 1024.f;
+  c.nrc_frequencies = 12;
+  c.nrc_oneblob_bins = 4;
+  c.mlp_nrc = gdf_mlp_config{64, 5};
+  c.precision = GDF_PREC_FP16;
+  c.seed = 7272u;  // KRR_DEFAULT_RND_SEED (src/lib/src/core/config.in.h:15)
+  gdf_grid_config hash{GDF_GRID_HASH, 8, 2, 16, 16, 2.0f, GDF_GRID_LINEAR};
+  switch (preset) {
+    case GDF_PRESET_SMALL:
+      c.n_bins_theta = c.n_bins_phi = 32;
+      c.grid_theta = c.grid_phi = hash;
+      c.mlp_theta = c.mlp_phi = gdf_mlp_config{64, 3};
+      c.nrc_enable = 1;
+      c.max_queries = 65536;
+      c.max_train_batch = 65536;
+      break;
+    case GDF_PRESET_FULL:
+      c.n_bins_theta = c.n_bins_phi = 64;
+      hash.n_levels = 16;
+      hash.log2_hashmap_size = 19;
+      c.grid_theta = c.grid_phi = hash;
+      c.mlp_theta = c.mlp_phi = gdf_mlp_config{64, 4};
+      c.nrc_enable = 1;
+      c.max_queries = 1920 * 1080;
+      c.max_train_batch = 262144;
+      break;
+    case GDF_PRESET_REFERENCE: {
+      // common/configs/nn/base_product_df.json + parameters.h:41,48.
+      c.n_bins_theta = 16;
+      c.n_bins_phi = 32;
+      gdf_grid_config dense{GDF_GRID_DENSE, 8, 4, 19, 8, 1.405f, GDF_GRID_SMOOTHSTEP};
+      c.grid_theta = c.grid_phi = dense;
+      c.mlp_theta = c.mlp_phi = gdf_mlp_config{64, 3};
+      c.nrc_enable = 1;
+      c.max_queries = 1280 * 720;  // MAX_RESOLUTION (parameters.h:51)
+      c.max_train_batch = 65536 * 8;
+      break;
+    }
+    default:
+      return fail(GDF_ERR_INVALID_ARG, "unknown preset");
+  }
+  *cfg = c;
+  return GDF_OK;
+}
+
+gdf_status gdf_create(const gdf_config* cfg, gdf_ctx** out) {
+  if (!cfg || !out) return fail(GDF_ERR_INVALID_ARG, "null argument");
+  *out = nullptr;
+  gdf_status s = validate(*cfg);
+  if (s) return s;
+  gdf_ctx* h = new (std::nothrow) gdf_ctx();
+  if (!h) return fail(GDF_ERR_OOM_BUDGET, "host allocation failed");
+  Context& c = h->c;
+  c.cfg = *cfg;
+  cudaError_t e = cudaGetDevice(&c.device);
+  if (e != cudaSuccess) { delete h; return cuda_fail(e, "cudaGetDevice"); }
+  cudaDeviceGetAttribute(&c.num_sms, cudaDevAttrMultiProcessorCount, c.device);
+  auto cleanup = [&](gdf_status st) {
+    for (Net& n : c.net) free_net(n);
+    cudaFree(c.d_err);
+    delete h;
+    return st;
+  };
+  if ((s = layout_df_net(c.cfg, 0, c.net[0])) || (s = layout_df_net(c.cfg, 1, c.net[1])))
+    return cleanup(s);
+  if (c.cfg.nrc_enable && (s = layout_nrc_net(c.cfg, c.net[2]))) return cleanup(s);
+  for (Net& n : c.net)
+    if (n.present && (s = alloc_net(n))) return cleanup(s);
+  if ((s = dalloc(&c.d_err, 1))) return cleanup(s);
+  e = cudaMemset(c.d_err, 0, 4);
+  if (e != cudaSuccess) return cleanup(cuda_fail(e, "cudaMemset"));
+  for (int i = 0; i < 3; ++i)
+    if (c.net[i].present && (s = init_params(c.net[i], c.cfg.seed, static_cast<uint32_t>(i))))
+      return cleanup(s);
+  *out = h;
+  return GDF_OK;
+}
+
+gdf_status gdf_destroy(gdf_ctx* ctx) {
+  if (!ctx) return GDF_OK;
+  cudaDeviceSynchronize();
+  for (Net& n : ctx->c.net) free_net(n);
+  cudaFree(ctx->c.d_err);
+  delete ctx;
+  return GDF_OK;
+}
+
+gdf_status gdf_reset_training(gdf_ctx* ctx, uint32_t seed) {
+  if (!ctx) return fail(GDF_ERR_INVALID_ARG, "ctx is null");
+  for (int i = 0; i < 3; ++i) {
+    Net& n = ctx->c.net[i];
+    if (!n.present) continue;
+    gdf_status s = init_params(n, seed, static_cast<uint32_t>(i));
+    if (s) return s;
+  }
+  return GDF_OK;
+}
+
+gdf_status gdf_n_params(const gdf_ctx* ctx, int32_t net, int64_t* n_params) {
+  Net* n = net_of(const_cast<Context*>(ctx ? &ctx->c : nullptr), net);
+  if (!n || !n_params) return fail(GDF_ERR_INVALID_ARG, "bad ctx / net id / output pointer");
+  *n_params = n->n_params;
+  return GDF_OK;
+}
+
+gdf_status gdf_set_params(gdf_ctx* ctx, int32_t net, const float* params_host, int64_t n) {
+  Net* nt = net_of(ctx ? &ctx->c : nullptr, net);
+  if (!nt || !params_host) return fail(GDF_ERR_INVALID_ARG, "bad ctx / net id / params");
+  if (n != nt->n_params) return fail(GDF_ERR_INVALID_ARG, "parameter count mismatch");
+  std::vector<float> h(params_host, params_host + n);
+  return upload_params(*nt, h);
+}
+
+gdf_status gdf_get_params(const gdf_ctx* ctx, int32_t net, float* params_host, int64_t n) {
+  Net* nt = net_of(const_cast<Context*>(ctx ? &ctx->c : nullptr), net);
+  if (!nt || !params_host) return fail(GDF_ERR_INVALID_ARG, "bad ctx / net id / params");
+  if (n != nt->n_params) return fail(GDF_ERR_INVALID_ARG, "parameter count mismatch");
+  GDF_CUDA(cudaDeviceSynchronize());
+  GDF_CUDA(cudaMemcpy(params_host, nt->master, static_cast<size_t>(n) * 4, cudaMemcpyDeviceToHost));
+  return GDF_OK;
+}
+
+gdf_status gdf_get_inference_params(const gdf_ctx* ctx, int32_t net, float* params_host, int64_t n) {
+  Net* nt = net_of(const_cast<Context*>(ctx ? &ctx->c : nullptr), net);
+  if (!nt || !params_host) return fail(GDF_ERR_INVALID_ARG, "bad ctx / net id / params");
+  if (n != nt->n_params) return fail(GDF_ERR_INVALID_ARG, "parameter count mismatch");
+  std::vector<__half> h(static_cast<size_t>(n));
+  GDF_CUDA(cudaDeviceSynchronize());
+  GDF_CUDA(cudaMemcpy(h.data(), nt->ema16, h.size() * 2, cudaMemcpyDeviceToHost));
+  for (size_t i = 0; i < h.size(); ++i) params_host[i] = __half2float(h[i]);
+  return GDF_OK;
+}
+
+gdf_status gdf_save_network(const gdf_ctx* ctx, const char* prefix) {
+  if (!ctx || !prefix) return fail(GDF_ERR_INVALID_ARG, "null argument");
+  const char* names[3] = {"AR_network_theta.bin", "AR_network_phi.bin", "NRC_network.bin"};
+  for (int i = 0; i < 3; ++i) {
+    const Net& n = ctx->c.net[i];
+    if (!n.present) continue;
+    std::vector<float> h(static_cast<size_t>(n.n_params));
+    gdf_status s = gdf_get_params(ctx, i, h.data(), n.n_params);
+    if (s) return s;
+    std::ofstream f(std::string(prefix) + names[i], std::ios::binary);
+    if (!f.good()) return fail(GDF_ERR_INVALID_ARG, std::string("cannot open ") + prefix + names[i]);
+    f.write(reinterpret_cast<const char*>(h.data()), static_cast<std::streamsize>(h.size() * 4));
+  }
+  return GDF_OK;
+}
+
+gdf_status gdf_load_network(gdf_ctx* ctx, const char* prefix) {
+  if (!ctx || !prefix) return fail(GDF_ERR_INVALID_ARG, "null argument");
+  const char* names[3] = {"AR_network_theta.bin", "AR_network_phi.bin", "NRC_network.bin"};
+  for (int i = 0; i < 3; ++i) {
+    Net& n = ctx->c.net[i];
+    if (!n.present) continue;
+    std::ifstream f(std::string(prefix) + names[i], std::ios::binary);
+    if (!f.good()) return fail(GDF_ERR_INVALID_ARG, std::string("cannot open ") + prefix + names[i]);
+    std::vector<float> h(static_cast<size_t>(n.n_params));
+    f.read(reinterpret_cast<char*>(h.data()), static_cast<std::streamsize>(h.size() * 4));
+    if (f.gcount() != static_cast<std::streamsize>(h.size() * 4))
+      return fail(GDF_ERR_INVALID_ARG, std::string("short file ") + prefix + names[i]);
+    gdf_status s = upload_params(n, h);
+    if (s) return s;
+  }
+  return GDF_OK;
+}
+
+static gdf::DfKernelParams df_params(Context& c) {
+  gdf::DfKernelParams p;
+  std::memset(&p, 0, sizeof(p));
+  const Net& t = c.net[0];
+  const Net& f = c.net[1];
+  p.grid_theta = t.ema16 + t.n_mlp;
+  p.grid_phi = f.ema16 + f.n_mlp;
+  p.blob_theta = t.blob_ema;
+  p.blob_phi = f.blob_ema;
+  p.blob_theta_bytes = t.blob_bytes;
+  p.blob_phi_bytes = f.blob_bytes;
+  p.hidden_theta = t.hidden;
+  p.hidden_phi = f.hidden;
+  p.gl_theta = t.gl;
+  p.gl_phi = f.gl;
+  p.err = c.d_err;
+  return p;
+}
+
+static gdf::DfShape df_shape(const Context& c) {
+  return gdf::DfShape{c.cfg.grid_theta.n_levels, c.cfg.grid_theta.n_features_per_level,
+                      c.cfg.n_bins_theta, c.cfg.n_bins_phi, c.cfg.pdf_interp == GDF_PDF_LINEAR};
+}
+
+gdf_status gdf_infer(gdf_ctx* ctx, const float* queries, const uint8_t* guided,
+                     const float* uniforms, uint64_t philox_seed, uint64_t philox_offset,
+                     float* wi, int64_t n, void* stream) {
+  if (!ctx) return fail(GDF_ERR_INVALID_ARG, "ctx is null");
+  if (n < 0) return fail(GDF_ERR_INVALID_ARG, "n < 0");
+  if (n == 0) return GDF_OK;
+  gdf_status s;
+  if ((s = check_ptr(queries, "queries")) || (s = check_ptr(wi, "wi"))) return s;
+  if (ctx->c.cfg.max_queries > 0 && n > ctx->c.cfg.max_queries)
+    return fail(GDF_ERR_INVALID_ARG, "n exceeds max_queries");
+  if ((reinterpret_cast<uintptr_t>(wi) & 15u) || (uniforms && (reinterpret_cast<uintptr_t>(uniforms) & 15u)))
+    return fail(GDF_ERR_INVALID_ARG, "wi and uniforms must be 16-byte aligned");
+  gdf::DfKernelParams p = df_params(ctx->c);
+  p.queries = queries;
+  p.guided = guided;
+  p.uniforms = uniforms;
+  p.wi = wi;
+  p.n = n;
+  p.philox_seed = philox_seed;
+  p.philox_offset = philox_offset;
+  cudaError_t e = gdf::launch_df_fused(df_shape(ctx->c), gdf::kModeInfer, p, ctx->c.num_sms,
+                                       static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cuda_fail(e, "df_fused (infer)");
+  return GDF_OK;
+}
+
+gdf_status gdf_eval_pdf(gdf_ctx* ctx, const float* queries, const float* u, float* pdf_out,
+                        int64_t n, void* stream) {
+  if (!ctx) return fail(GDF_ERR_INVALID_ARG, "ctx is null");
+  if (n < 0) return fail(GDF_ERR_INVALID_ARG, "n < 0");
+  if (n == 0) return GDF_OK;
+  gdf_status s;
+  if ((s = check_ptr(queries, "queries")) || (s = check_ptr(u, "u")) || (s = check_ptr(pdf_out, "pdf_out")))
+    return s;
+  if (reinterpret_cast<uintptr_t>(pdf_out) & 7u) return fail(GDF_ERR_INVALID_ARG, "pdf_out must be 8-byte aligned");
+  gdf::DfKernelParams p = df_params(ctx->c);
+  p.queries = queries;
+  p.u_eval = u;
+  p.pdf_out = pdf_out;
+  p.n = n;
+  cudaError_t e = gdf::launch_df_fused(df_shape(ctx->c), gdf::kModeEval, p, ctx->c.num_sms,
+                                       static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cuda_fail(e, "df_fused (eval)");
+  return GDF_OK;
+}
+
+gdf_status gdf_post_inference(gdf_ctx* ctx, const float* lt, const float* lp, const uint8_t* guided,
+                              const float* uniforms, float* wi, int64_t n, void* stream) {
+  if (!ctx) return fail(GDF_ERR_INVALID_ARG, "ctx is null");
+  if (n < 0) return fail(GDF_ERR_INVALID_ARG, "n < 0");
+  if (n == 0) return GDF_OK;
+  gdf_status s;
+  if ((s = check_ptr(lt, "logits_theta")) || (s = check_ptr(lp, "logits_phi")) ||
+      (s = check_ptr(uniforms, "uniforms")) || (s = check_ptr(wi, "wi")))
+    return s;
+  const gdf_config& c = ctx->c.cfg;
+  cudaError_t e = gdf::launch_df_post(c.n_bins_theta, c.n_bins_phi, c.pdf_interp == GDF_PDF_LINEAR,
+                                      lt, lp, guided, uniforms, wi, n, static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cuda_fail(e, "df_post");
+  return GDF_OK;
+}
+
+gdf_status gdf_train_step(gdf_ctx*, const float*, const float*, const float*, int64_t,
+                          gdf_train_stats*, void*) {
+  return fail(GDF_ERR_UNSUPPORTED, "gdf_train_step: not built yet");
+}
+
+gdf_status gdf_nrc_query(gdf_ctx*, const float*, float*, int64_t, void*) {
+  return fail(GDF_ERR_UNSUPPORTED, "gdf_nrc_query: not built yet");
+}
+
+gdf_status gdf_nrc_train_step(gdf_ctx*, const float*, const float*, int64_t, gdf_train_stats*, void*) {
+  return fail(GDF_ERR_UNSUPPORTED, "gdf_nrc_train_step: not built yet");
+}
+
+gdf_status gdf_sync_status(gdf_ctx* ctx, void* stream) {
+  if (!ctx) return fail(GDF_ERR_INVALID_ARG, "ctx is null");
+  GDF_CUDA(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+  uint32_t err = 0;
+  GDF_CUDA(cudaMemcpy(&err, ctx->c.d_err, 4, cudaMemcpyDeviceToHost));
+  if (err) {
+    cudaMemset(ctx->c.d_err, 0, 4);
+    return fail(GDF_ERR_TIMEOUT, "a bounded device wait gave up (code " + std::to_string(err) + ")");
+  }
+  return GDF_OK;
+}
+
+}  // extern "C"

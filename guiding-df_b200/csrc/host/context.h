@@ -1,0 +1,51 @@
+// context.h -- internal state behind the gdf C ABI (not installed).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include "../../../include/gdf.h"
+#include "../device/grid_levels.h"
+
+namespace gdf {
+
+// One network with its encoding, in tcnn parameter order
+// (network_with_input_encoding.h set_params): MLP matrices, then grid.
+struct Net {
+  bool present = false;
+  int32_t k0 = 0, width = 64, hidden = 0, n_out = 0, n_out_pad = 0;
+  int64_t n_mlp = 0, n_grid = 0, n_params = 0;
+  int32_t levels = 0, features = 0;
+  GridLevels gl{};
+  std::vector<int32_t> rows, cols;  // per weight matrix
+
+  // Device state (all n_params long unless noted).
+  float* master = nullptr;   // fp32 master weights (Trainer params_full_precision)
+  __half* w16 = nullptr;     // fp16 copy used by the training forward
+  __half* ema16 = nullptr;   // fp16 EMA copy used by inference
+  float* adam_m = nullptr;
+  float* adam_v = nullptr;
+  uint32_t* adam_step = nullptr;
+  float* grad = nullptr;     // fp32 gradient accumulator
+  __half* blob_ema = nullptr;  // n_mlp, canonical tensor-core layout of ema16
+  __half* blob_w16 = nullptr;  // n_mlp, canonical layout of w16
+  uint32_t blob_bytes = 0;
+  uint32_t opt_step = 0;       // optimizer step counter (Adam m_current_step)
+};
+
+struct Context {
+  gdf_config cfg{};
+  int device = 0;
+  int num_sms = 148;
+  Net net[3];  // theta, phi, nrc
+  uint32_t* d_err = nullptr;  // device error word of bounded waits
+};
+
+// Grid level tables (tcnn encodings/grid.h:967-1012, grid_index :165-188).
+bool build_grid_levels(const gdf_grid_config& c, GridLevels* gl, int64_t* n_params);
+
+}  // namespace gdf

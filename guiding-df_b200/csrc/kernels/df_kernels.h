@@ -1,0 +1,58 @@
+// df_kernels.h -- host-side declarations of the DF / NRC kernel launchers.
+// Parameter structs are plain data shared by host and device code.
+#pragma once
+
+#include <cstdint>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include "../device/grid_levels.h"
+
+namespace gdf {
+
+// Warpgroups (128-row tiles in flight) per CTA of the fused DF kernel.
+constexpr int kDfWarpgroups = 4;
+constexpr int kDfThreads = 128 * kDfWarpgroups;
+
+enum DfMode : int { kModeInfer = 0, kModeEval = 1 };
+
+struct DfKernelParams {
+  const float* queries;      // n x 9
+  const uint8_t* guided;     // n, nullable
+  const float* uniforms;     // n x 4, nullable -> in-kernel Philox
+  float* wi;                 // n x 4 in/out (infer)
+  const float* u_eval;       // n x 2 (eval)
+  float* pdf_out;            // n x 2 (eval)
+  int64_t n;
+  uint64_t philox_seed, philox_offset;
+  const __half* grid_theta;  // grid tables (entries x F halfs), inference copy
+  const __half* grid_phi;
+  const __half* blob_theta;  // MLP weights in the canonical tensor-core layout
+  const __half* blob_phi;
+  uint32_t blob_theta_bytes, blob_phi_bytes;
+  int32_t hidden_theta, hidden_phi;  // tcnn n_hidden_layers
+  uint32_t* err;                     // device error word
+  GridLevels gl_theta, gl_phi;
+};
+
+struct DfShape {
+  int levels, features, bins_theta, bins_phi;
+  bool linear;
+};
+
+// Returns cudaErrorNotSupported when no kernel is built for the shape.
+cudaError_t launch_df_fused(const DfShape& s, int mode, const DfKernelParams& p, int num_sms,
+                            cudaStream_t stream);
+size_t df_fused_smem_bytes(const DfShape& s, uint32_t blob_theta_bytes, uint32_t blob_phi_bytes);
+bool df_shape_supported(const DfShape& s);
+
+// Epilogue-only kernel (gdf_post_inference).
+cudaError_t launch_df_post(int bins_theta, int bins_phi, bool linear, const float* logits_theta,
+                           const float* logits_phi, const uint8_t* guided, const float* uniforms,
+                           float* wi, int64_t n, cudaStream_t stream);
+
+// Packs fp16 row-major [rows x cols] matrices into the canonical layout.
+cudaError_t launch_pack_mlp(const __half* src, __half* dst, const int32_t* rows,
+                            const int32_t* cols, int n_layers, cudaStream_t stream);
+
+}  // namespace gdf

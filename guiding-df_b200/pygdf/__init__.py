@@ -1,0 +1,216 @@
+"""ctypes binding of the gdf C ABI (include/gdf.h) for tests and the bench.
+
+This module only forwards to libgdf_b200.so; it computes nothing itself and
+raises if the library is missing, so a missing build can never fall back to
+another implementation.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.dirname(HERE)
+LIB_PATH = os.path.join(PKG, "lib", "libgdf_b200.so")
+
+GDF_ABI_VERSION = 1
+GDF_OK = 0
+STATUS = {0: "OK", 1: "INVALID_ARG", 2: "OOM_BUDGET", 3: "CUDA", 4: "TIMEOUT", 5: "NUMERIC",
+          6: "UNSUPPORTED", 7: "STATE"}
+PRESET_SMALL, PRESET_FULL, PRESET_REFERENCE = 0, 1, 2
+NET_THETA, NET_PHI, NET_NRC = 0, 1, 2
+PDF_LINEAR, PDF_NEAREST = 0, 1
+
+
+class GridConfig(C.Structure):
+    _fields_ = [("type", C.c_int32), ("n_levels", C.c_int32), ("n_features_per_level", C.c_int32),
+                ("log2_hashmap_size", C.c_int32), ("base_resolution", C.c_int32),
+                ("per_level_scale", C.c_float), ("interpolation", C.c_int32)]
+
+
+class MlpConfig(C.Structure):
+    _fields_ = [("n_neurons", C.c_int32), ("n_hidden_layers", C.c_int32)]
+
+
+class AdamConfig(C.Structure):
+    _fields_ = [("learning_rate", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float),
+                ("epsilon", C.c_float), ("l2_reg", C.c_float), ("ema_decay", C.c_float)]
+
+
+class Config(C.Structure):
+    _fields_ = [("abi_version", C.c_int32), ("n_bins_theta", C.c_int32), ("n_bins_phi", C.c_int32),
+                ("pdf_interp", C.c_int32), ("grid_theta", GridConfig), ("grid_phi", GridConfig),
+                ("sh_degree", C.c_int32), ("oneblob_bins", C.c_int32), ("tw_frequencies", C.c_int32),
+                ("mlp_theta", MlpConfig), ("mlp_phi", MlpConfig), ("adam_df", AdamConfig),
+                ("loss_scale", C.c_float), ("nrc_enable", C.c_int32), ("nrc_frequencies", C.c_int32),
+                ("nrc_oneblob_bins", C.c_int32), ("mlp_nrc", MlpConfig), ("adam_nrc", AdamConfig),
+                ("nrc_loss_scale", C.c_float), ("precision", C.c_int32), ("seed", C.c_uint32),
+                ("max_queries", C.c_int64), ("max_train_batch", C.c_int64)]
+
+
+class TrainStats(C.Structure):
+    _fields_ = [("loss", C.c_double), ("grad_norm", C.c_double), ("n_records", C.c_int64),
+                ("n_dropped", C.c_int64)]
+
+
+class GdfError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"gdf status {STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+_lib = None
+P = C.c_void_p
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"libgdf_b200.so not built at {LIB_PATH}; run guiding-df_b200/build.py")
+        L = C.CDLL(LIB_PATH)
+        sig = {
+            "gdf_default_config": [C.c_int32, C.POINTER(Config)],
+            "gdf_create": [C.POINTER(Config), C.POINTER(C.c_void_p)],
+            "gdf_destroy": [P],
+            "gdf_reset_training": [P, C.c_uint32],
+            "gdf_n_params": [P, C.c_int32, C.POINTER(C.c_int64)],
+            "gdf_set_params": [P, C.c_int32, P, C.c_int64],
+            "gdf_get_params": [P, C.c_int32, P, C.c_int64],
+            "gdf_get_inference_params": [P, C.c_int32, P, C.c_int64],
+            "gdf_save_network": [P, C.c_char_p],
+            "gdf_load_network": [P, C.c_char_p],
+            "gdf_infer": [P, P, P, P, C.c_uint64, C.c_uint64, P, C.c_int64, P],
+            "gdf_eval_pdf": [P, P, P, P, C.c_int64, P],
+            "gdf_post_inference": [P, P, P, P, P, P, C.c_int64, P],
+            "gdf_train_step": [P, P, P, P, C.c_int64, C.POINTER(TrainStats), P],
+            "gdf_nrc_query": [P, P, P, C.c_int64, P],
+            "gdf_nrc_train_step": [P, P, P, C.c_int64, C.POINTER(TrainStats), P],
+            "gdf_sync_status": [P, P],
+        }
+        for name, args in sig.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = C.c_int
+        L.gdf_last_error.restype = C.c_char_p
+        L.gdf_last_error.argtypes = []
+        L.gdf_status_string.restype = C.c_char_p
+        L.gdf_status_string.argtypes = [C.c_int]
+        _lib = L
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != GDF_OK:
+        raise GdfError(status, lib().gdf_last_error().decode())
+
+
+def default_config(preset: int) -> Config:
+    c = Config()
+    check(lib().gdf_default_config(preset, C.byref(c)))
+    return c
+
+
+def _ptr(x):
+    """Device/host pointer of a torch tensor, numpy array or int (None -> NULL)."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        return x.data_ptr()
+    if hasattr(x, "ctypes"):
+        return x.ctypes.data
+    raise TypeError(type(x))
+
+
+def _stream(s):
+    if s is None:
+        return None
+    if isinstance(s, int):
+        return s
+    return s.cuda_stream
+
+
+class Context:
+    """Owns one gdf_ctx (LearnedDistribution + NRC state on the current device)."""
+
+    def __init__(self, cfg: Config):
+        self.cfg = cfg
+        h = C.c_void_p()
+        check(lib().gdf_create(C.byref(cfg), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().gdf_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def n_params(self, net: int) -> int:
+        n = C.c_int64()
+        check(lib().gdf_n_params(self.h, net, C.byref(n)))
+        return n.value
+
+    def set_params(self, net: int, params):
+        import numpy as np
+        a = np.ascontiguousarray(params, dtype=np.float32)
+        check(lib().gdf_set_params(self.h, net, a.ctypes.data, a.size))
+
+    def get_params(self, net: int):
+        import numpy as np
+        a = np.empty(self.n_params(net), dtype=np.float32)
+        check(lib().gdf_get_params(self.h, net, a.ctypes.data, a.size))
+        return a
+
+    def get_inference_params(self, net: int):
+        import numpy as np
+        a = np.empty(self.n_params(net), dtype=np.float32)
+        check(lib().gdf_get_inference_params(self.h, net, a.ctypes.data, a.size))
+        return a
+
+    def save(self, prefix: str):
+        check(lib().gdf_save_network(self.h, prefix.encode()))
+
+    def load(self, prefix: str):
+        check(lib().gdf_load_network(self.h, prefix.encode()))
+
+    def infer(self, queries, wi, guided=None, uniforms=None, seed=0, offset=0, n=None, stream=None):
+        n = queries.shape[0] if n is None else n
+        check(lib().gdf_infer(self.h, _ptr(queries), _ptr(guided), _ptr(uniforms), seed, offset,
+                              _ptr(wi), n, _stream(stream)))
+
+    def eval_pdf(self, queries, u, pdf_out, n=None, stream=None):
+        n = queries.shape[0] if n is None else n
+        check(lib().gdf_eval_pdf(self.h, _ptr(queries), _ptr(u), _ptr(pdf_out), n, _stream(stream)))
+
+    def post_inference(self, logits_theta, logits_phi, uniforms, wi, guided=None, n=None, stream=None):
+        n = logits_theta.shape[0] if n is None else n
+        check(lib().gdf_post_inference(self.h, _ptr(logits_theta), _ptr(logits_phi), _ptr(guided),
+                                       _ptr(uniforms), _ptr(wi), n, _stream(stream)))
+
+    def train_step(self, in_theta, in_phi, target, n=None, stream=None, stats=True):
+        n = in_theta.shape[0] if n is None else n
+        st = TrainStats()
+        check(lib().gdf_train_step(self.h, _ptr(in_theta), _ptr(in_phi), _ptr(target), n,
+                                   C.byref(st) if stats else None, _stream(stream)))
+        return st
+
+    def nrc_query(self, inp, out, n=None, stream=None):
+        n = inp.shape[0] if n is None else n
+        check(lib().gdf_nrc_query(self.h, _ptr(inp), _ptr(out), n, _stream(stream)))
+
+    def nrc_train_step(self, inp, target, n=None, stream=None, stats=True):
+        n = inp.shape[0] if n is None else n
+        st = TrainStats()
+        check(lib().gdf_nrc_train_step(self.h, _ptr(inp), _ptr(target), n,
+                                       C.byref(st) if stats else None, _stream(stream)))
+        return st
+
+    def sync(self, stream=None):
+        check(lib().gdf_sync_status(self.h, _stream(stream)))

@@ -1,0 +1,251 @@
+/*
+ * gdf.h -- C ABI of the B200-native neural path-guiding module (Distribution
+ * Factorization, DF) and its Neural Radiance Cache (NRC).
+ *
+ * The entry points replace the guiding-module interface of guiding-df
+ * (pedrovfigueiredo/guiding-df):
+ *   - LearnedDistribution  src/render/guided/learnedDistribution.h:37-168
+ *   - NRC                  src/render/guided/nrc.h:30-97
+ * Each declaration below cites the reference member it stands in for.
+ *
+ * Conventions
+ *   - Every function returns gdf_status; nothing throws across the ABI.
+ *     gdf_last_error() returns a thread-local message for the last failure.
+ *   - Buffers named *_dev are device pointers owned by the caller; the
+ *     library owns network weights, optimizer state and workspaces.
+ *   - `stream` is a cudaStream_t passed as void* (0 = legacy default stream).
+ *     Work is stream-ordered; no entry point below synchronises the device
+ *     except where the comment says "synchronises".
+ *   - Query layout (one row per query, fp32), identical to the reference's
+ *     inference input buffer (train.cu:334-362, guideditem.h:53-72):
+ *       [0..2] position normalised to [0,1]^3
+ *       [3..5] outgoing direction warped to [0,1]^3, (wo + 1) / 2
+ *       [6]    shading-normal theta / pi, [7] shading-normal phi / (2 pi)
+ *       [8]    1 - exp(-roughness)
+ *   - Guiding-data layout, identical to the reference's inferenceWiBuffer
+ *     (parameters.h:44): [u_theta, u_phi, pdf_theta, pdf_phi] per query.
+ */
+#ifndef GDF_H_
+#define GDF_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GDF_ABI_VERSION 1
+#define GDF_MAX_GRID_LEVELS 24
+
+typedef enum gdf_status {
+  GDF_OK = 0,
+  GDF_ERR_INVALID_ARG = 1,  /* malformed config, bad size or null pointer    */
+  GDF_ERR_OOM_BUDGET = 2,   /* allocation refused by the HBM budget / device */
+  GDF_ERR_CUDA = 3,         /* a CUDA runtime call failed                    */
+  GDF_ERR_TIMEOUT = 4,      /* a bounded device-side wait gave up            */
+  GDF_ERR_NUMERIC = 5,      /* NaN/Inf detected where the contract forbids it */
+  GDF_ERR_UNSUPPORTED = 6,  /* configuration outside what the kernels build  */
+  GDF_ERR_STATE = 7         /* call order violated (e.g. no parameters yet)  */
+} gdf_status;
+
+/* Interpolation of the per-bin PDF (parameters.h:20 AR_LINEAR_INTERPOLATION). */
+typedef enum gdf_pdf_interp { GDF_PDF_LINEAR = 0, GDF_PDF_NEAREST = 1 } gdf_pdf_interp;
+
+/* tiny-cuda-nn GridType / InterpolationType (encodings/grid.h:944-1000). */
+typedef enum gdf_grid_type { GDF_GRID_HASH = 0, GDF_GRID_DENSE = 1, GDF_GRID_TILED = 2 } gdf_grid_type;
+typedef enum gdf_grid_interp {
+  GDF_GRID_LINEAR = 0, GDF_GRID_SMOOTHSTEP = 1, GDF_GRID_NEAREST = 2
+} gdf_grid_interp;
+
+/* Arithmetic type of the MLP layers (tensor-core operands); accumulation is fp32. */
+typedef enum gdf_precision { GDF_PREC_FP16 = 0, GDF_PREC_BF16 = 1, GDF_PREC_FP8 = 2 } gdf_precision;
+
+/* Network ids for parameter access. */
+typedef enum gdf_net { GDF_NET_THETA = 0, GDF_NET_PHI = 1, GDF_NET_NRC = 2 } gdf_net;
+
+typedef struct gdf_grid_config {
+  int32_t type;                 /* gdf_grid_type                         */
+  int32_t n_levels;             /* grid.h:1457 n_levels                  */
+  int32_t n_features_per_level; /* 2 or 4                                */
+  int32_t log2_hashmap_size;    /* hash table entries per level = 2^this */
+  int32_t base_resolution;
+  float per_level_scale;
+  int32_t interpolation;        /* gdf_grid_interp                       */
+} gdf_grid_config;
+
+typedef struct gdf_mlp_config {
+  int32_t n_neurons;       /* only 64 is built                                */
+  int32_t n_hidden_layers; /* tcnn semantics: hidden layers incl. the first  */
+} gdf_mlp_config;
+
+typedef struct gdf_adam_config {
+  float learning_rate, beta1, beta2, epsilon, l2_reg;
+  float ema_decay;  /* EmaOptimizer decay (optimizers/ema.h)           */
+} gdf_adam_config;
+
+typedef struct gdf_config {
+  int32_t abi_version;     /* must be GDF_ABI_VERSION                      */
+  int32_t n_bins_theta;    /* N_DIM_OUTPUT      (parameters.h:41): 16/32/64 */
+  int32_t n_bins_phi;      /* N_DIM_OUTPUT_PHI  (parameters.h:48): 16/32/64 */
+  int32_t pdf_interp;      /* gdf_pdf_interp                               */
+  gdf_grid_config grid_theta, grid_phi; /* the positional grid of each net */
+  int32_t sh_degree;       /* SphericalHarmonics degree (4)                */
+  int32_t oneblob_bins;    /* OneBlob n_bins (4)                           */
+  int32_t tw_frequencies;  /* TriangleWave n_frequencies of the phi net (12) */
+  gdf_mlp_config mlp_theta, mlp_phi;
+  gdf_adam_config adam_df;  /* base_product_df.json optimizer               */
+  float loss_scale;         /* TRAIN_LOSS_SCALE (parameters.h:45) = 1024     */
+  int32_t nrc_enable;
+  int32_t nrc_frequencies;  /* Frequency n_frequencies (12)                 */
+  int32_t nrc_oneblob_bins; /* OneBlob n_bins (4)                           */
+  gdf_mlp_config mlp_nrc;
+  gdf_adam_config adam_nrc; /* base_hashgrid_nrc_df.json optimizer          */
+  float nrc_loss_scale;     /* TRAIN_LOSS_SCALE_NRC (parameters.h:62) = 1024 */
+  int32_t precision;        /* gdf_precision of the inference MLP layers     */
+  uint32_t seed;            /* parameter initialisation seed (7272)          */
+  int64_t max_queries;      /* capacity of one inference call                */
+  int64_t max_train_batch;  /* capacity of one training call                 */
+} gdf_config;
+
+typedef enum gdf_preset {
+  GDF_PRESET_SMALL = 0,     /* 65,536 queries: hash 8x2, 2^16, 64x3, 32 bins    */
+  GDF_PRESET_FULL = 1,      /* 1920x1080 queries: hash 16x2, 2^19, 64x4, 64 bins */
+  GDF_PRESET_REFERENCE = 2  /* common/configs/nn/base_product_df.json exactly   */
+} gdf_preset;
+
+typedef struct gdf_ctx gdf_ctx;
+
+/* Per-call statistics of the last training step. */
+typedef struct gdf_train_stats {
+  double loss;          /* mean divergence loss of the batch (FP64 reduction) */
+  double grad_norm;     /* L2 norm of the unscaled parameter gradient (FP64)  */
+  int64_t n_records;    /* records used                                       */
+  int64_t n_dropped;    /* records rejected as non-finite                     */
+} gdf_train_stats;
+
+/* ------------------------------------------------------------------ setup */
+
+/* Fills *cfg with one of the presets. */
+gdf_status gdf_default_config(int32_t preset, gdf_config* cfg);
+
+/* LearnedDistribution::resetNetwork (learnedDistribution.cpp:64) and
+ * NRC::resetNetwork (nrc.cpp:35): validates the config, allocates weights,
+ * optimizer state and workspaces on the current device, initialises the
+ * weights (Xavier-uniform MLP, U(-1e-4, 1e-4) grid) and zeroes the Adam/EMA
+ * state. Synchronises. */
+gdf_status gdf_create(const gdf_config* cfg, gdf_ctx** out);
+gdf_status gdf_destroy(gdf_ctx* ctx);
+
+/* LearnedDistribution::resetTraining (learnedDistribution.h:44): re-draws the
+ * weights from `seed` and clears optimizer + EMA state. Synchronises. */
+gdf_status gdf_reset_training(gdf_ctx* ctx, uint32_t seed);
+
+/* Number of parameters of one network, in tcnn order: MLP weight matrices
+ * (first, hidden..., output; each row-major [out][in], output rows padded to
+ * a multiple of 16) followed by the grid encoding's tables
+ * (network_with_input_encoding.h set_params order). */
+gdf_status gdf_n_params(const gdf_ctx* ctx, int32_t net, int64_t* n_params);
+
+/* Trainer::set_params_full_precision (trainer.h:238) through
+ * LearnedDistribution::loadNetwork (learnedDistribution.cpp:340): copies fp32
+ * host parameters; the fp16 training copy and the EMA inference copy are both
+ * set to fp16(params). Synchronises. */
+gdf_status gdf_set_params(gdf_ctx* ctx, int32_t net, const float* params_host, int64_t n);
+
+/* Trainer::params_full_precision read-back used by saveNetwork
+ * (learnedDistribution.cpp:295): fp32 master parameters. Synchronises. */
+gdf_status gdf_get_params(const gdf_ctx* ctx, int32_t net, float* params_host, int64_t n);
+
+/* Read-back of the fp16 EMA weights that inference uses (trainer.h:317-332),
+ * widened to fp32. Synchronises. */
+gdf_status gdf_get_inference_params(const gdf_ctx* ctx, int32_t net, float* params_host, int64_t n);
+
+/* saveNetwork / loadNetwork (learnedDistribution.cpp:295-384, nrc.cpp:62-112):
+ * raw fp32 parameter dumps `<prefix>AR_network_theta.bin`,
+ * `<prefix>AR_network_phi.bin` and, with NRC enabled, `<prefix>NRC_network.bin`. */
+gdf_status gdf_save_network(const gdf_ctx* ctx, const char* path_prefix);
+gdf_status gdf_load_network(gdf_ctx* ctx, const char* path_prefix);
+
+/* -------------------------------------------------------------- inference */
+
+/* LearnedDistribution::inferenceStep (learnedDistribution.cpp:167-206) with
+ * thetaPostInference / phiPostInference (train.h:896-929) fused into one
+ * kernel: encode -> theta MLP -> softmax x N -> sample u_theta (guided rows)
+ * -> phi MLP conditioned on u_theta -> softmax x N -> sample u_phi (guided
+ * rows) -> pdf_theta(wi[0]), pdf_phi(wi[1]) multiplied into wi[2], wi[3].
+ *
+ *   queries_dev  [n x 9] fp32, layout above
+ *   guided_dev   [n] uint8, nonzero = guided_pass (guideditem.h:109); NULL = all
+ *   uniforms_dev [n x 4] fp32 in [0,1): theta main, theta fallback, phi main,
+ *                phi fallback (the sampler.get1D() draws of train.h:438,482,494);
+ *                NULL = draw them in-kernel with Philox4x32-10 keyed by
+ *                (philox_seed) at counter (row, philox_offset)
+ *   wi_dev       [n x 4] fp32 in/out: slots 0,1 hold the BSDF-sampled square
+ *                direction of non-guided rows; slots 2,3 hold the caller's
+ *                sign (+1/-1) that the pdfs multiply into.
+ * Inference uses the EMA weights, like tcnn's inference params. */
+gdf_status gdf_infer(gdf_ctx* ctx, const float* queries_dev, const uint8_t* guided_dev,
+                     const float* uniforms_dev, uint64_t philox_seed, uint64_t philox_offset,
+                     float* wi_dev, int64_t n, void* stream);
+
+/* compute_AR_pdf_combined_F (train.h:730-751) for given square directions:
+ * pdf_out_dev[i] = {pdf_theta(u[i].x), pdf_phi(u[i].y)} of the learned
+ * distribution at query i (the phi net is conditioned on u[i].x). */
+gdf_status gdf_eval_pdf(gdf_ctx* ctx, const float* queries_dev, const float* u_dev,
+                        float* pdf_out_dev, int64_t n, void* stream);
+
+/* The DF epilogue alone on given logits, i.e. thetaPostInference +
+ * phiPostInference (train.h:896-929) without the networks: softmax x N,
+ * inversion sampling of guided rows and pdf evaluation into wi. logits are
+ * [n x n_bins] fp32 row-major per net. */
+gdf_status gdf_post_inference(gdf_ctx* ctx, const float* logits_theta_dev,
+                              const float* logits_phi_dev, const uint8_t* guided_dev,
+                              const float* uniforms_dev, float* wi_dev, int64_t n,
+                              void* stream);
+
+/* --------------------------------------------------------------- training */
+
+/* One iteration of LearnedDistribution::trainStep (learnedDistribution.cpp:
+ * 230-289) on a batch of n records: theta/phi forward with fp16 pdfs
+ * (softmaxMultFactor), divergence loss and dL/dlogits
+ * (combine_AR_pdf_and_dl_doutput, train.h:932-965), backward through both
+ * MLPs and grids, Adam + EMA (optimizers/adam.h:48, ema.h:102).
+ *   in_theta_dev [n x 9]  GuidedInput
+ *   in_phi_dev   [n x 10] GuidedInputPhi (slot 9 = theta condition)
+ *   target_dev   [n x 9]  GuidedOutput: dir[2], L[3], wiPdf, bsdfVal[3]
+ * stats_host (nullable) receives the loss; filling it synchronises. */
+gdf_status gdf_train_step(gdf_ctx* ctx, const float* in_theta_dev, const float* in_phi_dev,
+                          const float* target_dev, int64_t n, gdf_train_stats* stats_host,
+                          void* stream);
+
+/* -------------------------------------------------------------------- NRC */
+
+/* NRC::inferenceStep (nrc.cpp:172-181): in [m x 15] fp32 (GuidedInputNRC,
+ * guideditem.h:89-93) -> out [m x 3] fp32 RGB radiance, EMA weights. */
+gdf_status gdf_nrc_query(gdf_ctx* ctx, const float* in_dev, float* out_dev, int64_t m,
+                         void* stream);
+
+/* One iteration of NRC::trainStep (nrc.cpp:132-167) on m records with
+ * RelativeL2Luminance loss (losses/relative_l2_luminance.h:40-86) and
+ * Adam + EMA. target [m x 3] fp32. */
+gdf_status gdf_nrc_train_step(gdf_ctx* ctx, const float* in_dev, const float* target_dev,
+                              int64_t m, gdf_train_stats* stats_host, void* stream);
+
+/* ----------------------------------------------------------------- errors */
+
+/* Synchronises `stream` and reports device-side failures of the kernels
+ * launched on it: GDF_ERR_TIMEOUT when a bounded device wait gave up (the
+ * error word is then cleared), GDF_ERR_CUDA for an asynchronous CUDA error.
+ * The reference has no counterpart (it aborts on CUDA errors,
+ * src/lib/src/core/device/cuda.h:58-60). */
+gdf_status gdf_sync_status(gdf_ctx* ctx, void* stream);
+
+const char* gdf_last_error(void);
+const char* gdf_status_string(gdf_status s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif  /* GDF_H_ */

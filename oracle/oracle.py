@@ -1,0 +1,261 @@
+"""Python driver of the C oracle (oracle/gdf_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline leg as the checker. The product never imports it.
+
+The shared object is built on demand with gcc into oracle/_build/.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+BUILD = os.path.join(HERE, "_build")
+SO = os.path.join(BUILD, "libgdf_oracle.so")
+SRCS = [os.path.join(HERE, "gdf_oracle.c"), os.path.join(HERE, "gdf_oracle_train.c")]
+HDR = os.path.join(HERE, "gdf_oracle.h")
+
+
+def build(force: bool = False) -> str:
+    srcs = [s for s in SRCS if os.path.exists(s)]
+    newest = max(os.path.getmtime(p) for p in srcs + [HDR])
+    if not force and os.path.exists(SO) and os.path.getmtime(SO) >= newest:
+        return SO
+    os.makedirs(BUILD, exist_ok=True)
+    tmp = SO + ".tmp"
+    cmd = ["gcc", "-O2", "-std=c11", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC",
+           "-shared", "-o", tmp, *srcs, "-lm"]
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, SO)
+    return SO
+
+
+class GridCfg(C.Structure):
+    _fields_ = [("type", C.c_int32), ("n_levels", C.c_int32), ("n_features_per_level", C.c_int32),
+                ("log2_hashmap_size", C.c_int32), ("base_resolution", C.c_int32),
+                ("per_level_scale", C.c_float), ("interpolation", C.c_int32)]
+
+
+class DfCfg(C.Structure):
+    _fields_ = [("n_bins_theta", C.c_int32), ("n_bins_phi", C.c_int32), ("pdf_interp", C.c_int32),
+                ("grid_theta", GridCfg), ("grid_phi", GridCfg), ("sh_degree", C.c_int32),
+                ("oneblob_bins", C.c_int32), ("tw_frequencies", C.c_int32), ("width", C.c_int32),
+                ("hidden_theta", C.c_int32), ("hidden_phi", C.c_int32)]
+
+
+class NrcCfg(C.Structure):
+    _fields_ = [("frequencies", C.c_int32), ("oneblob_bins", C.c_int32), ("width", C.c_int32),
+                ("hidden", C.c_int32)]
+
+
+class Grid(C.Structure):
+    _fields_ = [("c", GridCfg), ("scale", C.c_float * 24), ("resolution", C.c_uint32 * 24),
+                ("offset", C.c_uint32 * 25), ("n_params", C.c_int64)]
+
+
+_lib = None
+P = C.c_void_p
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        L = C.CDLL(build())
+        for name, args, res in [
+            ("go_philox_uniforms", [C.c_uint64, C.c_uint64, C.c_int64, P], None),
+            ("go_philox4x32_10", [P, P, P], None),
+            ("go_grid_init", [C.POINTER(Grid), C.POINTER(GridCfg)], C.c_int),
+            ("go_df_n_params", [C.POINTER(DfCfg), C.c_int], C.c_int64),
+            ("go_df_mlp_params", [C.POINTER(DfCfg), C.c_int], C.c_int64),
+            ("go_df_input_width", [C.POINTER(DfCfg), C.c_int], C.c_int32),
+            ("go_nrc_n_params", [C.POINTER(NrcCfg)], C.c_int64),
+            ("go_nrc_input_width", [C.POINTER(NrcCfg)], C.c_int32),
+            ("go_df_encode", [C.POINTER(DfCfg), C.POINTER(Grid), C.c_int, P, P, C.c_float, P], None),
+            ("go_nrc_encode", [C.POINTER(NrcCfg), P, P], None),
+            ("go_sh_encode", [C.c_int, P, P], None),
+            ("go_oneblob_encode", [C.c_int, P, C.c_int, P], None),
+            ("go_post_inference", [C.POINTER(DfCfg), P, P, P, P, P, P, C.c_int64], None),
+            ("go_infer", [C.POINTER(DfCfg), P, P, P, P, P, P, P, C.c_int64, C.c_int], None),
+            ("go_infer_fp32", [C.POINTER(DfCfg), P, P, P, P, P, P, C.c_int64, C.c_int], None),
+            ("go_eval_pdf", [C.POINTER(DfCfg), P, P, P, P, P, C.c_int64, C.c_int], None),
+            ("go_nrc_query", [C.POINTER(NrcCfg), P, P, P, C.c_int64, C.c_int], None),
+            ("go_sample_dir", [P, C.c_int, C.c_int, C.c_float, C.c_float, P, P], C.c_int),
+            ("go_sample_dir_f64", [P, C.c_int, C.c_int, C.c_double, C.c_double], C.c_double),
+            ("go_sample_pdf", [P, C.c_float, C.c_int, C.c_int], C.c_float),
+            ("go_softmax2_times_n", [P, C.c_int], None),
+            ("go_round_f16", [C.c_double], C.c_float),
+            ("go_grid_encode", [C.POINTER(Grid), P, P, P], None),
+        ]:
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = res
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data
+
+
+def f32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def df_cfg_from(cfg) -> DfCfg:
+    """gdf_config (pygdf.Config) -> oracle config."""
+    d = DfCfg()
+    d.n_bins_theta, d.n_bins_phi, d.pdf_interp = cfg.n_bins_theta, cfg.n_bins_phi, cfg.pdf_interp
+    for dst, src in ((d.grid_theta, cfg.grid_theta), (d.grid_phi, cfg.grid_phi)):
+        for f, _ in GridCfg._fields_:
+            setattr(dst, f, getattr(src, f))
+    d.sh_degree, d.oneblob_bins, d.tw_frequencies = cfg.sh_degree, cfg.oneblob_bins, cfg.tw_frequencies
+    d.width = cfg.mlp_theta.n_neurons
+    d.hidden_theta, d.hidden_phi = cfg.mlp_theta.n_hidden_layers, cfg.mlp_phi.n_hidden_layers
+    return d
+
+
+def nrc_cfg_from(cfg) -> NrcCfg:
+    n = NrcCfg()
+    n.frequencies, n.oneblob_bins = cfg.nrc_frequencies, cfg.nrc_oneblob_bins
+    n.width, n.hidden = cfg.mlp_nrc.n_neurons, cfg.mlp_nrc.n_hidden_layers
+    return n
+
+
+def round_f16(a) -> np.ndarray:
+    return np.asarray(a, dtype=np.float32).astype(np.float16).astype(np.float32)
+
+
+def philox_uniforms(seed: int, offset: int, n: int) -> np.ndarray:
+    out = np.empty((n, 4), dtype=np.float32)
+    lib().go_philox_uniforms(seed, offset, n, _p(out))
+    return out
+
+
+def philox_block(ctr, key) -> list[int]:
+    c = np.asarray(ctr, dtype=np.uint32)
+    k = np.asarray(key, dtype=np.uint32)
+    o = np.empty(4, dtype=np.uint32)
+    lib().go_philox4x32_10(_p(c), _p(k), _p(o))
+    return [int(x) for x in o]
+
+
+def df_n_params(d: DfCfg, net: int) -> int:
+    return int(lib().go_df_n_params(C.byref(d), net))
+
+
+def df_mlp_params(d: DfCfg, net: int) -> int:
+    return int(lib().go_df_mlp_params(C.byref(d), net))
+
+
+def infer(d: DfCfg, p_theta, p_phi, queries, wi, guided=None, uniforms=None, n_threads=0,
+          edge_gap=False):
+    """gdf_infer restated; params are fp32 and rounded to fp16 here (EMA copy)."""
+    pt, pp = round_f16(p_theta), round_f16(p_phi)
+    q = f32(queries)
+    w = f32(wi).copy()
+    g = None if guided is None else np.ascontiguousarray(guided, dtype=np.uint8)
+    u = f32(uniforms)
+    n = q.shape[0]
+    gap = np.empty((n, 2), dtype=np.float32) if edge_gap else None
+    lib().go_infer(C.byref(d), _p(pt), _p(pp), _p(q), _p(g), _p(u), _p(w), _p(gap), n, n_threads)
+    return (w, gap) if edge_gap else w
+
+
+def infer_fp32(d: DfCfg, p_theta16, p_phi16, queries, wi, guided, uniforms, n_threads=0):
+    w = f32(wi).copy()
+    n = queries.shape[0]
+    lib().go_infer_fp32(C.byref(d), _p(p_theta16), _p(p_phi16), _p(queries), _p(guided),
+                        _p(uniforms), _p(w), n, n_threads)
+    return w
+
+
+def eval_pdf(d: DfCfg, p_theta, p_phi, queries, u, n_threads=0):
+    pt, pp = round_f16(p_theta), round_f16(p_phi)
+    q, uu = f32(queries), f32(u)
+    out = np.empty((q.shape[0], 2), dtype=np.float32)
+    lib().go_eval_pdf(C.byref(d), _p(pt), _p(pp), _p(q), _p(uu), _p(out), q.shape[0], n_threads)
+    return out
+
+
+def post_inference(d: DfCfg, lt, lp, uniforms, wi, guided=None, edge_gap=False):
+    lt, lp, u = f32(lt), f32(lp), f32(uniforms)
+    w = f32(wi).copy()
+    g = None if guided is None else np.ascontiguousarray(guided, dtype=np.uint8)
+    gap = np.empty((lt.shape[0], 2), dtype=np.float32)
+    lib().go_post_inference(C.byref(d), _p(lt), _p(lp), _p(g), _p(u), _p(w), _p(gap), lt.shape[0])
+    return (w, gap) if edge_gap else w
+
+
+def nrc_query(nc: NrcCfg, params, inp, n_threads=0):
+    p = round_f16(params)
+    x = f32(inp)
+    out = np.empty((x.shape[0], 3), dtype=np.float32)
+    lib().go_nrc_query(C.byref(nc), _p(p), _p(x), _p(out), x.shape[0], n_threads)
+    return out
+
+
+def df_encode(d: DfCfg, net: int, params, q, theta_cond=0.0) -> np.ndarray:
+    g = Grid()
+    lib().go_grid_init(C.byref(g), C.byref(d.grid_theta if net == 0 else d.grid_phi))
+    pr = round_f16(params)
+    k0 = int(lib().go_df_input_width(C.byref(d), net))
+    out = np.empty(k0, dtype=np.float32)
+    qq = f32(q)
+    lib().go_df_encode(C.byref(d), C.byref(g), net, _p(pr), _p(qq), theta_cond, _p(out))
+    return out
+
+
+def grid_tables(gc: GridCfg) -> Grid:
+    g = Grid()
+    lib().go_grid_init(C.byref(g), C.byref(gc))
+    return g
+
+
+def sh_encode(degree: int, dirs01: np.ndarray) -> np.ndarray:
+    out = np.empty((dirs01.shape[0], degree * degree), dtype=np.float64)
+    for i in range(dirs01.shape[0]):
+        v = f32(dirs01[i])
+        lib().go_sh_encode(degree, _p(v), _p(out[i]))
+    return out
+
+
+def oneblob_encode(n_bins: int, x: np.ndarray) -> np.ndarray:
+    x = f32(x)
+    out = np.empty(x.shape[0] * n_bins, dtype=np.float64)
+    lib().go_oneblob_encode(n_bins, _p(x), x.shape[0], _p(out))
+    return out.reshape(x.shape[0], n_bins)
+
+
+def sample_dir(pdf, linear: bool, u: float, u2: float):
+    p = f32(pdf)
+    d = np.zeros(1, dtype=np.float32)
+    gap = np.zeros(1, dtype=np.float32)
+    seg = lib().go_sample_dir(_p(p), p.size, int(linear), u, u2, _p(d), _p(gap))
+    return int(seg), float(d[0]), float(gap[0])
+
+
+def sample_pdf(pdf, u: float, linear: bool) -> float:
+    p = f32(pdf)
+    return float(lib().go_sample_pdf(_p(p), u, p.size, int(linear)))
+
+
+def softmax_times_n(v) -> np.ndarray:
+    a = f32(v).copy()
+    lib().go_softmax2_times_n(_p(a), a.size)
+    return a
+
+
+def round_f16_scalar(x: float) -> float:
+    return float(lib().go_round_f16(float(x)))
+
+
+def grid_encode(g: Grid, table, pos) -> np.ndarray:
+    t = f32(table)
+    p = f32(pos)
+    out = np.empty(g.c.n_levels * g.c.n_features_per_level, dtype=np.float64)
+    lib().go_grid_encode(C.byref(g), _p(t), _p(p), _p(out))
+    return out
