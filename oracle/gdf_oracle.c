@@ -359,6 +359,23 @@ void go_nrc_encode(const go_nrc_config* c, const float* q15, float* out) {
 
 /* kernel_mlp_fused (tcnn/src/fully_fused_mlp.cu:500-556): ReLU hidden layers,
  * linear output, no biases; hidden activations stored as fp16. */
+/* Accumulation model of go_mlp_forward: 0 = FP64 (checker), 1 = sequential
+ * FP32 (an emulation of a tensor-core kernel's accumulation, used only to
+ * calibrate test tolerances). */
+static int g_acc32 = 0;
+void go_set_accumulation(int acc32) { g_acc32 = acc32; }
+
+static double dot_acc(const float* a, const float* b, int k) {
+  if (g_acc32) {
+    float acc = 0.f;
+    for (int i = 0; i < k; ++i) acc += a[i] * b[i];
+    return acc;
+  }
+  double acc = 0.0;
+  for (int i = 0; i < k; ++i) acc += (double)a[i] * (double)b[i];
+  return acc;
+}
+
 void go_mlp_forward(const float* w16, int k0, int width, int n_hidden, int n_out_pad,
                     const float* x16, float* out, float* hidden_out) {
   float h[256], hn[256];
@@ -367,9 +384,7 @@ void go_mlp_forward(const float* w16, int k0, int width, int n_hidden, int n_out
   const float* w = w16;
   for (int l = 0; l < n_hidden; ++l) {
     for (int o = 0; o < width; ++o) {
-      double acc = 0.0;
-      const float* row = w + (size_t)o * k;
-      for (int i = 0; i < k; ++i) acc += (double)row[i] * (double)h[i];
+      const double acc = dot_acc(w + (size_t)o * k, h, k);
       hn[o] = go_round_f16(acc > 0.0 ? acc : 0.0);
     }
     w += (size_t)width * k;
@@ -377,12 +392,7 @@ void go_mlp_forward(const float* w16, int k0, int width, int n_hidden, int n_out
     memcpy(h, hn, sizeof(float) * (size_t)width);
     if (hidden_out) memcpy(hidden_out + (size_t)l * width, h, sizeof(float) * (size_t)width);
   }
-  for (int o = 0; o < n_out_pad; ++o) {
-    double acc = 0.0;
-    const float* row = w + (size_t)o * k;
-    for (int i = 0; i < k; ++i) acc += (double)row[i] * (double)h[i];
-    out[o] = (float)acc;
-  }
+  for (int o = 0; o < n_out_pad; ++o) out[o] = (float)dot_acc(w + (size_t)o * k, h, k);
 }
 
 /* fp32 variant of the same forward for the CPU baseline. */
@@ -709,5 +719,29 @@ void go_nrc_query(const go_nrc_config* c, const float* params16, const float* in
     out3[i * 3 + 0] = o[0];
     out3[i * 3 + 1] = o[1];
     out3[i * 3 + 2] = o[2];
+  }
+}
+
+/* Per-row pdf tables (softmax x N) of both networks, the phi net conditioned
+ * on u_theta[i]; diagnostics for tests. */
+void go_df_pdf_tables(const go_df_config* c, const float* p_theta, const float* p_phi,
+                      const float* queries, const float* u_theta, float* pdf_theta,
+                      float* pdf_phi, int64_t n) {
+  go_grid gt, gp;
+  go_grid_init(&gt, &c->grid_theta);
+  go_grid_init(&gp, &c->grid_phi);
+  const int k0t = go_df_input_width(c, 0), k0p = go_df_input_width(c, 1);
+  const int nbt = c->n_bins_theta, nbp = c->n_bins_phi, lin = c->pdf_interp == 0;
+  for (int64_t i = 0; i < n; ++i) {
+    float x[256], lt[128], lp[128];
+    const float* q = queries + i * 9;
+    go_df_encode(c, &gt, 0, p_theta, q, 0.f, x);
+    go_mlp_forward(p_theta, k0t, c->width, c->hidden_theta, pad16(nbt), x, lt, 0);
+    go_softmax2_times_n(lt, nbt);
+    go_df_encode(c, &gp, 1, p_phi, q, go_theta_condition(u_theta[i], nbt, lin), x);
+    go_mlp_forward(p_phi, k0p, c->width, c->hidden_phi, pad16(nbp), x, lp, 0);
+    go_softmax2_times_n(lp, nbp);
+    memcpy(pdf_theta + i * nbt, lt, sizeof(float) * (size_t)nbt);
+    memcpy(pdf_phi + i * nbp, lp, sizeof(float) * (size_t)nbp);
   }
 }

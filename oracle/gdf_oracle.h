@@ -86,6 +86,8 @@ void go_nrc_encode(const go_nrc_config* c, const float* q15, float* out);
 void go_mlp_forward(const float* w16, int k0, int width, int n_hidden, int n_out_pad,
                     const float* x16, float* out, float* hidden_out /* nullable, n_hidden x width */);
 
+void go_set_accumulation(int acc32);
+
 /* ---- DF epilogue, reference float semantics ---- */
 void go_softmax2_times_n(float* v, int n);
 int go_sample_dir(const float* pdf, int n, int linear, float u_main, float u_fallback,
@@ -115,6 +117,11 @@ void go_infer_fp32(const go_df_config* c, const float* params_theta16,
 /* pdf evaluation at given directions (gdf_eval_pdf semantics). */
 void go_eval_pdf(const go_df_config* c, const float* params_theta16, const float* params_phi16,
                  const float* queries, const float* u, float* pdf_out, int64_t n, int n_threads);
+
+/* Per-row softmax x N tables of both networks (phi conditioned on u_theta). */
+void go_df_pdf_tables(const go_df_config* c, const float* p_theta, const float* p_phi,
+                      const float* queries, const float* u_theta, float* pdf_theta,
+                      float* pdf_phi, int64_t n);
 
 /* NRC query (gdf_nrc_query semantics). */
 void go_nrc_query(const go_nrc_config* c, const float* params16, const float* in15, float* out3,

@@ -88,6 +88,8 @@ def lib():
             ("go_sample_pdf", [P, C.c_float, C.c_int, C.c_int], C.c_float),
             ("go_softmax2_times_n", [P, C.c_int], None),
             ("go_round_f16", [C.c_double], C.c_float),
+            ("go_df_pdf_tables", [C.POINTER(DfCfg), P, P, P, P, P, P, C.c_int64], None),
+            ("go_set_accumulation", [C.c_int], None),
             ("go_grid_encode", [C.POINTER(Grid), P, P, P], None),
         ]:
             f = getattr(L, name)
@@ -259,3 +261,13 @@ def grid_encode(g: Grid, table, pos) -> np.ndarray:
     out = np.empty(g.c.n_levels * g.c.n_features_per_level, dtype=np.float64)
     lib().go_grid_encode(C.byref(g), _p(t), _p(p), _p(out))
     return out
+
+
+def pdf_tables(d: DfCfg, p_theta, p_phi, queries, u_theta):
+    pt, pp = round_f16(p_theta), round_f16(p_phi)
+    q, ut = f32(queries), f32(u_theta)
+    n = q.shape[0]
+    a = np.empty((n, d.n_bins_theta), dtype=np.float32)
+    b = np.empty((n, d.n_bins_phi), dtype=np.float32)
+    lib().go_df_pdf_tables(C.byref(d), _p(pt), _p(pp), _p(q), _p(ut), _p(a), _p(b), n)
+    return a, b

@@ -8,7 +8,8 @@ import pytest
 
 import oracle as O
 import pygdf
-from gdf_testutil import compare_infer, dev, make_ctx, run_infer_pair
+from gdf_testutil import (check_directions, check_pdfs, compare_infer, dev, fp32_emulation_spread,
+                          make_ctx, run_infer_pair)
 
 pytestmark = pytest.mark.gpu
 
@@ -17,31 +18,65 @@ pytestmark = pytest.mark.gpu
                                       (pygdf.PRESET_REFERENCE, 4096)])
 def test_infer_matches_oracle(preset, n):
     ctx, pt, pp = make_ctx(preset, seed=11)
-    got, ref, gap, guided = run_infer_pair(ctx, pt, pp, n, seed=5)
-    stats = compare_infer(ctx.cfg, got, ref, gap, guided)
-    assert stats["edge_skipped"] < n * 0.01
+    got, ref, gap, guided, ref_pdf, _, exact = run_infer_pair(ctx, pt, pp, n, seed=5)
+    stats = compare_infer(ctx, got, ref, gap, guided, ref_pdf, exact)
+    # rows whose uniform ties a CDF edge within EDGE_TOL_E2E are excluded
+    assert stats["edge_skipped"] < n * 0.05
+    ctx.close()
+
+
+@pytest.mark.parametrize("preset", [pygdf.PRESET_FULL, pygdf.PRESET_REFERENCE])
+def test_infer_peaky_weights_no_worse_than_fp32_accumulation(preset):
+    """Large weights make fp16 activation-rounding flips visible. The kernel's
+    deviation from the FP64 oracle must stay within a small multiple of that
+    of an FP32-accumulating forward (the oracle with sequential fp32 sums;
+    the tensor cores sum in a different order), for directions (max and 99th
+    percentile) and pdfs."""
+    import oracle as O
+    ctx, pt, pp = make_ctx(preset, seed=21, gain=2.5, amp=0.5)
+    got, ref, gap, guided, ref_pdf, q, exact = run_infer_pair(ctx, pt, pp, 3000, seed=6)
+    d = O.df_cfg_from(ctx.cfg)
+    from pygdf import workload as W
+    wi, _ = W.wi_init(3000, 6, 0.8, 0.2)
+    u = W.uniforms(3000, 6)
+    L = O.lib()
+    L.go_set_accumulation(1)
+    try:
+        ref32 = O.infer(d, pt, pp, q, wi, guided, u)
+    finally:
+        L.go_set_accumulation(0)
+    ref64 = O.infer(d, pt, pp, q, wi, guided, u)
+    g = guided.astype(bool)
+    dg = np.abs(got[g, 0] - ref64[g, 0])
+    de = np.abs(ref32[g, 0] - ref64[g, 0])
+    assert dg.max() <= 2 * de.max() + 1e-4, (dg.max(), de.max())
+    assert np.percentile(dg, 99) <= 3 * np.percentile(de, 99) + 2e-5
+    spread = fp32_emulation_spread(d, pt, pp, q, got[:, :2])
+    rel = np.abs(got[:, 2:4] - ref_pdf) / (np.abs(ref_pdf) + 1e-6)
+    assert rel.max() <= 2 * spread.max() + 1e-4, (rel.max(), spread.max())
     ctx.close()
 
 
 def test_infer_nearest_interpolation():
     ctx, pt, pp = make_ctx(pygdf.PRESET_SMALL, seed=3, pdf_interp=pygdf.PDF_NEAREST)
-    got, ref, gap, guided = run_infer_pair(ctx, pt, pp, 4096, seed=9)
-    compare_infer(ctx.cfg, got, ref, gap, guided)
+    got, ref, gap, guided, ref_pdf, _, exact = run_infer_pair(ctx, pt, pp, 4096, seed=9)
+    compare_infer(ctx, got, ref, gap, guided, ref_pdf, exact)
     ctx.close()
 
 
 @pytest.mark.parametrize("n", [1, 7, 127, 128, 129, 513, 1000])
 def test_infer_ragged_sizes(n):
     ctx, pt, pp = make_ctx(pygdf.PRESET_SMALL, seed=4)
-    got, ref, gap, guided = run_infer_pair(ctx, pt, pp, n, seed=n)
-    compare_infer(ctx.cfg, got, ref, gap, guided)
+    got, ref, gap, guided, ref_pdf, _, exact = run_infer_pair(ctx, pt, pp, n, seed=n)
+    compare_infer(ctx, got, ref, gap, guided, ref_pdf, exact)
     ctx.close()
 
 
 def test_infer_in_kernel_philox_matches_oracle_philox():
     ctx, pt, pp = make_ctx(pygdf.PRESET_SMALL, seed=6)
-    got, ref, gap, guided = run_infer_pair(ctx, pt, pp, 3000, seed=2, philox=(0xC0FFEE1234, 77))
-    compare_infer(ctx.cfg, got, ref, gap, guided)
+    got, ref, gap, guided, ref_pdf, _, exact = run_infer_pair(ctx, pt, pp, 3000, seed=2,
+                                                       philox=(0xC0FFEE1234, 77))
+    compare_infer(ctx, got, ref, gap, guided, ref_pdf, exact)
     ctx.close()
 
 
@@ -96,10 +131,15 @@ def test_post_inference_matches_oracle(preset):
     ctx.post_inference(dev(lt), dev(lp), dev(u), wi_dev, guided=dev(guided))
     ctx.sync()
     got = wi_dev.cpu().numpy()
-    ref, gap = O.post_inference(O.df_cfg_from(cfg), lt, lp, u, wi, guided, edge_gap=True)
-    compare_infer(cfg, got, ref, gap, guided)
-    # same logits: the only differences are libm ulps of expf/logf
-    assert np.abs(got[:, 2:] - ref[:, 2:]).max() / np.abs(ref[:, 2:]).max() < 1e-5
+    d = O.df_cfg_from(cfg)
+    ref, gap = O.post_inference(d, lt, lp, u, wi, guided, edge_gap=True)
+    check_directions(cfg, got, ref, gap, guided, edge_tol=1e-6)
+    # same logits: the oracle's pdfs at the kernel's directions differ only by
+    # the libm ulps of expf/logf
+    at = wi.copy()
+    at[:, :2] = got[:, :2]
+    ref_at = O.post_inference(d, lt, lp, u, at, np.zeros(n, np.uint8))
+    check_pdfs(got[:, 2:], ref_at[:, 2:], rtol=2e-5)
     ctx.close()
 
 
