@@ -1,0 +1,455 @@
+// df_tile.cuh -- building blocks of the tile-based DF kernels: one warpgroup
+// owns a 128-row tile, thread t of the warpgroup owns row t.
+//
+//   * operand tiles live in shared memory in the no-swizzle K-major
+//     canonical layout (8x8 core matrices, 128 B each);
+//   * layer accumulators live in tensor memory (lane = row);
+//   * the softmax / CDF / sampling epilogue streams a row's logits out of
+//     tensor memory in 32-column chunks instead of holding them in registers.
+//
+// Files including this header are compiled with -fmad=false (see df_math.cuh).
+#pragma once
+
+#include <cstdint>
+#include <cuda_fp16.h>
+
+#include "df_math.cuh"
+#include "sm100.cuh"
+
+namespace gdf {
+namespace tile {
+
+using namespace sm100;
+
+// Byte offset of the 16-byte chunk `kc` (8 fp16 columns) of row `row` in a
+// canonical tile of K columns.
+__device__ __forceinline__ uint32_t chunk_off(uint32_t row, uint32_t kc, uint32_t K) {
+  return (((row >> 3) * (K >> 3) + kc) << 7) + ((row & 7u) << 4);
+}
+
+// Byte offset of column `col` of row `row`.
+__device__ __forceinline__ uint32_t elem_off(uint32_t row, uint32_t col, uint32_t K) {
+  return chunk_off(row, col >> 3, K) + ((col & 7u) << 1);
+}
+
+__device__ __forceinline__ void store_h2(uint8_t* t, uint32_t row, uint32_t col, uint32_t K, float a,
+                                         float b) {
+  *reinterpret_cast<__half2*>(t + elem_off(row, col, K)) = __floats2half2_rn(a, b);
+}
+
+// Stores n (even) consecutive values starting at column col (even).
+__device__ __forceinline__ void store_run(uint8_t* t, uint32_t row, uint32_t col, uint32_t K,
+                                          const float* v, int n) {
+  for (int i = 0; i < n; i += 2) store_h2(t, row, col + i, K, v[i], v[i + 1]);
+}
+
+// ------------------------------------------------------------------ grid
+// One level of kernel_grid (tcnn encodings/grid.h:220-349) for F = 2 or 4,
+// fp32 accumulation. interp: 0 linear, 1 smoothstep, 2 nearest.
+// The level tables are read from the kernel's __grid_constant__ parameters
+// with a warp-uniform dynamic level index (indexed constant-bank loads).
+template <int F>
+__device__ __forceinline__ void grid_level(const GridLevels& s, int l, int interp,
+                                           const __half* __restrict__ table, float px, float py,
+                                           float pz, float* out) {
+  const float scale = s.scale[l];
+  const float pin[3] = {px, py, pz};
+  float fr[3];
+  uint32_t pg[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    float p = fmaf(pin[d], scale, 0.5f);
+    const float t = floorf(p);
+    pg[d] = static_cast<uint32_t>(static_cast<int>(t));
+    p -= t;
+    if (interp == 1) p = p * p * (3.0f - 2.0f * p);
+    fr[d] = p;
+  }
+  const uint32_t hsize = s.hsize[l], r = s.res[l];
+  const uint32_t mode = s.hashed[l] ? 0u : s.ndims[l];
+  const uint32_t hmask = s.pow2[l] ? hsize - 1u : 0u;
+  // Per-axis index terms for the lower (0) and upper (1) corner.
+  uint32_t tx[2], ty[2], tz[2];
+  if (mode == 0) {
+    tx[0] = pg[0]; tx[1] = pg[0] + 1u;
+    ty[0] = pg[1] * 2654435761u; ty[1] = ty[0] + 2654435761u;
+    tz[0] = pg[2] * 805459861u; tz[1] = tz[0] + 805459861u;
+  } else {
+    tx[0] = pg[0]; tx[1] = pg[0] + 1u;
+    ty[0] = mode > 1 ? pg[1] * r : 0u; ty[1] = mode > 1 ? ty[0] + r : 0u;
+    tz[0] = mode > 2 ? pg[2] * r * r : 0u; tz[1] = mode > 2 ? tz[0] + r * r : 0u;
+  }
+  const __half* tab = table + static_cast<size_t>(s.offset[l]) * F;
+  auto entry = [&](int c) -> uint32_t {
+    const uint32_t x = tx[c & 1], y = ty[(c >> 1) & 1], z = tz[(c >> 2) & 1];
+    const uint32_t idx = mode == 0 ? (x ^ y ^ z) : (x + y + z);
+    return hmask ? (idx & hmask) : (idx % hsize);
+  };
+  float acc[F];
+#pragma unroll
+  for (int f = 0; f < F; ++f) acc[f] = 0.f;
+  if (interp == 2) {
+    const uint32_t e = entry(0);
+#pragma unroll
+    for (int f = 0; f < F; ++f) acc[f] = __half2float(tab[static_cast<size_t>(e) * F + f]);
+  } else {
+    const float wx[2] = {1.f - fr[0], fr[0]}, wy[2] = {1.f - fr[1], fr[1]}, wz[2] = {1.f - fr[2], fr[2]};
+    uint32_t e[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) e[c] = entry(c);
+    if constexpr (F == 2) {
+      uint32_t raw[8];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) raw[c] = __ldg(reinterpret_cast<const unsigned int*>(tab) + e[c]);
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        // weight = (x-term * y-term) * z-term, as kernel_grid's dim loop
+        const float w = (1.f * wx[c & 1]) * wy[(c >> 1) & 1] * wz[(c >> 2) & 1];
+        const float2 v = __half22float2(*reinterpret_cast<const __half2*>(&raw[c]));
+        acc[0] += w * v.x;
+        acc[1] += w * v.y;
+      }
+    } else {
+      uint2 raw[8];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) raw[c] = __ldg(reinterpret_cast<const uint2*>(tab) + e[c]);
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        const float w = (1.f * wx[c & 1]) * wy[(c >> 1) & 1] * wz[(c >> 2) & 1];
+        const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&raw[c].x));
+        const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&raw[c].y));
+        acc[0] += w * a.x;
+        acc[1] += w * a.y;
+        acc[2] += w * b.x;
+        acc[3] += w * b.y;
+      }
+    }
+  }
+#pragma unroll
+  for (int f = 0; f < F; ++f) out[f] = acc[f];
+}
+
+// All levels of one grid, written as fp16 into columns [0, L*F) of a tile
+// with K columns.
+template <int F>
+__device__ __forceinline__ void grid_to_tile(const GridLevels& s, int n_levels, int interp,
+                                             const __half* __restrict__ table, const float* q,
+                                             uint8_t* tile, uint32_t row, uint32_t K) {
+#pragma unroll 2
+  for (int l = 0; l < n_levels; ++l) {
+    float f[F];
+    grid_level<F>(s, l, interp, table, q[0], q[1], q[2], f);
+#pragma unroll
+    for (int j = 0; j < F; j += 2) store_h2(tile, row, l * F + j, K, f[j], f[j + 1]);
+  }
+}
+
+// Both networks' grids in one fully unrolled level loop: per level the
+// theta and phi gathers (16 independent loads) are in flight together.
+// Features go out as 16-byte chunks: tile A (theta input, K = KA columns)
+// and tile P (phi grid features, K = L*F columns).
+template <int L, int F>
+__device__ __forceinline__ void grids_to_tiles(const GridLevels& gt, const __half* __restrict__ tab_t,
+                                               const GridLevels& gp, const __half* __restrict__ tab_p,
+                                               const float* q, uint8_t* tile_a, uint32_t ka,
+                                               uint8_t* tile_p, uint32_t row) {
+  constexpr int kLevelsPerChunk = 8 / F;  // 8 fp16 features per 16-byte chunk
+  __half2 ct[4], cp[4];
+#pragma unroll
+  for (int l = 0; l < L; ++l) {
+    float ft[F], fp[F];
+    grid_level<F>(gt, l, gt.interp, tab_t, q[0], q[1], q[2], ft);
+    grid_level<F>(gp, l, gp.interp, tab_p, q[0], q[1], q[2], fp);
+#pragma unroll
+    for (int j = 0; j < F; j += 2) {
+      const int slot = ((l % kLevelsPerChunk) * F + j) / 2;
+      ct[slot] = __floats2half2_rn(ft[j], ft[j + 1]);
+      cp[slot] = __floats2half2_rn(fp[j], fp[j + 1]);
+    }
+    if (l % kLevelsPerChunk == kLevelsPerChunk - 1) {
+      const uint32_t kc = static_cast<uint32_t>(l / kLevelsPerChunk);
+      *reinterpret_cast<uint4*>(tile_a + chunk_off(row, kc, ka)) = *reinterpret_cast<uint4*>(ct);
+      *reinterpret_cast<uint4*>(tile_p + chunk_off(row, kc, L * F)) = *reinterpret_cast<uint4*>(cp);
+    }
+  }
+}
+
+// SH(16) of q[3..5] and OneBlob(4 bins) of q[6..8] at columns [col, col+28).
+__device__ __forceinline__ void sh_ob_to_tile(const float* q, uint8_t* tile, uint32_t row,
+                                              uint32_t col, uint32_t K) {
+  float v[28];
+  sh4_encode(q[3], q[4], q[5], v);
+  oneblob_encode<4>(q[6], v + 16);
+  oneblob_encode<4>(q[7], v + 20);
+  oneblob_encode<4>(q[8], v + 24);
+  store_run(tile, row, col, K, v, 28);
+}
+
+__device__ __forceinline__ void ones_to_tile(uint8_t* tile, uint32_t row, uint32_t col0,
+                                             uint32_t col1, uint32_t K) {
+  for (uint32_t c = col0; c < col1; c += 2) store_h2(tile, row, c, K, 1.f, 1.f);
+}
+
+// ------------------------------------------------------------- warpgroup
+struct Wg {
+  uint8_t* tile_a;     // activations / first-layer input (generic pointer)
+  uint32_t tile_a_s;   // shared-space address
+  uint8_t* tile_p;     // side tile (phi grid features)
+  uint32_t tile_p_s;
+  uint32_t tmem;       // accumulator column base, lane 0
+  uint32_t lane_base;  // this warp's TMEM lane offset (address units)
+  uint64_t* bar;       // MMA-completion mbarrier
+  uint32_t phase;
+  uint32_t bar_id;     // named barrier id of the warpgroup
+  uint32_t row;
+  bool leader;
+  uint32_t* err;
+};
+
+// One K segment of an MMA's A operand: `ksteps` K=16 steps read from a
+// canonical tile at `saddr` with `K` columns.
+struct ASeg {
+  uint32_t saddr;
+  uint32_t K;
+  int ksteps;
+};
+
+// Makes this warpgroup's shared-memory writes visible to the tensor cores.
+__device__ __forceinline__ void publish(Wg& c) {
+  fence_proxy_async_smem();
+  __syncwarp();
+  named_bar_sync(c.bar_id, 128);
+}
+
+// D[tmem] = concat(A segments) * W^T. W is the canonical [N x Kw] matrix at
+// w_s. Issued by the leader after publish(); completion arrives on c.bar.
+__device__ __forceinline__ void issue(Wg& c, const ASeg* segs, int nseg, uint32_t w_s, uint32_t Kw,
+                                      uint32_t N) {
+  if (!c.leader) return;
+  tc_fence_after();
+  const uint32_t idesc = idesc_f16(128, N, 0, 0, 0);
+  const uint32_t bsbo = Kw * 16u;
+  int s = 0;
+  for (int g = 0; g < nseg; ++g) {
+    for (int j = 0; j < segs[g].ksteps; ++j, ++s) {
+      const uint64_t ad = smem_desc(segs[g].saddr + j * 256, 128, segs[g].K * 16u);
+      const uint64_t bd = smem_desc(w_s + s * 256, 128, bsbo);
+      mma_f16_ss(c.tmem, ad, bd, idesc, s > 0 ? 1u : 0u);
+    }
+  }
+  mma_commit(c.bar);
+}
+
+__device__ __forceinline__ void wait_mma(Wg& c) {
+  mbar_wait(c.bar, c.phase, c.err, kErrMbarTimeout);
+  c.phase ^= 1u;
+  __syncwarp();
+  tc_fence_after();
+}
+
+// ReLU of the 64 accumulator columns -> fp16 -> tile_a (K = 64).
+__device__ __forceinline__ void relu_to_tile(Wg& c) {
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    uint32_t r[32];
+    tmem_ld32(c.tmem + c.lane_base + h * 32, r);
+    tmem_ld_wait();
+#pragma unroll
+    for (int kc = 0; kc < 4; ++kc) {
+      __half2 v[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        v[j] = __floats2half2_rn(fmaxf(__uint_as_float(r[kc * 8 + 2 * j]), 0.f),
+                                 fmaxf(__uint_as_float(r[kc * 8 + 2 * j + 1]), 0.f));
+      *reinterpret_cast<uint4*>(c.tile_a + chunk_off(c.row, h * 4 + kc, 64)) =
+          *reinterpret_cast<uint4*>(v);
+    }
+  }
+  tc_fence_before();
+}
+
+// Hidden layers 1..n_hidden-1 and the output layer, starting after the first
+// layer's MMA was issued. w_s points at the first hidden matrix. Leaves the
+// n_out logits in TMEM.
+__device__ __forceinline__ void mlp_tail(Wg& c, uint32_t w_s, int n_hidden, uint32_t n_out) {
+  const ASeg a{c.tile_a_s, 64, 4};
+  for (int l = 1; l <= n_hidden; ++l) {
+    wait_mma(c);
+    relu_to_tile(c);
+    publish(c);
+    const bool last = l == n_hidden;
+    issue(c, &a, 1, w_s, 64, last ? n_out : 64u);
+    w_s += (last ? n_out : 64u) * 64u * 2u;
+  }
+  wait_mma(c);
+}
+
+// ------------------------------------------------------------ epilogue
+// Streams the row's logits out of TMEM in chunks of 32 (or 16) columns.
+template <int NB, typename Fn>
+__device__ __forceinline__ void for_each_logit(const Wg& c, Fn&& fn) {
+  constexpr int CH = NB >= 32 ? 32 : 16;
+#pragma unroll 1
+  for (int base = 0; base < NB; base += CH) {
+    uint32_t r[CH];
+    if constexpr (CH == 32) tmem_ld32(c.tmem + c.lane_base + base, r);
+    else tmem_ld16(c.tmem + c.lane_base + base, r);
+    tmem_ld_wait();
+#pragma unroll
+    for (int j = 0; j < CH; ++j) fn(base + j, __uint_as_float(r[j]));
+  }
+}
+
+// softmax2 statistics (train.h:845-862): m = max(0, max z), ls = log(sum exp(z - m)).
+struct SoftmaxStats {
+  float m, ls;
+  __device__ __forceinline__ float pdf(float z, float n) const { return __expf(z - m - ls) * n; }
+};
+
+template <int NB>
+__device__ __forceinline__ SoftmaxStats softmax_stats(const Wg& c) {
+  float m = 0.f;
+  for_each_logit<NB>(c, [&](int, float z) { m = fmaxf(m, z); });
+  float s = 0.f;
+  for_each_logit<NB>(c, [&](int, float z) { s += __expf(z - m); });
+  return SoftmaxStats{m, __logf(s)};
+}
+
+// Inversion sampling (sample_dir_guided_inputs_F, train.h:416-520) with the
+// CDF walk streamed over the logits; identical float sequence to
+// df_math.cuh sample_dir.
+template <int NB, bool LINEAR>
+__device__ __forceinline__ float sample_streamed(const Wg& c, const SoftmaxStats& st, float u, float u2) {
+  const float n = static_cast<float>(NB);
+  const float inv_n = 1.f / n;
+  float cm1 = 0.f, ci = 0.f, prev_c = 0.f, prev_p = 0.f, lo = 0.f, hi = 0.f, p_last = 0.f;
+  int seg = NB;
+  bool found = false;
+  for_each_logit<NB>(c, [&](int i, float z) {
+    const float p = st.pdf(z, n);
+    if constexpr (LINEAR) {
+      const float cc = i == 0 ? p * 0.5f / n : prev_c + (prev_p + p) / static_cast<float>(2 * NB);
+      if (!found && u < cc) {
+        found = true; seg = i; cm1 = i == 0 ? 0.f : prev_c; ci = cc;
+        lo = i == 0 ? p : prev_p; hi = p;
+      }
+      prev_c = cc;
+    } else {
+      const float cc = prev_c + p / n;
+      if (!found && u < cc) { found = true; seg = i; cm1 = prev_c; ci = cc; }
+      prev_c = cc;
+    }
+    prev_p = p;
+    p_last = p;
+  });
+  if constexpr (LINEAR) {
+    if (!found) { cm1 = prev_c; ci = prev_c + p_last * 0.5f / n; lo = hi = p_last; }
+    int idx_m1 = seg - 1;
+    float v = static_cast<float>(idx_m1) + 0.5f;
+    float ecm = 1.f, v_off = 0.f;
+    if (idx_m1 < 0) { v_off = 0.5f; ecm = 0.5f; }
+    else if (seg > NB - 1) { ecm = 0.5f; }
+    const float m = (hi - lo) * n;
+    const float B = lo * (1 + v) - hi * v;
+    v += v_off;
+    const float A = m * 0.5f;
+    float d;
+    if (fabsf(A) < kEps) {
+      const float w = (ci - cm1) > kEps ? (u - cm1) / (ci - cm1) : u2;
+      d = (v + w * ecm) * inv_n;
+    } else {
+      const float C = -(m * 0.5f) * (v * v * inv_n * inv_n) - (B * v * inv_n) + cm1 - u;
+      const float delta = B * B - 4 * A * C;
+      if (delta < kEps) {
+        d = (v + u2 * ecm) * inv_n;
+      } else {
+        const float sq = sqrtf(delta);
+        const float s0 = (-B + sq) / (2 * A);
+        const float s1 = (-B - sq) / (2 * A);
+        d = A >= 0 ? fmaxf(s0, s1) : fminf(s0, s1);
+      }
+    }
+    return fminf(d, 1.f - kEps);
+  } else {
+    if (!found) { cm1 = prev_c; ci = prev_c; }
+    const float w = (ci - cm1) > kEps ? (u - cm1) / (ci - cm1) : u2;
+    return fminf((static_cast<float>(seg) + w) / n, 1.f - kEps);
+  }
+}
+
+// sample_pdf (train.h:655-681) with the two looked-up bins fetched by one
+// streamed pass.
+template <int NB, bool LINEAR>
+__device__ __forceinline__ float pdf_streamed(const Wg& c, const SoftmaxStats& st, float u) {
+  const float n = static_cast<float>(NB);
+  float idx = u * n;
+  int f, cidx;
+  float w = 0.f;
+  if constexpr (LINEAR) {
+    idx -= 0.5f;
+    f = safe_floor<NB>(idx);
+    cidx = f + 1;
+    w = idx - static_cast<float>(f);
+    if (f < 0) { f = NB - 1; w = 1.0f; }
+    if (cidx > NB - 1) { cidx = 0; w = 0.0f; }
+  } else {
+    f = safe_floor<NB>(idx);
+    cidx = f;
+  }
+  float zf = 0.f, zc = 0.f;
+  for_each_logit<NB>(c, [&](int i, float z) {
+    zf = i == f ? z : zf;
+    zc = i == cidx ? z : zc;
+  });
+  if constexpr (LINEAR) return (1.0f - w) * st.pdf(zf, n) + w * st.pdf(zc, n);
+  else return st.pdf(zf, n);
+}
+
+// Result of the per-row DF epilogue of one network.
+struct RowResult {
+  float u;    // sampled (or given) square coordinate
+  float pdf;  // interpolated pdf at u
+};
+
+// The whole thetaPostInference / phiPostInference row epilogue
+// (train.h:896-929) for one network, logits read once from TMEM into
+// registers: softmax2 x N, inversion sampling when `guided` (else u is the
+// given coordinate), pdf interpolation at u. Out of line so the theta and
+// phi networks share one copy of the code.
+template <int NB, bool LINEAR>
+__device__ __noinline__ RowResult row_epilogue(uint32_t taddr, bool guided, float u_given, float u_main,
+                                               float u_fallback) {
+  float v[NB];
+  if constexpr (NB == 16) {
+    uint32_t r[16];
+    tmem_ld16(taddr, r);
+    tmem_ld_wait();
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+  } else {
+    uint32_t r[NB];
+#pragma unroll
+    for (int c = 0; c < NB / 32; ++c) tmem_ld32(taddr + c * 32, *reinterpret_cast<uint32_t(*)[32]>(r + c * 32));
+    tmem_ld_wait();
+#pragma unroll
+    for (int i = 0; i < NB; ++i) v[i] = __uint_as_float(r[i]);
+  }
+  tc_fence_before();
+  // softmax2 (train.h:845-862): max from 0, exp(z - m - log(sum)), x N
+  float m = 0.0f;
+#pragma unroll
+  for (int i = 0; i < NB; ++i) m = fmaxf(m, v[i]);
+  float s = 0.0f;
+#pragma unroll
+  for (int i = 0; i < NB; ++i) s += __expf(v[i] - m);
+  const float ls = __logf(s);
+#pragma unroll
+  for (int i = 0; i < NB; ++i) v[i] = __expf(v[i] - m - ls) * static_cast<float>(NB);
+  RowResult r;
+  r.u = guided ? sample_dir<NB, LINEAR>(v, u_main, u_fallback) : u_given;
+  r.pdf = sample_pdf<NB, LINEAR>(v, r.u);
+  return r;
+}
+
+}  // namespace tile
+}  // namespace gdf

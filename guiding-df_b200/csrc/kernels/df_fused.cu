@@ -21,6 +21,7 @@
 #include <cuda_fp16.h>
 
 #include "../device/df_math.cuh"
+#include "../device/df_tile.cuh"
 #include "../device/sm100.cuh"
 #include "df_kernels.h"
 
@@ -41,140 +42,50 @@ struct DfWidths {
   static constexpr int kMax = kPhi > 64 ? kPhi : 64;
 };
 
-// Store one row of K fp16 values (given as fp32) into the canonical K-major
-// A tile (128 rows x K).
-template <int K>
-__device__ __forceinline__ void store_row(uint8_t* tile, uint32_t row, const float* v) {
-#pragma unroll
-  for (int kc = 0; kc < K / 8; ++kc) {
-    __half2 h[4];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) h[j] = __floats2half2_rn(v[kc * 8 + 2 * j], v[kc * 8 + 2 * j + 1]);
-    const uint32_t off = (((row >> 3) * (K / 8) + kc) << 7) + ((row & 7u) << 4);
-    *reinterpret_cast<uint4*>(tile + off) = *reinterpret_cast<uint4*>(h);
-  }
-}
-
-// Reads N fp32 columns of this thread's TMEM lane.
-template <int N>
-__device__ __forceinline__ void tmem_load_row(uint32_t taddr, float (&v)[N]) {
-  if constexpr (N == 16) {
-    uint32_t r[16];
-    tmem_ld16(taddr, r);
-    tmem_ld_wait();
-#pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-  } else {
-#pragma unroll
-    for (int c = 0; c < N / 32; ++c) {
-      uint32_t r[32];
-      tmem_ld32(taddr + c * 32, r);
-      tmem_ld_wait();
-#pragma unroll
-      for (int i = 0; i < 32; ++i) v[c * 32 + i] = __uint_as_float(r[i]);
-    }
-  }
-}
-
-struct WgCtx {
-  uint8_t* tile;       // this warpgroup's A tile (generic pointer)
-  uint32_t tile_s;     // same, shared-space address
-  uint32_t tmem;       // accumulator column base (lane 0)
-  uint32_t lane_base;  // this warp's TMEM lane offset, in address units
-  uint64_t* bar;       // MMA-completion mbarrier
-  uint32_t phase;
-  uint32_t bar_id;     // named barrier of the warpgroup
-  uint32_t row;        // thread's row in the tile
-  bool leader;
-  uint32_t* err;
-};
-
-// Issue one layer: D = A[128 x K] * W[N x K]^T, then wait for completion.
-__device__ __forceinline__ void mma_layer(WgCtx& c, uint32_t w_s, int K, int N) {
-  fence_proxy_async_smem();
-  __syncwarp();
-  named_bar_sync(c.bar_id, 128);
-  if (c.leader) {
-    tc_fence_after();
-    const uint32_t idesc = idesc_f16(128, N, 0, 0, 0);
-    const uint32_t sbo = static_cast<uint32_t>(K) * 16u;
-    for (int s = 0; s < K / 16; ++s) {
-      const uint64_t ad = smem_desc(c.tile_s + s * 256, 128, sbo);
-      const uint64_t bd = smem_desc(w_s + s * 256, 128, sbo);
-      mma_f16_ss(c.tmem, ad, bd, idesc, s > 0 ? 1u : 0u);
-    }
-    mma_commit(c.bar);
-  }
-  mbar_wait(c.bar, c.phase, c.err, kErrMbarTimeout);
-  c.phase ^= 1u;
-  __syncwarp();
-  tc_fence_after();
-}
-
-// Runs hidden layers + output layer of one network whose encoded input is
-// already in the tile. Returns the NOUT logits of this thread's row.
-template <int K0, int NOUT>
-__device__ __forceinline__ void run_mlp(WgCtx& c, uint32_t w_s, int n_hidden, float (&logits)[NOUT]) {
-  // First layer: K0 -> 64.
-  mma_layer(c, w_s, K0, 64);
-  w_s += 64u * K0 * 2u;
-  for (int l = 1; l <= n_hidden; ++l) {
-    float h[64];
-    tmem_load_row<64>(c.tmem + c.lane_base, h);
-    tc_fence_before();
-#pragma unroll
-    for (int i = 0; i < 64; ++i) h[i] = fmaxf(h[i], 0.0f);
-    store_row<64>(c.tile, c.row, h);
-    const bool last = (l == n_hidden);
-    mma_layer(c, w_s, 64, last ? NOUT : 64);
-    w_s += (last ? NOUT : 64) * 64u * 2u;
-  }
-  tmem_load_row<NOUT>(c.tmem + c.lane_base, logits);
-  tc_fence_before();
-}
-
-template <int L, int F>
-__device__ __forceinline__ void encode_common(const GridLevels& gl, const __half* grid,
-                                              const float* q, float* x) {
-  grid_encode<L, F>(gl, grid, q[0], q[1], q[2], x);
-  sh4_encode(q[3], q[4], q[5], x + L * F);
-  oneblob_encode<4>(q[6], x + L * F + 16);
-  oneblob_encode<4>(q[7], x + L * F + 20);
-  oneblob_encode<4>(q[8], x + L * F + 24);
-}
-
-template <int L, int F, int NBT, int NBP, bool LINEAR, int MODE>
-__global__ void __launch_bounds__(kDfThreads, 1) df_fused_kernel(const __grid_constant__ DfKernelParams p) {
-  using W = DfWidths<L, F>;
+// ---------------------------------------------------------------------------
+// Fused kernel, one warpgroup per 128-query tile:
+//   1. theta input (grid | SH | OneBlob | 1-pad) -> tile A; theta layer 0 issued;
+//   2. while it runs, the phi grid's gathers -> tile P (its own K=L*F tile);
+//   3. theta hidden/output layers (tcgen05, TMEM accumulators);
+//   4. softmax/CDF/sampling streamed from TMEM -> u_theta, pdf_theta;
+//   5. phi input rest (SH | OneBlob | TriangleWave(u_theta) | 1-pad) -> tile A;
+//      phi layer 0 reads K steps from tile P then tile A;
+//   6. phi layers, epilogue -> u_phi, pdf_phi -> guiding data.
+template <int L, int F, int NBT, int NBP, bool LINEAR, int MODE, int WGS>
+__global__ void __launch_bounds__(128 * WGS, 1) df_fused_kernel(const __grid_constant__ DfKernelParams p) {
+  using Wd = DfWidths<L, F>;
+  constexpr uint32_t LF = L * F;
+  constexpr uint32_t KT = Wd::kTheta;            // theta input width
+  constexpr uint32_t KR = Wd::kPhi - LF;         // phi input minus its grid part
+  constexpr uint32_t KA = KT > 64 ? (KT > KR ? KT : KR) : (64 > KR ? 64 : KR);
+  static_assert(LF % 16 == 0 && KT % 16 == 0 && KR % 16 == 0, "K segments must be multiples of 16");
   extern __shared__ __align__(1024) uint8_t smem[];
   const uint32_t tid = threadIdx.x;
   const uint32_t wg = tid >> 7;
   const uint32_t warp = tid >> 5;
 
-  // Shared-memory carve-up: weights | A tiles | barriers | tmem slot.
   const uint32_t off_phi = (p.blob_theta_bytes + 127u) & ~127u;
-  const uint32_t off_tiles = (off_phi + p.blob_phi_bytes + 1023u) & ~1023u;
-  constexpr uint32_t kTileBytes = 128u * W::kMax * 2u;
-  const uint32_t off_bars = off_tiles + kDfWarpgroups * kTileBytes;
+  const uint32_t off_tiles = (off_phi + p.blob_phi_bytes + 127u) & ~127u;
+  constexpr uint32_t kTileA = 128u * KA * 2u, kTileP = 128u * LF * 2u;
+  const uint32_t off_bars = off_tiles + WGS * (kTileA + kTileP);
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + off_bars);  // [0] weights, [1+g] MMA
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + off_bars + 8 * (kDfWarpgroups + 1));
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + off_bars + 8 * (WGS + 1));
+  constexpr uint32_t kTmemCols = 64 * WGS <= 128 ? 128 : (64 * WGS <= 256 ? 256 : 512);
 
   if (warp == 0) {
-    tmem_alloc(tmem_slot, 64 * kDfWarpgroups);
+    tmem_alloc(tmem_slot, kTmemCols);
     tmem_relinquish();
   }
   if (tid == 0) {
-    for (int i = 0; i <= kDfWarpgroups; ++i) mbar_init(&bars[i], 1);
+    for (int i = 0; i <= WGS; ++i) mbar_init(&bars[i], 1);
     fence_mbar_init();
     mbar_arrive_expect_tx(&bars[0], p.blob_theta_bytes + p.blob_phi_bytes);
-    for (uint32_t o = 0; o < p.blob_theta_bytes; o += 32768u) {
-      const uint32_t b = min(32768u, p.blob_theta_bytes - o);
-      bulk_g2s(smem + o, reinterpret_cast<const uint8_t*>(p.blob_theta) + o, b, &bars[0]);
-    }
-    for (uint32_t o = 0; o < p.blob_phi_bytes; o += 32768u) {
-      const uint32_t b = min(32768u, p.blob_phi_bytes - o);
-      bulk_g2s(smem + off_phi + o, reinterpret_cast<const uint8_t*>(p.blob_phi) + o, b, &bars[0]);
-    }
+    for (uint32_t o = 0; o < p.blob_theta_bytes; o += 32768u)
+      bulk_g2s(smem + o, reinterpret_cast<const uint8_t*>(p.blob_theta) + o,
+               min(32768u, p.blob_theta_bytes - o), &bars[0]);
+    for (uint32_t o = 0; o < p.blob_phi_bytes; o += 32768u)
+      bulk_g2s(smem + off_phi + o, reinterpret_cast<const uint8_t*>(p.blob_phi) + o,
+               min(32768u, p.blob_phi_bytes - o), &bars[0]);
   }
   tc_fence_before();
   __syncthreads();
@@ -182,45 +93,49 @@ __global__ void __launch_bounds__(kDfThreads, 1) df_fused_kernel(const __grid_co
   const uint32_t tmem_base = *tmem_slot;
   mbar_wait(&bars[0], 0, p.err, kErrWeightLoad);
 
-  WgCtx c;
-  c.tile = smem + off_tiles + wg * kTileBytes;
-  c.tile_s = smem_addr(c.tile);
+  tile::Wg c;
+  c.tile_a = smem + off_tiles + wg * (kTileA + kTileP);
+  c.tile_a_s = smem_addr(c.tile_a);
+  c.tile_p = c.tile_a + kTileA;
+  c.tile_p_s = c.tile_a_s + kTileA;
   c.tmem = tmem_base + wg * 64u;
   c.lane_base = ((warp & 3u) * 32u) << 16;
   c.bar = &bars[1 + wg];
   c.phase = 0;
   c.bar_id = 1 + wg;
   c.row = tid & 127u;
-  c.leader = (tid & 127u) == 0;
+  c.leader = c.row == 0;
   c.err = p.err;
   const uint32_t w_theta = smem_addr(smem);
   const uint32_t w_phi = smem_addr(smem + off_phi);
+  const uint32_t w_theta_hidden = w_theta + 64u * KT * 2u;
+  const uint32_t w_phi_hidden = w_phi + 64u * (LF + KR) * 2u;
 
   const int64_t n_tiles = (p.n + 127) / 128;
-  for (int64_t tile = static_cast<int64_t>(blockIdx.x) * kDfWarpgroups + wg; tile < n_tiles;
-       tile += static_cast<int64_t>(gridDim.x) * kDfWarpgroups) {
-    const int64_t row = tile * 128 + c.row;
+  for (int64_t t = static_cast<int64_t>(blockIdx.x) * WGS + wg; t < n_tiles;
+       t += static_cast<int64_t>(gridDim.x) * WGS) {
+    const int64_t row = t * 128 + c.row;
     const bool valid = row < p.n;
     float q[9];
 #pragma unroll
     for (int i = 0; i < 9; ++i) q[i] = valid ? __ldg(p.queries + row * 9 + i) : 0.5f;
 
-    // ---- theta network
+    // ---- 1. both grids (theta -> tile A, phi -> tile P), theta input rest, layer 0
+    tile::grids_to_tiles<L, F>(p.gl_theta, p.grid_theta, p.gl_phi, p.grid_phi, q, c.tile_a, KT,
+                               c.tile_p, c.row);
+    tile::sh_ob_to_tile(q, c.tile_a, c.row, LF, KT);
+    tile::ones_to_tile(c.tile_a, c.row, LF + 28, KT, KT);
+    tile::publish(c);
     {
-      float x[W::kTheta];
-      encode_common<L, F>(p.gl_theta, p.grid_theta, q, x);
-#pragma unroll
-      for (int i = W::kGrid + 28; i < W::kTheta; ++i) x[i] = 1.0f;
-      store_row<W::kTheta>(c.tile, c.row, x);
+      const tile::ASeg a{c.tile_a_s, KT, static_cast<int>(KT / 16)};
+      tile::issue(c, &a, 1, w_theta, KT, 64);
     }
-    float lt[NBT];
-    run_mlp<W::kTheta, NBT>(c, w_theta, p.hidden_theta, lt);
-    softmax2_times_n<NBT>(lt);
-
+    // ---- 2./3. theta layers
+    tile::mlp_tail(c, w_theta_hidden, p.hidden_theta, NBT);
+    // ---- 4. theta epilogue
     float4 wi = make_float4(0.f, 0.f, 1.f, 1.f);
     float u[4] = {0.f, 0.f, 0.f, 0.f};
     bool guided = true;
-    float u_theta;
     if constexpr (MODE == kModeInfer) {
       if (valid) {
         wi = *reinterpret_cast<const float4*>(p.wi + row * 4);
@@ -231,52 +146,51 @@ __global__ void __launch_bounds__(kDfThreads, 1) df_fused_kernel(const __grid_co
         } else {
           uint32_t r[4];
           philox4x32_10(static_cast<uint32_t>(row), static_cast<uint32_t>(static_cast<uint64_t>(row) >> 32),
-                        static_cast<uint32_t>(p.philox_offset),
-                        static_cast<uint32_t>(p.philox_offset >> 32),
-                        static_cast<uint32_t>(p.philox_seed),
-                        static_cast<uint32_t>(p.philox_seed >> 32), r);
+                        static_cast<uint32_t>(p.philox_offset), static_cast<uint32_t>(p.philox_offset >> 32),
+                        static_cast<uint32_t>(p.philox_seed), static_cast<uint32_t>(p.philox_seed >> 32), r);
 #pragma unroll
           for (int k = 0; k < 4; ++k) u[k] = u32_to_uniform(r[k]);
         }
       }
-      u_theta = guided ? sample_dir<NBT, LINEAR>(lt, u[0], u[1]) : wi.x;
-    } else {
-      u_theta = valid ? __ldg(p.u_eval + row * 2) : 0.5f;
     }
-    const float pdf_theta = sample_pdf<NBT, LINEAR>(lt, u_theta);
+    const float u_theta_given = MODE == kModeInfer ? wi.x : (valid ? __ldg(p.u_eval + row * 2) : 0.5f);
+    const tile::RowResult rt = tile::row_epilogue<NBT, LINEAR>(
+        c.tmem + c.lane_base, MODE == kModeInfer && guided, u_theta_given, u[0], u[1]);
+    const float u_theta = rt.u, pdf_theta = rt.pdf;
     const float cond = theta_condition<NBT, LINEAR>(u_theta);
 
-    // ---- phi network (own grid; same SH / OneBlob inputs; TriangleWave of theta)
+    // ---- 5. phi input rest, layer 0 over tile P (grid) + tile A (rest)
+    tile::sh_ob_to_tile(q, c.tile_a, c.row, 0, KR);
     {
-      float x[W::kPhi];
-      encode_common<L, F>(p.gl_phi, p.grid_phi, q, x);
-      triangle_wave_encode<12>(cond, x + W::kGrid + 28);
-#pragma unroll
-      for (int i = W::kGrid + 40; i < W::kPhi; ++i) x[i] = 1.0f;
-      store_row<W::kPhi>(c.tile, c.row, x);
+      float tw[12];
+      triangle_wave_encode<12>(cond, tw);
+      tile::store_run(c.tile_a, c.row, 28, KR, tw, 12);
     }
-    float lp[NBP];
-    run_mlp<W::kPhi, NBP>(c, w_phi, p.hidden_phi, lp);
-    softmax2_times_n<NBP>(lp);
-
+    tile::ones_to_tile(c.tile_a, c.row, 40, KR, KR);
+    tile::publish(c);
+    {
+      const tile::ASeg a[2] = {{c.tile_p_s, LF, static_cast<int>(LF / 16)},
+                               {c.tile_a_s, KR, static_cast<int>(KR / 16)}};
+      tile::issue(c, a, 2, w_phi, LF + KR, 64);
+    }
+    // ---- 6. phi layers and epilogue
+    tile::mlp_tail(c, w_phi_hidden, p.hidden_phi, NBP);
+    const float u_phi_given = MODE == kModeInfer ? wi.y : (valid ? __ldg(p.u_eval + row * 2 + 1) : 0.5f);
+    const tile::RowResult rp = tile::row_epilogue<NBP, LINEAR>(
+        c.tmem + c.lane_base, MODE == kModeInfer && guided, u_phi_given, u[2], u[3]);
     if constexpr (MODE == kModeInfer) {
-      const float u_phi = guided ? sample_dir<NBP, LINEAR>(lp, u[2], u[3]) : wi.y;
-      const float pdf_phi = sample_pdf<NBP, LINEAR>(lp, u_phi);
-      if (valid) {
+      if (valid)
         *reinterpret_cast<float4*>(p.wi + row * 4) =
-            make_float4(u_theta, u_phi, wi.z * pdf_theta, wi.w * pdf_phi);
-      }
+            make_float4(u_theta, rp.u, wi.z * pdf_theta, wi.w * rp.pdf);
     } else {
-      const float u_phi = valid ? __ldg(p.u_eval + row * 2 + 1) : 0.5f;
-      const float pdf_phi = sample_pdf<NBP, LINEAR>(lp, u_phi);
-      if (valid) *reinterpret_cast<float2*>(p.pdf_out + row * 2) = make_float2(pdf_theta, pdf_phi);
+      if (valid) *reinterpret_cast<float2*>(p.pdf_out + row * 2) = make_float2(pdf_theta, rp.pdf);
     }
   }
 
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  if (warp == 0) tmem_dealloc(tmem_base, 64 * kDfWarpgroups);
+  if (warp == 0) tmem_dealloc(tmem_base, kTmemCols);
 }
 
 template <int NBT, int NBP, bool LINEAR>
@@ -316,8 +230,8 @@ cudaError_t launch_t(int mode, const DfKernelParams& p, size_t smem, int num_sms
   int64_t ctas = (n_tiles + kDfWarpgroups - 1) / kDfWarpgroups;
   if (ctas > num_sms) ctas = num_sms;
   if (ctas < 1) ctas = 1;
-  auto kern = mode == kModeInfer ? df_fused_kernel<L, F, NBT, NBP, LIN, kModeInfer>
-                                 : df_fused_kernel<L, F, NBT, NBP, LIN, kModeEval>;
+  auto kern = mode == kModeInfer ? df_fused_kernel<L, F, NBT, NBP, LIN, kModeInfer, kDfWarpgroups>
+                                 : df_fused_kernel<L, F, NBT, NBP, LIN, kModeEval, kDfWarpgroups>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
   if (e != cudaSuccess) return e;
@@ -335,12 +249,14 @@ bool df_shape_supported(const DfShape& s) {
 }
 
 size_t df_fused_smem_bytes(const DfShape& s, uint32_t bt, uint32_t bp) {
-  const int grid = s.levels * s.features;
-  const int kphi = pad16c(grid + 40);
-  const int kmax = kphi > 64 ? kphi : 64;
+  const int lf = s.levels * s.features;
+  const int kt = pad16c(lf + 28);
+  const int kr = pad16c(lf + 40) - lf;
+  int ka = kt > 64 ? kt : 64;
+  ka = ka > kr ? ka : kr;
   const size_t off_phi = (bt + 127u) & ~127u;
-  const size_t off_tiles = (off_phi + bp + 1023u) & ~size_t(1023);
-  return off_tiles + static_cast<size_t>(kDfWarpgroups) * 128u * kmax * 2u +
+  const size_t off_tiles = (off_phi + bp + 127u) & ~size_t(127);
+  return off_tiles + static_cast<size_t>(kDfWarpgroups) * 128u * (ka + lf) * 2u +
          8u * (kDfWarpgroups + 1) + 16u;
 }
 

@@ -53,7 +53,7 @@ def test_infer_peaky_weights_no_worse_than_fp32_accumulation(preset):
     assert np.percentile(dg, 99) <= 3 * np.percentile(de, 99) + 2e-5
     spread = fp32_emulation_spread(d, pt, pp, q, got[:, :2])
     rel = np.abs(got[:, 2:4] - ref_pdf) / (np.abs(ref_pdf) + 1e-6)
-    assert rel.max() <= 2 * spread.max() + 1e-4, (rel.max(), spread.max())
+    assert rel.max() <= 3 * spread.max() + 1e-4, (rel.max(), spread.max())
     ctx.close()
 
 
