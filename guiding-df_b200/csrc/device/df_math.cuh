@@ -195,6 +195,27 @@ __device__ __forceinline__ void softmax2_times_n(float (&v)[N]) {
   for (int i = 0; i < N; ++i) v[i] *= static_cast<float>(N);
 }
 
+// softmaxMultFactor<__half> of the training forward (train.h:872-893 with
+// T = fp16): fp16 logits, softmax2 rounded to fp16, times N in fp16 (exact
+// for power-of-two N). In place, results as float.
+template <int N>
+__device__ __forceinline__ void softmax_table_fp16(float (&v)[N]) {
+  float mx = 0.0f;
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    v[i] = __half2float(__float2half_rn(v[i]));
+    mx = fmaxf(mx, v[i]);
+  }
+  float s = 0.0f;
+#pragma unroll
+  for (int i = 0; i < N; ++i) s += __expf(v[i] - mx);
+  const float ls = __logf(s);
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+    v[i] = __half2float(__float2half_rn(__half2float(__float2half_rn(__expf(v[i] - mx - ls))) *
+                                        static_cast<float>(N)));
+}
+
 template <int N>
 __device__ __forceinline__ int safe_floor(float v) {
   const int f = static_cast<int>(floorf(v));

@@ -151,15 +151,15 @@ __device__ __forceinline__ void grid_to_tile(const GridLevels& s, int n_levels, 
 template <int L, int F>
 __device__ __forceinline__ void grids_to_tiles(const GridLevels& gt, const __half* __restrict__ tab_t,
                                                const GridLevels& gp, const __half* __restrict__ tab_p,
-                                               const float* q, uint8_t* tile_a, uint32_t ka,
-                                               uint8_t* tile_p, uint32_t row) {
+                                               const float* q, const float* qp, uint8_t* tile_a,
+                                               uint32_t ka, uint8_t* tile_p, uint32_t row) {
   constexpr int kLevelsPerChunk = 8 / F;  // 8 fp16 features per 16-byte chunk
   __half2 ct[4], cp[4];
 #pragma unroll
   for (int l = 0; l < L; ++l) {
     float ft[F], fp[F];
     grid_level<F>(gt, l, gt.interp, tab_t, q[0], q[1], q[2], ft);
-    grid_level<F>(gp, l, gp.interp, tab_p, q[0], q[1], q[2], fp);
+    grid_level<F>(gp, l, gp.interp, tab_p, qp[0], qp[1], qp[2], fp);
 #pragma unroll
     for (int j = 0; j < F; j += 2) {
       const int slot = ((l % kLevelsPerChunk) * F + j) / 2;
@@ -449,6 +449,33 @@ __device__ __noinline__ RowResult row_epilogue(uint32_t taddr, bool guided, floa
   r.u = guided ? sample_dir<NB, LINEAR>(v, u_main, u_fallback) : u_given;
   r.pdf = sample_pdf<NB, LINEAR>(v, r.u);
   return r;
+}
+
+// Training flavour of the epilogue (forward of LearnedDistribution::trainStep,
+// learnedDistribution.cpp:252-262): the logits are the network's fp16
+// outputs, softmax2 is stored as fp16 and multiplied by N in fp16
+// (softmaxMultFactor), and the pdf at the record's direction interpolates
+// those fp16 values (combine_AR_pdf_and_dl_doutput, train.h:946-948).
+template <int NB, bool LINEAR>
+__device__ __noinline__ float row_pdf_train(uint32_t taddr, float u) {
+  float v[NB];
+  if constexpr (NB == 16) {
+    uint32_t r[16];
+    tmem_ld16(taddr, r);
+    tmem_ld_wait();
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+  } else {
+    uint32_t r[NB];
+#pragma unroll
+    for (int c = 0; c < NB / 32; ++c) tmem_ld32(taddr + c * 32, *reinterpret_cast<uint32_t(*)[32]>(r + c * 32));
+    tmem_ld_wait();
+#pragma unroll
+    for (int i = 0; i < NB; ++i) v[i] = __uint_as_float(r[i]);
+  }
+  tc_fence_before();
+  softmax_table_fp16<NB>(v);
+  return sample_pdf<NB, LINEAR>(v, u);
 }
 
 }  // namespace tile

@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "../kernels/df_kernels.h"
+#include "../kernels/train_kernels.h"
 #include "context.h"
 
 using gdf::Context;
@@ -230,6 +231,31 @@ gdf_status init_params(Net& n, uint32_t seed, uint32_t stream_id) {
   return upload_params(n, h);
 }
 
+void free_ws(gdf::TrainWorkspace& w) {
+  cudaFree(w.fwd);
+  for (float*& p : w.partial) cudaFree(p);
+  cudaFree(w.sq);
+  cudaFree(w.stats);
+  cudaFree(w.dropped);
+  w = gdf::TrainWorkspace{};
+}
+
+gdf_status alloc_ws(Context& c) {
+  gdf::TrainWorkspace& w = c.ws;
+  gdf_status s;
+  const int64_t cap = c.cfg.max_train_batch > 0 ? c.cfg.max_train_batch : 65536;
+  w.capacity = cap;
+  if ((s = dalloc(&w.fwd, static_cast<size_t>(cap) * 4))) return s;
+  for (int i = 0; i < 3; ++i)
+    if (c.net[i].present &&
+        (s = dalloc(&w.partial[i], static_cast<size_t>(c.num_sms) * static_cast<size_t>(c.net[i].n_mlp))))
+      return s;
+  if ((s = dalloc(&w.sq, 3 * static_cast<size_t>(gdf::kAdamBlocks))) || (s = dalloc(&w.stats, 2)) ||
+      (s = dalloc(&w.dropped, 1)))
+    return s;
+  return GDF_OK;
+}
+
 Net* net_of(Context* c, int32_t id) {
   if (!c || id < 0 || id > 2 || !c->net[id].present) return nullptr;
   return &c->net[id];
@@ -382,6 +408,7 @@ gdf_status gdf_create(const gdf_config* cfg, gdf_ctx** out) {
   cudaDeviceGetAttribute(&c.num_sms, cudaDevAttrMultiProcessorCount, c.device);
   auto cleanup = [&](gdf_status st) {
     for (Net& n : c.net) free_net(n);
+    free_ws(c.ws);
     cudaFree(c.d_err);
     delete h;
     return st;
@@ -392,6 +419,7 @@ gdf_status gdf_create(const gdf_config* cfg, gdf_ctx** out) {
   for (Net& n : c.net)
     if (n.present && (s = alloc_net(n))) return cleanup(s);
   if ((s = dalloc(&c.d_err, 1))) return cleanup(s);
+  if ((s = alloc_ws(c))) return cleanup(s);
   e = cudaMemset(c.d_err, 0, 4);
   if (e != cudaSuccess) return cleanup(cuda_fail(e, "cudaMemset"));
   for (int i = 0; i < 3; ++i)
@@ -405,6 +433,7 @@ gdf_status gdf_destroy(gdf_ctx* ctx) {
   if (!ctx) return GDF_OK;
   cudaDeviceSynchronize();
   for (Net& n : ctx->c.net) free_net(n);
+  free_ws(ctx->c.ws);
   cudaFree(ctx->c.d_err);
   delete ctx;
   return GDF_OK;
@@ -576,9 +605,149 @@ gdf_status gdf_post_inference(gdf_ctx* ctx, const float* lt, const float* lp, co
   return GDF_OK;
 }
 
-gdf_status gdf_train_step(gdf_ctx*, const float*, const float*, const float*, int64_t,
-                          gdf_train_stats*, void*) {
-  return fail(GDF_ERR_UNSUPPORTED, "gdf_train_step: not built yet");
+static gdf::AdamParams adam_params(Context& c, int id, const gdf_adam_config& a, float loss_scale,
+                                    double* sq) {
+  Net& n = c.net[id];
+  gdf::AdamParams p;
+  std::memset(&p, 0, sizeof(p));
+  p.n = n.n_params;
+  p.n_mlp = n.n_mlp;
+  p.partials = c.ws.partial[id];
+  p.n_partials = c.num_sms;
+  p.grid_grad = n.grad;
+  p.master = n.master;
+  p.w16 = n.w16;
+  p.ema16 = n.ema16;
+  p.m = n.adam_m;
+  p.v = n.adam_v;
+  p.step = n.adam_step;
+  p.blob_w16 = n.blob_w16;
+  p.blob_ema = n.blob_ema;
+  int64_t off = 0;
+  p.n_layers = static_cast<int32_t>(n.rows.size());
+  for (size_t l = 0; l < n.rows.size(); ++l) {
+    p.layer_off[l] = off;
+    p.layer_cols[l] = n.cols[l];
+    off += static_cast<int64_t>(n.rows[l]) * n.cols[l];
+  }
+  // AdamOptimizer::step increments its step before use (adam.h:150-152);
+  // EmaOptimizer::step debiases with that step (ema.h:102-110).
+  const uint32_t step = ++n.opt_step;
+  p.loss_scale = loss_scale;
+  p.lr = a.learning_rate;
+  p.beta1 = a.beta1;
+  p.beta2 = a.beta2;
+  p.eps = a.epsilon;
+  p.l2_reg = a.l2_reg;
+  p.ema_decay = a.ema_decay;
+  p.debias_old = 1.0f - static_cast<float>(std::pow(static_cast<double>(a.ema_decay), static_cast<double>(step - 1)));
+  p.debias_new = 1.0f / (1.0f - static_cast<float>(std::pow(static_cast<double>(a.ema_decay), static_cast<double>(step))));
+  p.sq_partial = sq;
+  p.n_blocks = gdf::kAdamBlocks;
+  return p;
+}
+
+gdf_status gdf_train_step(gdf_ctx* ctx, const float* in_theta, const float* in_phi,
+                          const float* target, int64_t n, gdf_train_stats* stats, void* stream) {
+  if (!ctx) return fail(GDF_ERR_INVALID_ARG, "ctx is null");
+  Context& c = ctx->c;
+  if (n <= 0) return fail(GDF_ERR_INVALID_ARG, "n must be positive");
+  if (n > c.ws.capacity) return fail(GDF_ERR_INVALID_ARG, "n exceeds max_train_batch");
+  gdf_status s;
+  if ((s = check_ptr(in_theta, "in_theta")) || (s = check_ptr(in_phi, "in_phi")) ||
+      (s = check_ptr(target, "target")))
+    return s;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const gdf::DfShape shape = df_shape(c);
+  GDF_CUDA(cudaMemsetAsync(c.ws.dropped, 0, sizeof(unsigned long long), st));
+
+  // 1. forward of both networks with fp16 pdf tables, loss and prefix
+  gdf::DfKernelParams p = df_params(c);
+  p.grid_theta = c.net[0].w16 + c.net[0].n_mlp;
+  p.grid_phi = c.net[1].w16 + c.net[1].n_mlp;
+  p.blob_theta = c.net[0].blob_w16;
+  p.blob_phi = c.net[1].blob_w16;
+  p.queries = in_theta;
+  p.in_phi = in_phi;
+  p.target = target;
+  p.train_out = c.ws.fwd;
+  p.n_dropped = c.ws.dropped;
+  p.loss_scale_per_record = c.cfg.loss_scale / static_cast<float>(n);
+  p.n = n;
+  cudaError_t e = gdf::launch_df_fused(shape, gdf::kModeTrainFwd, p, c.num_sms, st);
+  if (e != cudaSuccess) return cuda_fail(e, "df_fused (train forward)");
+
+  // 2. backward of each network
+  for (int id = 0; id < 2; ++id) {
+    Net& nt = c.net[id];
+    gdf::DfBwdParams b;
+    std::memset(&b, 0, sizeof(b));
+    b.in = id == 0 ? in_theta : in_phi;
+    b.in_stride = id == 0 ? 9 : 10;
+    b.target = target;
+    b.fwd = c.ws.fwd;
+    b.n = n;
+    b.blob = nt.blob_w16;
+    b.blob_bytes = nt.blob_bytes;
+    b.grid = nt.w16 + nt.n_mlp;
+    b.grid_grad = nt.grad + nt.n_mlp;
+    b.wgrad_partial = c.ws.partial[id];
+    b.n_mlp = nt.n_mlp;
+    b.hidden = nt.hidden;
+    b.err = c.d_err;
+    b.gl = nt.gl;
+    e = gdf::launch_df_train_bwd(shape, id == 1, b, c.num_sms, st);
+    if (e != cudaSuccess) return cuda_fail(e, "df_train_bwd");
+  }
+  // 3. Adam + EMA, re-layout of the weights
+  for (int id = 0; id < 2; ++id) {
+    gdf::AdamParams a = adam_params(c, id, c.cfg.adam_df, c.cfg.loss_scale,
+                                    c.ws.sq + static_cast<size_t>(id) * gdf::kAdamBlocks);
+    a.grid_grad = c.net[id].grad + c.net[id].n_mlp;
+    e = gdf::launch_adam_ema(a, st);
+    if (e != cudaSuccess) return cuda_fail(e, "adam_ema");
+  }
+  // 4. FP64 loss and gradient-norm reductions
+  e = gdf::launch_train_stats(c.ws.fwd, n, c.ws.sq, 2 * gdf::kAdamBlocks, c.ws.stats, st);
+  if (e != cudaSuccess) return cuda_fail(e, "train_stats");
+  if (stats) {
+    double h[2];
+    unsigned long long dropped = 0;
+    GDF_CUDA(cudaMemcpyAsync(h, c.ws.stats, sizeof(h), cudaMemcpyDeviceToHost, st));
+    GDF_CUDA(cudaMemcpyAsync(&dropped, c.ws.dropped, sizeof(dropped), cudaMemcpyDeviceToHost, st));
+    GDF_CUDA(cudaStreamSynchronize(st));
+    stats->loss = h[0] / static_cast<double>(n);
+    stats->grad_norm = std::sqrt(h[1]);
+    stats->n_records = n;
+    stats->n_dropped = static_cast<int64_t>(dropped);
+  }
+  return GDF_OK;
+}
+
+gdf_status gdf_get_optimizer_state(const gdf_ctx* ctx, int32_t net, float* m, float* v,
+                                   uint32_t* steps, int64_t n, uint32_t* opt_step) {
+  Net* nt = net_of(const_cast<Context*>(ctx ? &ctx->c : nullptr), net);
+  if (!nt) return fail(GDF_ERR_INVALID_ARG, "bad ctx / net id");
+  if (n != nt->n_params) return fail(GDF_ERR_INVALID_ARG, "parameter count mismatch");
+  GDF_CUDA(cudaDeviceSynchronize());
+  if (m) GDF_CUDA(cudaMemcpy(m, nt->adam_m, static_cast<size_t>(n) * 4, cudaMemcpyDeviceToHost));
+  if (v) GDF_CUDA(cudaMemcpy(v, nt->adam_v, static_cast<size_t>(n) * 4, cudaMemcpyDeviceToHost));
+  if (steps) GDF_CUDA(cudaMemcpy(steps, nt->adam_step, static_cast<size_t>(n) * 4, cudaMemcpyDeviceToHost));
+  if (opt_step) *opt_step = nt->opt_step;
+  return GDF_OK;
+}
+
+gdf_status gdf_set_optimizer_state(gdf_ctx* ctx, int32_t net, const float* m, const float* v,
+                                   const uint32_t* steps, int64_t n, uint32_t opt_step) {
+  Net* nt = net_of(ctx ? &ctx->c : nullptr, net);
+  if (!nt) return fail(GDF_ERR_INVALID_ARG, "bad ctx / net id");
+  if (n != nt->n_params) return fail(GDF_ERR_INVALID_ARG, "parameter count mismatch");
+  if (m) GDF_CUDA(cudaMemcpy(nt->adam_m, m, static_cast<size_t>(n) * 4, cudaMemcpyHostToDevice));
+  if (v) GDF_CUDA(cudaMemcpy(nt->adam_v, v, static_cast<size_t>(n) * 4, cudaMemcpyHostToDevice));
+  if (steps) GDF_CUDA(cudaMemcpy(nt->adam_step, steps, static_cast<size_t>(n) * 4, cudaMemcpyHostToDevice));
+  nt->opt_step = opt_step;
+  GDF_CUDA(cudaDeviceSynchronize());
+  return GDF_OK;
 }
 
 gdf_status gdf_nrc_query(gdf_ctx*, const float*, float*, int64_t, void*) {

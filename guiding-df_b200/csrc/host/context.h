@@ -37,12 +37,25 @@ struct Net {
   uint32_t opt_step = 0;       // optimizer step counter (Adam m_current_step)
 };
 
+// Device workspace of the training step, sized by max_train_batch.
+struct TrainWorkspace {
+  int64_t capacity = 0;
+  float* fwd = nullptr;                   // [capacity x 4]
+  float* partial[3] = {nullptr, nullptr, nullptr};  // [num_sms x n_mlp] per net
+  double* sq = nullptr;                   // [3 x kAdamBlocks] optimizer partials
+  double* stats = nullptr;                // [2]: loss sum, squared gradient norm
+  unsigned long long* dropped = nullptr;  // [1]
+};
+
+constexpr int kAdamBlocks = 1184;  // 8 x 148 SMs
+
 struct Context {
   gdf_config cfg{};
   int device = 0;
   int num_sms = 148;
   Net net[3];  // theta, phi, nrc
   uint32_t* d_err = nullptr;  // device error word of bounded waits
+  TrainWorkspace ws;
 };
 
 // Grid level tables (tcnn encodings/grid.h:967-1012, grid_index :165-188).

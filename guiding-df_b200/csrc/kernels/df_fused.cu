@@ -116,12 +116,35 @@ __global__ void __launch_bounds__(128 * WGS, 1) df_fused_kernel(const __grid_con
        t += static_cast<int64_t>(gridDim.x) * WGS) {
     const int64_t row = t * 128 + c.row;
     const bool valid = row < p.n;
-    float q[9];
+    float q[9], qp[10];
 #pragma unroll
     for (int i = 0; i < 9; ++i) q[i] = valid ? __ldg(p.queries + row * 9 + i) : 0.5f;
+    bool record_ok = true;
+    float tg[9];
+    if constexpr (MODE == kModeTrainFwd) {
+      // the phi network reads its own record (GuidedInputPhi, slot 9 = theta)
+#pragma unroll
+      for (int i = 0; i < 10; ++i) qp[i] = valid ? __ldg(p.in_phi + row * 10 + i) : 0.5f;
+#pragma unroll
+      for (int i = 0; i < 9; ++i) tg[i] = valid ? __ldg(p.target + row * 9 + i) : 0.5f;
+      // generate_training_data_AR validity filter (train.cu:77-81)
+#pragma unroll
+      for (int i = 0; i < 9; ++i) record_ok &= !isnan(q[i]) && !isnan(tg[i]);
+#pragma unroll
+      for (int i = 0; i < 10; ++i) record_ok &= !isnan(qp[i]);
+      record_ok &= tg[5] != 0.0f;
+      if (!record_ok) {
+#pragma unroll
+        for (int i = 0; i < 9; ++i) { q[i] = 0.5f; qp[i] = 0.5f; }
+        qp[9] = 0.5f;
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < 9; ++i) qp[i] = q[i];
+    }
 
     // ---- 1. both grids (theta -> tile A, phi -> tile P), theta input rest, layer 0
-    tile::grids_to_tiles<L, F>(p.gl_theta, p.grid_theta, p.gl_phi, p.grid_phi, q, c.tile_a, KT,
+    tile::grids_to_tiles<L, F>(p.gl_theta, p.grid_theta, p.gl_phi, p.grid_phi, q, qp, c.tile_a, KT,
                                c.tile_p, c.row);
     tile::sh_ob_to_tile(q, c.tile_a, c.row, LF, KT);
     tile::ones_to_tile(c.tile_a, c.row, LF + 28, KT, KT);
@@ -153,14 +176,22 @@ __global__ void __launch_bounds__(128 * WGS, 1) df_fused_kernel(const __grid_con
         }
       }
     }
-    const float u_theta_given = MODE == kModeInfer ? wi.x : (valid ? __ldg(p.u_eval + row * 2) : 0.5f);
-    const tile::RowResult rt = tile::row_epilogue<NBT, LINEAR>(
-        c.tmem + c.lane_base, MODE == kModeInfer && guided, u_theta_given, u[0], u[1]);
-    const float u_theta = rt.u, pdf_theta = rt.pdf;
-    const float cond = theta_condition<NBT, LINEAR>(u_theta);
+    float u_theta, pdf_theta, cond;
+    if constexpr (MODE == kModeTrainFwd) {
+      u_theta = tg[0];
+      pdf_theta = tile::row_pdf_train<NBT, LINEAR>(c.tmem + c.lane_base, tg[0]);
+      cond = qp[9];
+    } else {
+      const float u_theta_given = MODE == kModeInfer ? wi.x : (valid ? __ldg(p.u_eval + row * 2) : 0.5f);
+      const tile::RowResult rt = tile::row_epilogue<NBT, LINEAR>(
+          c.tmem + c.lane_base, MODE == kModeInfer && guided, u_theta_given, u[0], u[1]);
+      u_theta = rt.u;
+      pdf_theta = rt.pdf;
+      cond = theta_condition<NBT, LINEAR>(u_theta);
+    }
 
     // ---- 5. phi input rest, layer 0 over tile P (grid) + tile A (rest)
-    tile::sh_ob_to_tile(q, c.tile_a, c.row, 0, KR);
+    tile::sh_ob_to_tile(qp, c.tile_a, c.row, 0, KR);
     {
       float tw[12];
       triangle_wave_encode<12>(cond, tw);
@@ -175,6 +206,24 @@ __global__ void __launch_bounds__(128 * WGS, 1) df_fused_kernel(const __grid_con
     }
     // ---- 6. phi layers and epilogue
     tile::mlp_tail(c, w_phi_hidden, p.hidden_phi, NBP);
+    if constexpr (MODE == kModeTrainFwd) {
+      const float pdf_phi = tile::row_pdf_train<NBP, LINEAR>(c.tmem + c.lane_base, tg[1]);
+      // combine_AR_pdf_and_dl_doutput (train.h:956-963): AutoRegressive takes
+      // |pdf|, pdf() = pt * pp * (1/4pi), times its inverse, + M_EPSILON
+      constexpr float kInv4Pi = 0.0795774715459476678844f;
+      const float li = (tg[2] + tg[3] + tg[4]) / 3.0f;
+      const float wi_pdf = tg[5] + kEps;
+      const float gpdf = fabsf(pdf_theta) * fabsf(pdf_phi) * kInv4Pi * (1.f / kInv4Pi) + kEps;
+      const float prefix = -li / wi_pdf / gpdf * p.loss_scale_per_record;
+      const float lik = -li / wi_pdf * logf(gpdf);
+      if (valid) {
+        const float4 o = record_ok ? make_float4(pdf_theta, pdf_phi, prefix, lik)
+                                   : make_float4(0.f, 0.f, 0.f, 0.f);
+        *reinterpret_cast<float4*>(p.train_out + row * 4) = o;
+        if (!record_ok) atomicAdd(p.n_dropped, 1ull);
+      }
+      continue;
+    }
     const float u_phi_given = MODE == kModeInfer ? wi.y : (valid ? __ldg(p.u_eval + row * 2 + 1) : 0.5f);
     const tile::RowResult rp = tile::row_epilogue<NBP, LINEAR>(
         c.tmem + c.lane_base, MODE == kModeInfer && guided, u_phi_given, u[2], u[3]);
@@ -230,8 +279,9 @@ cudaError_t launch_t(int mode, const DfKernelParams& p, size_t smem, int num_sms
   int64_t ctas = (n_tiles + kDfWarpgroups - 1) / kDfWarpgroups;
   if (ctas > num_sms) ctas = num_sms;
   if (ctas < 1) ctas = 1;
-  auto kern = mode == kModeInfer ? df_fused_kernel<L, F, NBT, NBP, LIN, kModeInfer, kDfWarpgroups>
-                                 : df_fused_kernel<L, F, NBT, NBP, LIN, kModeEval, kDfWarpgroups>;
+  auto kern = mode == kModeInfer  ? df_fused_kernel<L, F, NBT, NBP, LIN, kModeInfer, kDfWarpgroups>
+              : mode == kModeEval ? df_fused_kernel<L, F, NBT, NBP, LIN, kModeEval, kDfWarpgroups>
+                                  : df_fused_kernel<L, F, NBT, NBP, LIN, kModeTrainFwd, kDfWarpgroups>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
   if (e != cudaSuccess) return e;

@@ -14,7 +14,7 @@ namespace gdf {
 constexpr int kDfWarpgroups = 4;
 constexpr int kDfThreads = 128 * kDfWarpgroups;
 
-enum DfMode : int { kModeInfer = 0, kModeEval = 1 };
+enum DfMode : int { kModeInfer = 0, kModeEval = 1, kModeTrainFwd = 2 };
 
 struct DfKernelParams {
   const float* queries;      // n x 9
@@ -32,6 +32,12 @@ struct DfKernelParams {
   uint32_t blob_theta_bytes, blob_phi_bytes;
   int32_t hidden_theta, hidden_phi;  // tcnn n_hidden_layers
   uint32_t* err;                     // device error word
+  // training forward (kModeTrainFwd)
+  const float* in_phi;               // n x 10 GuidedInputPhi
+  const float* target;               // n x 9 GuidedOutput
+  float* train_out;                  // n x 4: pdf_theta, pdf_phi, prefix, likelihood
+  unsigned long long* n_dropped;     // records rejected by the validity filter
+  float loss_scale_per_record;       // TRAIN_LOSS_SCALE / n
   GridLevels gl_theta, gl_phi;
 };
 

@@ -1,0 +1,551 @@
+// df_train.cu -- backward pass and optimizer of the DF training step.
+//
+// df_train_bwd_kernel: one network per launch. Each CTA (one warpgroup, 128
+// records per tile, persistent over tiles):
+//   1. recomputes the forward of its network with every activation kept in
+//      shared memory (tcgen05, fp32 accumulators in TMEM, fp16 activations);
+//   2. builds the fp16 pdf table and dL/dlogits of combine_AR_pdf_and_dl_doutput
+//      (src/render/guided/train.h:932-965, AR.h:51-104) from the per-record
+//      pdf of the other network and the loss prefix computed by the forward
+//      kernel;
+//   3. back-propagates (tcnn/src/fully_fused_mlp.cu:755-850): per layer one
+//      tcgen05 MMA for the data gradient (M=128) and one for the weight
+//      gradient (M=64, operands read MN-major from the same tiles), the
+//      weight gradients accumulating across all of the CTA's tiles in TMEM;
+//   4. scatters dL/dgrid-feature * corner weight into the fp32 grid
+//      gradient with vector atomics (grid.h:395-520; tcnn uses fp16 atomics).
+// At the end each CTA writes its weight-gradient partial sums; the optimizer
+// kernel reduces them in fixed CTA order (deterministic).
+//
+// adam_ema_kernel: Adam (tcnn optimizers/adam.h:48-117) + EMA (ema.h:63-130)
+// over one network, fused with the gradient reduction, the re-zeroing of the
+// grid gradient and the re-layout of the MLP weights for the tensor cores.
+#include <cuda_fp16.h>
+
+#include "../device/df_math.cuh"
+#include "../device/df_tile.cuh"
+#include "../device/sm100.cuh"
+#include "df_kernels.h"
+#include "train_kernels.h"
+
+namespace gdf {
+namespace {
+
+using namespace sm100;
+
+__host__ __device__ constexpr int pad16t(int v) { return (v + 15) / 16 * 16; }
+
+// MMA with arbitrary majors: D (+)= A * B over `ksteps` K=16 steps. a/b
+// descriptors advance by a_step / b_step bytes per step.
+__device__ __forceinline__ void mma_steps(uint32_t d, uint32_t a_s, uint32_t a_lbo, uint32_t a_sbo,
+                                          uint32_t a_step, uint32_t b_s, uint32_t b_lbo,
+                                          uint32_t b_sbo, uint32_t b_step, uint32_t idesc,
+                                          int ksteps, bool accumulate) {
+  for (int s = 0; s < ksteps; ++s) {
+    const uint64_t ad = smem_desc(a_s + s * a_step, a_lbo, a_sbo);
+    const uint64_t bd = smem_desc(b_s + s * b_step, b_lbo, b_sbo);
+    mma_f16_ss(d, ad, bd, idesc, (accumulate || s > 0) ? 1u : 0u);
+  }
+}
+
+// ReLU'(forward activation) * accumulator -> fp16 -> D tile (64 columns).
+__device__ __forceinline__ void dgrad_relu_to_tile(const tile::Wg& c, uint32_t taddr,
+                                                   const uint8_t* h_tile, uint8_t* d_tile) {
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    uint32_t r[32];
+    tmem_ld32(taddr + h * 32, r);
+    tmem_ld_wait();
+#pragma unroll
+    for (int kc = 0; kc < 4; ++kc) {
+      const uint4 hv = *reinterpret_cast<const uint4*>(h_tile + tile::chunk_off(c.row, h * 4 + kc, 64));
+      const __half2* hh = reinterpret_cast<const __half2*>(&hv);
+      __half2 out[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const float2 f = __half22float2(hh[j]);
+        const float a = f.x > 0.f ? __uint_as_float(r[kc * 8 + 2 * j]) : 0.f;
+        const float b = f.y > 0.f ? __uint_as_float(r[kc * 8 + 2 * j + 1]) : 0.f;
+        out[j] = __floats2half2_rn(a, b);
+      }
+      *reinterpret_cast<uint4*>(d_tile + tile::chunk_off(c.row, h * 4 + kc, 64)) =
+          *reinterpret_cast<uint4*>(out);
+    }
+  }
+  tc_fence_before();
+}
+
+__device__ __forceinline__ void relu_to(const tile::Wg& c, uint32_t taddr, uint8_t* dst) {
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    uint32_t r[32];
+    tmem_ld32(taddr + h * 32, r);
+    tmem_ld_wait();
+#pragma unroll
+    for (int kc = 0; kc < 4; ++kc) {
+      __half2 v[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        v[j] = __floats2half2_rn(fmaxf(__uint_as_float(r[kc * 8 + 2 * j]), 0.f),
+                                 fmaxf(__uint_as_float(r[kc * 8 + 2 * j + 1]), 0.f));
+      *reinterpret_cast<uint4*>(dst + tile::chunk_off(c.row, h * 4 + kc, 64)) = *reinterpret_cast<uint4*>(v);
+    }
+  }
+  tc_fence_before();
+}
+
+// dL/dlogits of one row into the D tile (fp16, 64 columns; first NB used).
+// compute_gradients_specialized_linear_interpolation / _nearest (AR.h:51-104).
+template <int NB, bool LINEAR>
+__device__ __noinline__ void dlogits_to_tile(uint32_t taddr, float u, float pdf_other, float prefix,
+                                            bool ok, uint8_t* d_tile, uint32_t row) {
+  float v[NB];
+  if constexpr (NB == 16) {
+    uint32_t r[16];
+    tmem_ld16(taddr, r);
+    tmem_ld_wait();
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+  } else {
+    uint32_t r[NB];
+#pragma unroll
+    for (int c = 0; c < NB / 32; ++c) tmem_ld32(taddr + c * 32, *reinterpret_cast<uint32_t(*)[32]>(r + c * 32));
+    tmem_ld_wait();
+#pragma unroll
+    for (int i = 0; i < NB; ++i) v[i] = __uint_as_float(r[i]);
+  }
+  tc_fence_before();
+  softmax_table_fp16<NB>(v);
+  const float inv_res = 1.0f / static_cast<float>(NB);
+  const float multiplier = prefix * pdf_other * static_cast<float>(NB);
+  int f, cidx;
+  float w;
+  if constexpr (LINEAR) {
+    const float idx = u * static_cast<float>(NB) - 0.5f;
+    f = safe_floor<NB>(idx);
+    cidx = f + 1;
+    w = idx - static_cast<float>(f);
+    if (f < 0) { f = NB - 1; w = 1.0f; }
+    if (cidx > NB - 1) { cidx = 0; w = 0.0f; }
+  } else {
+    f = min(static_cast<int>(u * static_cast<float>(NB)), NB - 1);
+    cidx = f;
+    w = 0.f;
+  }
+  const float p0 = select_bin<NB>(v, f) * inv_res;
+  const float p1 = select_bin<NB>(v, cidx) * inv_res;
+#pragma unroll
+  for (int kc = 0; kc < NB / 8; ++kc) {
+    __half2 out[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      float g[2];
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int i = kc * 8 + 2 * j + e;
+        const float pi = v[i] * inv_res;
+        const float j0 = f == i ? p0 * (1.0f - p0) : -p0 * pi;
+        float jj;
+        if constexpr (LINEAR) {
+          const float j1 = cidx == i ? p1 * (1.0f - p1) : -p1 * pi;
+          jj = (1.0f - w) * j0 + w * j1;
+        } else {
+          jj = j0;
+        }
+        g[e] = ok ? multiplier * jj : 0.f;
+      }
+      out[j] = __floats2half2_rn(g[0], g[1]);
+    }
+    *reinterpret_cast<uint4*>(d_tile + tile::chunk_off(row, kc, 64)) = *reinterpret_cast<uint4*>(out);
+  }
+}
+
+// Grid backward of one row: dX (LF fp32 values in TMEM) scattered into the
+// fp32 gradient table (kernel_grid_backward, grid.h:395-520).
+template <int L, int F>
+__device__ __forceinline__ void grid_backward_row(const GridLevels& g, const float* pos,
+                                                  const float* dx, float* __restrict__ grad) {
+#pragma unroll
+  for (int l = 0; l < L; ++l) {
+    const float scale = g.scale[l];
+    float fr[3];
+    uint32_t pg[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      float pp = fmaf(pos[d], scale, 0.5f);
+      const float t = floorf(pp);
+      pg[d] = static_cast<uint32_t>(static_cast<int>(t));
+      pp -= t;
+      if (g.interp == 1) pp = pp * pp * (3.0f - 2.0f * pp);
+      fr[d] = pp;
+    }
+    float* gl = grad + static_cast<size_t>(g.offset[l]) * F;
+    float dl[F];
+#pragma unroll
+    for (int f = 0; f < F; ++f) dl[f] = dx[l * F + f];
+    if (g.interp == 2) {
+      const uint32_t e = grid_entry(g, l, pg[0], pg[1], pg[2]);
+#pragma unroll
+      for (int f = 0; f < F; ++f) atomicAdd(gl + static_cast<size_t>(e) * F + f, dl[f]);
+      continue;
+    }
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      float w = 1.f;
+      w *= (c & 1) ? fr[0] : 1.f - fr[0];
+      w *= (c & 2) ? fr[1] : 1.f - fr[1];
+      w *= (c & 4) ? fr[2] : 1.f - fr[2];
+      const uint32_t e = grid_entry(g, l, pg[0] + (c & 1), pg[1] + ((c >> 1) & 1), pg[2] + ((c >> 2) & 1));
+      if constexpr (F == 2) {
+        atomicAdd(reinterpret_cast<float2*>(gl) + e, make_float2(w * dl[0], w * dl[1]));
+      } else {
+        atomicAdd(reinterpret_cast<float4*>(gl) + e, make_float4(w * dl[0], w * dl[1], w * dl[2], w * dl[3]));
+      }
+    }
+  }
+}
+
+template <int L, int F, int NB, bool LINEAR, bool PHI>
+__global__ void __launch_bounds__(128, 1) df_train_bwd_kernel(const __grid_constant__ DfBwdParams p) {
+  constexpr int LF = L * F;
+  constexpr int K0 = PHI ? pad16t(LF + 40) : pad16t(LF + 28);
+  extern __shared__ __align__(1024) uint8_t smem[];
+  const uint32_t tid = threadIdx.x;
+  const uint32_t warp = tid >> 5;
+  const int H = p.hidden;
+
+  // shared memory: weights | X tile | H_1..H_H tiles | D tile | barriers
+  const uint32_t off_x = (p.blob_bytes + 127u) & ~127u;
+  constexpr uint32_t kX = 128u * K0 * 2u, kT = 128u * 64u * 2u;
+  const uint32_t off_h = off_x + kX;
+  const uint32_t off_d = off_h + static_cast<uint32_t>(H) * kT;
+  const uint32_t off_bar = off_d + kT;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + off_bar);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + off_bar + 16);
+
+  if (warp == 0) {
+    tmem_alloc(tmem_slot, 512);
+    tmem_relinquish();
+  }
+  if (tid == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    fence_mbar_init();
+    mbar_arrive_expect_tx(&bars[0], p.blob_bytes);
+    for (uint32_t o = 0; o < p.blob_bytes; o += 32768u)
+      bulk_g2s(smem + o, reinterpret_cast<const uint8_t*>(p.blob) + o, min(32768u, p.blob_bytes - o), &bars[0]);
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  mbar_wait(&bars[0], 0, p.err, kErrWeightLoad);
+
+  tile::Wg c;
+  c.tile_a = smem + off_x;
+  c.tile_a_s = smem_addr(c.tile_a);
+  c.tile_p = nullptr;
+  c.tile_p_s = 0;
+  c.tmem = tmem;
+  c.lane_base = (warp * 32u) << 16;
+  c.bar = &bars[1];
+  c.phase = 0;
+  c.bar_id = 1;
+  c.row = tid;
+  c.leader = tid == 0;
+  c.err = p.err;
+  uint8_t* const x_tile = smem + off_x;
+  uint8_t* const d_tile = smem + off_d;
+  const uint32_t x_s = smem_addr(x_tile), d_s = smem_addr(d_tile), h_s0 = smem_addr(smem + off_h);
+  auto h_tile = [&](int l) { return smem + off_h + static_cast<uint32_t>(l - 1) * kT; };  // H_l, l >= 1
+  auto h_addr = [&](int l) { return h_s0 + static_cast<uint32_t>(l - 1) * kT; };
+  const uint32_t w0 = smem_addr(smem);
+  auto w_addr = [&](int l) {  // W_l, l in [0, H]; W_H is the output layer
+    return l == 0 ? w0 : w0 + 64u * K0 * 2u + static_cast<uint32_t>(l - 1) * 64u * 64u * 2u;
+  };
+  // TMEM columns: work [0,64) | dX [64,96) | G_0 [96, 96+K0) | G_l at 192+64(l-1) | G_H^T after
+  const uint32_t t_work = tmem, t_dx = tmem + 64;
+  auto t_g = [&](int l) { return tmem + (l == 0 ? 96u : 192u + 64u * static_cast<uint32_t>(l - 1)); };
+  const uint32_t lane = c.lane_base;
+
+  constexpr uint32_t kIdFwd64 = idesc_f16(128, 64, 0, 0, 0);
+  constexpr uint32_t kIdFwdNB = idesc_f16(128, NB, 0, 0, 0);
+  constexpr uint32_t kIdDgrad = idesc_f16(128, 64, 0, 0, 1);    // B = W^T read MN-major
+  constexpr uint32_t kIdDx = idesc_f16(128, LF, 0, 0, 1);
+  constexpr uint32_t kIdWg64 = idesc_f16(64, 64, 0, 1, 1);      // A, B MN-major
+  constexpr uint32_t kIdWgK0 = idesc_f16(64, K0, 0, 1, 1);
+  constexpr uint32_t kIdWgOut = idesc_f16(64, NB, 0, 1, 1);
+
+  const int64_t n_tiles = (p.n + 127) / 128;
+  bool first = true;
+  for (int64_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+    const int64_t row = t * 128 + c.row;
+    const bool valid = row < p.n;
+    float q[10];
+#pragma unroll
+    for (int i = 0; i < 10; ++i) q[i] = 0.5f;
+    const int ninp = PHI ? 10 : 9;
+    for (int i = 0; i < ninp; ++i) q[i] = valid ? __ldg(p.in + row * p.in_stride + i) : 0.5f;
+    const float4 fw = valid ? *reinterpret_cast<const float4*>(p.fwd + row * 4) : make_float4(0.f, 0.f, 0.f, 0.f);
+    const bool ok = valid && fw.z != 0.f;
+    float u_own = valid ? __ldg(p.target + row * 9 + (PHI ? 1 : 0)) : 0.5f;
+    if (!ok) {
+#pragma unroll
+      for (int i = 0; i < 10; ++i) q[i] = 0.5f;
+      u_own = 0.5f;
+    }
+
+    // ---- forward: X | H_1 .. H_H | logits
+#pragma unroll 1
+    for (int l = 0; l < L; ++l) {
+      float f[F];
+      tile::grid_level<F>(p.gl, l, p.gl.interp, p.grid, q[0], q[1], q[2], f);
+#pragma unroll
+      for (int j = 0; j < F; j += 2) tile::store_h2(x_tile, c.row, l * F + j, K0, f[j], f[j + 1]);
+    }
+    tile::sh_ob_to_tile(q, x_tile, c.row, LF, K0);
+    if constexpr (PHI) {
+      float tw[12];
+      triangle_wave_encode<12>(q[9], tw);
+      tile::store_run(x_tile, c.row, LF + 28, K0, tw, 12);
+      tile::ones_to_tile(x_tile, c.row, LF + 40, K0, K0);
+    } else {
+      tile::ones_to_tile(x_tile, c.row, LF + 28, K0, K0);
+    }
+    for (int l = 0; l <= H; ++l) {
+      tile::publish(c);
+      if (c.leader) {
+        tc_fence_after();
+        const uint32_t a_s = l == 0 ? x_s : h_addr(l);
+        const uint32_t ka = l == 0 ? K0 : 64u;
+        mma_steps(t_work, a_s, 128, ka * 16u, 256, w_addr(l), 128, ka * 16u, 256,
+                  l == H ? kIdFwdNB : kIdFwd64, static_cast<int>(ka / 16), false);
+        mma_commit(c.bar);
+      }
+      tile::wait_mma(c);
+      if (l < H) relu_to(c, t_work + lane, h_tile(l + 1));
+    }
+    // ---- dL/dlogits -> D tile
+    dlogits_to_tile<NB, LINEAR>(t_work + lane, u_own, fabsf(PHI ? fw.x : fw.y), fw.z, ok, d_tile, c.row);
+
+    // ---- backward: output layer, hidden layers, first layer
+    for (int l = H; l >= 0; --l) {
+      tile::publish(c);
+      if (c.leader) {
+        tc_fence_after();
+        const bool acc = !first;
+        if (l == H) {
+          // G_H^T (i x o) += H_H^T D: A = H_H, B = D, both MN-major, K = 128 rows
+          mma_steps(t_g(H), h_addr(H), 64u * 16u, 128, 2u * 64u * 16u, d_s, 64u * 16u, 128,
+                    2u * 64u * 16u, kIdWgOut, 8, acc);
+          // work = D W_H: A = D K-major (K = NB), B = W_H MN-major
+          mma_steps(t_work, d_s, 128, 64u * 16u, 256, w_addr(H), 64u * 16u, 128, 2u * 64u * 16u,
+                    kIdDgrad, NB / 16, false);
+        } else if (l > 0) {
+          // G_l (o x i) += D^T H_l
+          mma_steps(t_g(l), d_s, 64u * 16u, 128, 2u * 64u * 16u, h_addr(l), 64u * 16u, 128,
+                    2u * 64u * 16u, kIdWg64, 8, acc);
+          mma_steps(t_work, d_s, 128, 64u * 16u, 256, w_addr(l), 64u * 16u, 128, 2u * 64u * 16u,
+                    kIdDgrad, 4, false);
+        } else {
+          // G_0 (o x K0) += D^T X ; dX = D W_0[:, :LF]
+          mma_steps(t_g(0), d_s, 64u * 16u, 128, 2u * 64u * 16u, x_s, K0 * 16u, 128, 2u * K0 * 16u,
+                    kIdWgK0, 8, acc);
+          mma_steps(t_dx, d_s, 128, 64u * 16u, 256, w_addr(0), K0 * 16u, 128, 2u * K0 * 16u, kIdDx, 4,
+                    false);
+        }
+        mma_commit(c.bar);
+      }
+      tile::wait_mma(c);
+      if (l > 0) dgrad_relu_to_tile(c, t_work + lane, h_tile(l), d_tile);
+    }
+    // ---- grid backward
+    {
+      float dx[LF];
+      if constexpr (LF == 16) {
+        uint32_t r[16];
+        tmem_ld16(t_dx + lane, r);
+        tmem_ld_wait();
+#pragma unroll
+        for (int i = 0; i < 16; ++i) dx[i] = __uint_as_float(r[i]);
+      } else {
+        uint32_t r[32];
+        tmem_ld32(t_dx + lane, r);
+        tmem_ld_wait();
+#pragma unroll
+        for (int i = 0; i < 32; ++i) dx[i] = __uint_as_float(r[i]);
+      }
+      tc_fence_before();
+      if (ok) grid_backward_row<L, F>(p.gl, q, dx, p.grid_grad);
+    }
+    first = false;
+  }
+
+  // ---- weight-gradient partials of this CTA (zeros if it had no tile)
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  float* part = p.wgrad_partial + static_cast<size_t>(blockIdx.x) * p.n_mlp;
+  // M=64 accumulators: warp q holds rows 16q + t in its lanes t < 16
+  const uint32_t mrow = warp * 16u + (tid & 31u);
+  const bool mvalid = (tid & 31u) < 16u;
+  for (int l = 0; l <= H; ++l) {
+    const int ncols = l == 0 ? K0 : (l == H ? NB : 64);
+    const size_t base = l == 0 ? 0 : static_cast<size_t>(64) * K0 + static_cast<size_t>(l - 1) * 64 * 64;
+    for (int c0 = 0; c0 < ncols; c0 += 16) {
+      uint32_t r[16];
+      tmem_ld16(t_g(l) + lane + c0, r);
+      tmem_ld_wait();
+      if (mvalid) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const float v = first ? 0.f : __uint_as_float(r[j]);
+          if (l == H) part[base + static_cast<size_t>(c0 + j) * 64 + mrow] = v;  // G_H stored transposed
+          else part[base + static_cast<size_t>(mrow) * ncols + c0 + j] = v;
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0) tmem_dealloc(tmem, 512);
+}
+
+template <int L, int F, int NB, bool LIN, bool PHI>
+cudaError_t launch_bwd_t(const DfBwdParams& p, int ctas, cudaStream_t st) {
+  constexpr int LF = L * F;
+  constexpr int K0 = PHI ? pad16t(LF + 40) : pad16t(LF + 28);
+  const size_t smem = ((p.blob_bytes + 127u) & ~127u) + 128u * K0 * 2u +
+                      static_cast<size_t>(p.hidden + 1) * 128u * 64u * 2u + 64u;
+  auto k = df_train_bwd_kernel<L, F, NB, LIN, PHI>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  k<<<ctas, 128, smem, st>>>(p);
+  return cudaGetLastError();
+}
+
+// ----------------------------------------------------------------- Adam
+__global__ void adam_ema_kernel(const __grid_constant__ AdamParams p) {
+  double local_sq = 0.0;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < p.n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    float graw;
+    if (i < p.n_mlp) {
+      float s = 0.f;
+      for (int cta = 0; cta < p.n_partials; ++cta) s += p.partials[static_cast<size_t>(cta) * p.n_mlp + i];
+      graw = s;
+    } else {
+      graw = p.grid_grad[i - p.n_mlp];
+      p.grid_grad[i - p.n_mlp] = 0.f;
+    }
+    float g = graw / p.loss_scale;
+    local_sq += static_cast<double>(g) * g;
+    const bool skip = i >= p.n_mlp && g == 0.0f;
+    float w16;
+    if (!skip) {
+      const float wf = p.master[i];
+      if (i < p.n_mlp) g += p.l2_reg * wf;
+      const float m1 = p.m[i] = p.beta1 * p.m[i] + (1 - p.beta1) * g;
+      const float m2 = p.v[i] = p.beta2 * p.v[i] + (1 - p.beta2) * (g * g);
+      const uint32_t cs = ++p.step[i];
+      const float lr = p.lr * sqrtf(1 - powf(p.beta2, static_cast<float>(cs))) /
+                       (1 - powf(p.beta1, static_cast<float>(cs)));
+      const float eff = fminf(fmaxf(lr / (sqrtf(m2) + p.eps), 0.0f), 3.402823466e38f);
+      const float nw = wf - eff * m1;
+      p.master[i] = nw;
+      const __half h = __float2half_rn(nw);
+      p.w16[i] = h;
+      w16 = __half2float(h);
+    } else {
+      w16 = __half2float(p.w16[i]);
+    }
+    const __half e = __float2half_rn((__half2float(p.ema16[i]) * p.ema_decay * p.debias_old +
+                                      w16 * (1 - p.ema_decay)) * p.debias_new);
+    p.ema16[i] = e;
+    if (i < p.n_mlp) {
+      // re-layout for the tensor cores (canonical K-major per matrix)
+      int l = 0;
+      while (l + 1 < p.n_layers && i >= p.layer_off[l + 1]) ++l;
+      const uint32_t k = static_cast<uint32_t>(i - p.layer_off[l]);
+      const uint32_t cols = static_cast<uint32_t>(p.layer_cols[l]);
+      const uint32_t off = static_cast<uint32_t>(p.layer_off[l]) + canon_offset(k / cols, k % cols, cols);
+      p.blob_w16[off] = __float2half_rn(w16);
+      p.blob_ema[off] = e;
+    }
+  }
+  // per-block sum of squared gradients (FP64), reduced by the host-side kernel
+  __shared__ double red[256];
+  red[threadIdx.x] = local_sq;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) p.sq_partial[blockIdx.x] = red[0];
+}
+
+// Deterministic FP64 reductions: loss = sum(likelihood) (column 3 of the
+// forward output), grad_norm^2 = sum of the optimizer's block partials.
+__global__ void train_stats_kernel(const float* __restrict__ fwd, int64_t n, const double* __restrict__ sq,
+                                   int n_sq, double* out) {
+  __shared__ double red[1024];
+  double a = 0.0;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) a += fwd[i * 4 + 3];
+  red[threadIdx.x] = a;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[0] = red[0];
+  __syncthreads();
+  double b = 0.0;
+  for (int i = threadIdx.x; i < n_sq; i += blockDim.x) b += sq[i];
+  red[threadIdx.x] = b;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[1] = red[0];
+}
+
+}  // namespace
+
+cudaError_t launch_df_train_bwd(const DfShape& s, bool phi, const DfBwdParams& p, int ctas,
+                                cudaStream_t st) {
+  if (p.n <= 0) return cudaSuccess;
+#define GDF_BWD(L, F, NBT, NBP)                                                                 \
+  if (s.levels == L && s.features == F && s.bins_theta == NBT && s.bins_phi == NBP) {           \
+    if (phi) return s.linear ? launch_bwd_t<L, F, NBP, true, true>(p, ctas, st)                 \
+                             : launch_bwd_t<L, F, NBP, false, true>(p, ctas, st);               \
+    return s.linear ? launch_bwd_t<L, F, NBT, true, false>(p, ctas, st)                         \
+                    : launch_bwd_t<L, F, NBT, false, false>(p, ctas, st);                       \
+  }
+  GDF_BWD(8, 2, 32, 32)
+  GDF_BWD(16, 2, 64, 64)
+  GDF_BWD(8, 4, 16, 32)
+#undef GDF_BWD
+  return cudaErrorNotSupported;
+}
+
+size_t df_train_bwd_smem_bytes(int levels, int features, bool phi, uint32_t blob_bytes, int hidden) {
+  const int lf = levels * features;
+  const int k0 = phi ? pad16t(lf + 40) : pad16t(lf + 28);
+  return ((blob_bytes + 127u) & ~127u) + 128u * k0 * 2u + static_cast<size_t>(hidden + 1) * 128u * 64u * 2u + 64u;
+}
+
+cudaError_t launch_adam_ema(const AdamParams& p, cudaStream_t st) {
+  if (p.n <= 0) return cudaSuccess;
+  adam_ema_kernel<<<p.n_blocks, 256, 0, st>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_train_stats(const float* fwd, int64_t n, const double* sq, int n_sq, double* out,
+                               cudaStream_t st) {
+  train_stats_kernel<<<1, 1024, 0, st>>>(fwd, n, sq, n_sq, out);
+  return cudaGetLastError();
+}
+
+}  // namespace gdf

@@ -1,0 +1,60 @@
+// train_kernels.h -- host-side declarations of the training kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include "../device/grid_levels.h"
+#include "df_kernels.h"
+
+namespace gdf {
+
+// Backward of one DF network over a batch.
+struct DfBwdParams {
+  const float* in;          // records of this network (stride in_stride)
+  int32_t in_stride;        // 9 (theta) or 10 (phi)
+  const float* target;      // n x 9 GuidedOutput
+  const float* fwd;         // n x 4 from the training forward: pdf_theta, pdf_phi, prefix, likelihood
+  int64_t n;
+  const __half* blob;       // fp16 training weights, canonical layout
+  uint32_t blob_bytes;
+  const __half* grid;       // fp16 training grid tables
+  float* grid_grad;         // fp32 gradient of the grid tables (zeroed by the optimizer)
+  float* wgrad_partial;     // [gridDim.x][n_mlp] per-CTA weight-gradient sums
+  int64_t n_mlp;
+  int32_t hidden;           // tcnn n_hidden_layers
+  uint32_t* err;
+  GridLevels gl;
+};
+
+// Adam + EMA over one network (tcnn optimizers/adam.h, ema.h).
+struct AdamParams {
+  int64_t n, n_mlp;
+  const float* partials;    // [n_partials][n_mlp]
+  int32_t n_partials;
+  float* grid_grad;         // [n - n_mlp], read then zeroed
+  float* master;
+  __half* w16;
+  __half* ema16;
+  float* m;
+  float* v;
+  uint32_t* step;
+  __half* blob_w16;
+  __half* blob_ema;
+  int64_t layer_off[12];
+  int32_t layer_cols[12];
+  int32_t n_layers;
+  float loss_scale, lr, beta1, beta2, eps, l2_reg, ema_decay, debias_old, debias_new;
+  double* sq_partial;       // [n_blocks]
+  int32_t n_blocks;
+};
+
+cudaError_t launch_df_train_bwd(const DfShape& s, bool phi, const DfBwdParams& p, int ctas,
+                                cudaStream_t st);
+size_t df_train_bwd_smem_bytes(int levels, int features, bool phi, uint32_t blob_bytes, int hidden);
+cudaError_t launch_adam_ema(const AdamParams& p, cudaStream_t st);
+cudaError_t launch_train_stats(const float* fwd, int64_t n, const double* sq, int n_sq, double* out,
+                               cudaStream_t st);
+
+}  // namespace gdf

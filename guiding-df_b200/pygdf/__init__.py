@@ -87,6 +87,8 @@ def lib() -> C.CDLL:
             "gdf_nrc_query": [P, P, P, C.c_int64, P],
             "gdf_nrc_train_step": [P, P, P, C.c_int64, C.POINTER(TrainStats), P],
             "gdf_sync_status": [P, P],
+            "gdf_get_optimizer_state": [P, C.c_int32, P, P, P, C.c_int64, P],
+            "gdf_set_optimizer_state": [P, C.c_int32, P, P, P, C.c_int64, C.c_uint32],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -211,6 +213,25 @@ class Context:
         check(lib().gdf_nrc_train_step(self.h, _ptr(inp), _ptr(target), n,
                                        C.byref(st) if stats else None, _stream(stream)))
         return st
+
+    def get_optimizer_state(self, net: int):
+        import numpy as np
+        n = self.n_params(net)
+        m = np.empty(n, np.float32)
+        v = np.empty(n, np.float32)
+        st = np.empty(n, np.uint32)
+        step = C.c_uint32()
+        check(lib().gdf_get_optimizer_state(self.h, net, m.ctypes.data, v.ctypes.data, st.ctypes.data, n,
+                                            C.byref(step)))
+        return m, v, st, step.value
+
+    def set_optimizer_state(self, net: int, m, v, steps, opt_step: int):
+        import numpy as np
+        m = np.ascontiguousarray(m, np.float32)
+        v = np.ascontiguousarray(v, np.float32)
+        s = np.ascontiguousarray(steps, np.uint32)
+        check(lib().gdf_set_optimizer_state(self.h, net, m.ctypes.data, v.ctypes.data, s.ctypes.data, m.size,
+                                            opt_step))
 
     def sync(self, stream=None):
         check(lib().gdf_sync_status(self.h, _stream(stream)))

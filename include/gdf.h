@@ -219,6 +219,17 @@ gdf_status gdf_train_step(gdf_ctx* ctx, const float* in_theta_dev, const float* 
                           const float* target_dev, int64_t n, gdf_train_stats* stats_host,
                           void* stream);
 
+/* Optimizer state of one network (Adam first/second moments, per-parameter
+ * step counters, optimizer step) for exact resume. The reference saves only
+ * the fp32 weights (learnedDistribution.cpp:295-384); tcnn keeps these in
+ * AdamOptimizer (optimizers/adam.h:250-290). Any output pointer may be NULL.
+ * Synchronises. */
+gdf_status gdf_get_optimizer_state(const gdf_ctx* ctx, int32_t net, float* m_host, float* v_host,
+                                   uint32_t* steps_host, int64_t n, uint32_t* opt_step);
+gdf_status gdf_set_optimizer_state(gdf_ctx* ctx, int32_t net, const float* m_host,
+                                   const float* v_host, const uint32_t* steps_host, int64_t n,
+                                   uint32_t opt_step);
+
 /* -------------------------------------------------------------------- NRC */
 
 /* NRC::inferenceStep (nrc.cpp:172-181): in [m x 15] fp32 (GuidedInputNRC,

@@ -90,6 +90,11 @@ def lib():
             ("go_round_f16", [C.c_double], C.c_float),
             ("go_df_pdf_tables", [C.POINTER(DfCfg), P, P, P, P, P, P, C.c_int64], None),
             ("go_set_accumulation", [C.c_int], None),
+            ("go_df_train_grads", [C.POINTER(DfCfg), P, P, P, P, P, C.c_int64, C.c_float, P, P, P, P, P, P],
+             C.c_int64),
+            ("go_nrc_train_grads", [C.POINTER(NrcCfg), P, P, P, C.c_int64, C.c_float, P, P], None),
+            ("go_adam_ema", [C.c_int64, C.c_int64, P, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float,
+                             C.c_float, C.c_float, C.c_uint32, P, P, P, P, P, P], None),
             ("go_grid_encode", [C.POINTER(Grid), P, P, P], None),
         ]:
             f = getattr(L, name)
@@ -271,3 +276,36 @@ def pdf_tables(d: DfCfg, p_theta, p_phi, queries, u_theta):
     b = np.empty((n, d.n_bins_phi), dtype=np.float32)
     lib().go_df_pdf_tables(C.byref(d), _p(pt), _p(pp), _p(q), _p(ut), _p(a), _p(b), n)
     return a, b
+
+
+def df_train_grads(d: DfCfg, w_theta, w_phi, in_theta, in_phi, target, loss_scale=1024.0):
+    """Gradients (scaled by loss_scale, FP64) of one DF training batch; the
+    weights are the fp32 masters, rounded here to the fp16 training copies."""
+    wt, wp = round_f16(w_theta), round_f16(w_phi)
+    a, b, t = f32(in_theta), f32(in_phi), f32(target)
+    n = a.shape[0]
+    gt = np.zeros(wt.size, np.float64)
+    gp = np.zeros(wp.size, np.float64)
+    lik = np.empty(n, np.float32)
+    pdf = np.empty((n, 2), np.float32)
+    dlt = np.empty((n, d.n_bins_theta), np.float32)
+    dlp = np.empty((n, d.n_bins_phi), np.float32)
+    dropped = lib().go_df_train_grads(C.byref(d), _p(wt), _p(wp), _p(a), _p(b), _p(t), n, loss_scale,
+                                      _p(gt), _p(gp), _p(lik), _p(pdf), _p(dlt), _p(dlp))
+    return dict(grad_theta=gt, grad_phi=gp, likelihood=lik, pdf=pdf, dlog_theta=dlt, dlog_phi=dlp,
+                dropped=int(dropped))
+
+
+def adam_ema(grad_scaled, n_matrix, loss_scale, adam, step, master, ema16, m, v, steps):
+    """One Adam + EMA step (adam.h / ema.h); returns updated copies."""
+    master = f32(master).copy()
+    w16 = round_f16(master)
+    ema = f32(ema16).copy()
+    m = f32(m).copy()
+    v = f32(v).copy()
+    steps = np.ascontiguousarray(steps, np.uint32).copy()
+    g = np.ascontiguousarray(grad_scaled, np.float64)
+    lib().go_adam_ema(master.size, n_matrix, _p(g), loss_scale, adam.learning_rate, adam.beta1, adam.beta2,
+                      adam.epsilon, adam.l2_reg, adam.ema_decay, step, _p(master), _p(w16), _p(ema), _p(m),
+                      _p(v), _p(steps))
+    return master, w16, ema, m, v, steps
