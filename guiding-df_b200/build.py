@@ -28,6 +28,7 @@ COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-I", os.path
 SOURCES = [
     ("kernels/df_fused.cu", ["-fmad=false"]),
     ("kernels/df_train.cu", ["-fmad=false"]),
+    ("kernels/loss_static.cu", []),
     ("host/api.cpp", []),
 ]
 

@@ -270,6 +270,8 @@ gdf_status check_ptr(const void* p, const char* name) {
 
 namespace gdf {
 
+void set_last_error(const char* msg) { g_last_error = msg; }
+
 bool build_grid_levels(const gdf_grid_config& c, GridLevels* gl, int64_t* n_params) {
   std::memset(gl, 0, sizeof(*gl));
   if (c.n_levels > 24) return false;
@@ -312,10 +314,6 @@ bool build_grid_levels(const gdf_grid_config& c, GridLevels* gl, int64_t* n_para
 }
 
 }  // namespace gdf
-
-struct gdf_ctx {
-  Context c;
-};
 
 extern "C" {
 

@@ -58,7 +58,15 @@ struct Context {
   TrainWorkspace ws;
 };
 
+// Sets the thread-local message returned by gdf_last_error().
+void set_last_error(const char* msg);
+
 // Grid level tables (tcnn encodings/grid.h:967-1012, grid_index :165-188).
 bool build_grid_levels(const gdf_grid_config& c, GridLevels* gl, int64_t* n_params);
 
 }  // namespace gdf
+
+// The opaque handle of the C ABI.
+struct gdf_ctx {
+  gdf::Context c;
+};

@@ -89,6 +89,7 @@ def lib() -> C.CDLL:
             "gdf_sync_status": [P, P],
             "gdf_get_optimizer_state": [P, C.c_int32, P, P, P, C.c_int64, P],
             "gdf_set_optimizer_state": [P, C.c_int32, P, P, P, C.c_int64, C.c_uint32],
+            "gdf_train_loss_static": [P, P, P, P, C.c_int64, P, P, P],
         }
         for name, args in sig.items():
             f = getattr(L, name)

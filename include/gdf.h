@@ -230,6 +230,25 @@ gdf_status gdf_set_optimizer_state(gdf_ctx* ctx, int32_t net, const float* m_hos
                                    const float* v_host, const uint32_t* steps_host, int64_t n,
                                    uint32_t opt_step);
 
+/* Mean divergence loss of a batch, like the loss gdf_train_step reports
+ * (same forward kernel, same FP64 reduction), without updating anything
+ * and without allocating: every intermediate lives in a fixed array that is
+ * part of the library image, for callers that cannot allocate device memory
+ * while they run (a renderer with a fixed arena, a host that forbids
+ * cudaMalloc after start-up). No counterpart in the reference.
+ *   - n <= 65536 records (the array's capacity, 1 MiB + 256 B held on every
+ *     GPU that loads the library until exit); larger n -> GDF_ERR_INVALID_ARG;
+ *   - loss_out_dev: one double (mean loss), dropped_out_dev: one int64
+ *     (records rejected by the validity filter), both device pointers;
+ *   - the first call on a device looks up the array's device address
+ *     (cudaGetSymbolAddress); make that first call before any stream
+ *     capture;
+ *   - all calls share the one array: calls whose work overlaps on the GPU
+ *     (other streams, other threads) race; order them on one stream. */
+gdf_status gdf_train_loss_static(gdf_ctx* ctx, const float* in_theta_dev, const float* in_phi_dev,
+                                 const float* target_dev, int64_t n, double* loss_out_dev,
+                                 int64_t* dropped_out_dev, void* stream);
+
 /* -------------------------------------------------------------------- NRC */
 
 /* NRC::inferenceStep (nrc.cpp:172-181): in [m x 15] fp32 (GuidedInputNRC,
