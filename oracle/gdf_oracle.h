@@ -8,6 +8,11 @@
  * Every function cites the reference file:line it restates. Paths are
  * relative to the guiding-df project root; `tcnn/` = src/ext/tcnn.
  *
+ * Pinning. tests/test_reference_pin.py checks the DF epilogue and training
+ * restatements bit for bit against the reference's own train.h / AR.h
+ * compiled for the host (oracle/build_ref.py -> oracle/_ref/); the encodings
+ * and MLP against analytic identities (tests/test_oracle.py).
+ *
  * Precision model. The checker computes in FP64 with fp16 rounding at the
  * storage points the product kernels use (fp16 parameters, fp16 encoded
  * inputs, fp16 hidden activations, fp32 logits). The DF epilogue

@@ -74,6 +74,33 @@ static void dlogits(const float* table, int n, int linear, float u, float pdf_ot
   }
 }
 
+/* Exported for the reference pin: dL/dlogits of one row from a pdf table. */
+void go_dlogits(const float* table, int n, int linear, float u, float pdf_other, float prefix, float* out) {
+  dlogits(table, n, linear, u, pdf_other, prefix, out);
+}
+
+/* combine_AR_pdf_and_dl_doutput (train.h:932-965) on given fp16 pdf tables
+ * (values as float): likelihood and fp16 dL/dlogits of both networks. */
+void go_combine(const float* target, int64_t n, const float* tab_theta, int nbt, const float* tab_phi,
+                int nbp, int linear, float loss_scale, float* dl_theta, float* dl_phi, float* likelihood) {
+  const float scale = loss_scale / (float)n;
+  for (int64_t i = 0; i < n; ++i) {
+    const float* tg = target + i * 9;
+    const float* tt = tab_theta + i * nbt;
+    const float* tp = tab_phi + i * nbp;
+    const float pt = go_sample_pdf(tt, tg[0], nbt, linear);
+    const float pp = go_sample_pdf(tp, tg[1], nbp, linear);
+    const float li = (tg[2] + tg[3] + tg[4]) / 3.0f;
+    const float wi_pdf = tg[5] + GO_EPS;
+    const float pdf_tr = GO_INV_4PI;
+    const float guided = fabsf(pt) * fabsf(pp) * pdf_tr * (1.f / pdf_tr) + GO_EPS;
+    const float prefix = -li / wi_pdf / guided * scale;
+    likelihood[i] = -li / wi_pdf * logf(guided);
+    dlogits(tt, nbt, linear, tg[0], fabsf(pp), prefix, dl_theta + i * nbt);
+    dlogits(tp, nbp, linear, tg[1], fabsf(pt), prefix, dl_phi + i * nbp);
+  }
+}
+
 static int finite_row(const float* a, int n) {
   for (int i = 0; i < n; ++i)
     if (isnan(a[i])) return 0;

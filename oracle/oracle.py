@@ -92,6 +92,9 @@ def lib():
             ("go_set_accumulation", [C.c_int], None),
             ("go_df_train_grads", [C.POINTER(DfCfg), P, P, P, P, P, C.c_int64, C.c_float, P, P, P, P, P, P],
              C.c_int64),
+            ("go_dlogits", [P, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float, P], None),
+            ("go_combine", [P, C.c_int64, P, C.c_int, P, C.c_int, C.c_int, C.c_float, P, P, P], None),
+            ("go_theta_condition", [C.c_float, C.c_int, C.c_int], C.c_float),
             ("go_nrc_train_grads", [C.POINTER(NrcCfg), P, P, P, C.c_int64, C.c_float, P, P], None),
             ("go_adam_ema", [C.c_int64, C.c_int64, P, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float,
                              C.c_float, C.c_float, C.c_uint32, P, P, P, P, P, P], None),
@@ -309,3 +312,35 @@ def adam_ema(grad_scaled, n_matrix, loss_scale, adam, step, master, ema16, m, v,
                       adam.epsilon, adam.l2_reg, adam.ema_decay, step, _p(master), _p(w16), _p(ema), _p(m),
                       _p(v), _p(steps))
     return master, w16, ema, m, v, steps
+
+
+REF_SO = os.path.join(HERE, "_ref", "libgdf_refpin.so")
+_ref = None
+
+
+def ref_lib():
+    """The reference's own DF functions compiled for the host (oracle/_ref),
+    or None when they could not be built (no reference tree)."""
+    global _ref
+    if _ref is None:
+        import importlib.util
+        spec = importlib.util.spec_from_file_location("build_ref", os.path.join(HERE, "build_ref.py"))
+        m = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(m)
+        so = m.build()
+        if not so or not os.path.exists(so):
+            return None
+        L = C.CDLL(so)
+        for name, args, res in [
+            ("ref_softmax_times_n", [P, C.c_int], C.c_int),
+            ("ref_sample_dir", [P, C.c_int, C.c_int, C.c_float, C.c_float], C.c_float),
+            ("ref_sample_pdf", [P, C.c_float, C.c_int, C.c_int], C.c_float),
+            ("ref_theta_condition16", [C.c_float], C.c_float),
+            ("ref_grads_linear", [C.c_float, C.c_float, C.c_float, P, C.c_int, C.c_int, P], C.c_int),
+            ("ref_combine", [P, C.c_int64, P, P, P, P, P, C.c_float], None),
+        ]:
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = res
+        _ref = L
+    return _ref

@@ -88,7 +88,8 @@ def test_sampling_float_matches_double_twin(linear):
         pdf = O.softmax_times_n(rng.normal(0, 2, n))
         u, u2 = rng.random(2)
         _, d, gap = O.sample_dir(pdf, linear, float(u), float(u2))
-        dd = O.lib().go_sample_dir_f64(O._p(O.f32(pdf)), n, int(linear), float(np.float32(u)),
+        pdf32 = O.f32(pdf)  # alive across the call
+        dd = O.lib().go_sample_dir_f64(O._p(pdf32), n, int(linear), float(np.float32(u)),
                                         float(np.float32(u2)))
         if gap > 1e-5:
             worst = max(worst, abs(d - dd))
