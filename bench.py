@@ -41,6 +41,10 @@ FLOP_PER_QUERY = {  # 2 * sum(fan_in * fan_out), unpadded encoded widths, theta 
     "small": 2 * ((44 * 64 + 2 * 64 * 64 + 64 * 32) + (56 * 64 + 2 * 64 * 64 + 64 * 32)),
 }
 N_QUERIES = {"full": 1920 * 1080, "small": 65536}
+TRAIN_BATCH = {"full": 262144, "small": 65536}
+# training flops per record: forward + data gradient + weight gradient of
+# both networks (3x the forward), plus the forward recomputed by the backward
+TRAIN_FLOP_PER_RECORD = {k: 4 * v for k, v in FLOP_PER_QUERY.items()}
 METRIC = "guided queries/s"
 
 
@@ -264,15 +268,33 @@ def main():
         e.synchronize()
         if i >= args.warmup:
             e2e_times.append(s.elapsed_time(e))
+    # ---- training step (gdf_train_step on one batch of synthetic records)
+    nb = TRAIN_BATCH[args.workload]
+    ta, tb, tt = W.training_batch(nb, 77 + rank, cfg.n_bins_theta)
+    da, db, dt = (torch.from_numpy(x).to(dev) for x in (ta, tb, tt))
+    for _ in range(args.warmup):
+        ctx.train_step(da, db, dt, stream=stream, stats=False)
+    torch.cuda.synchronize()
+    train_times = []
+    for i in range(args.steps):
+        flush.zero_()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        ctx.train_step(da, db, dt, stream=stream, stats=False)
+        e.record(stream)
+        e.synchronize()
+        train_times.append(s.elapsed_time(e))
+    last = ctx.train_step(da, db, dt, stream=stream, stats=True)
     clk = clocks.stop()
     ctx.sync(stream)
 
     ms = statistics.mean(times)
     ms_e2e = statistics.mean(e2e_times) if e2e_times else float("nan")
+    ms_train = statistics.mean(train_times)
     if dist:
-        t = torch.tensor([ms, ms_e2e], dtype=torch.float64, device=dev)
+        t = torch.tensor([ms, ms_e2e, ms_train], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, ms_e2e = float(t[0]), float(t[1])
+        ms, ms_e2e, ms_train = float(t[0]), float(t[1]), float(t[2])
     value = n * world / (ms * 1e-3)
     e2e_value = n * world / (ms_e2e * 1e-3)
     h2d = q_h.nbytes + wi_h.nbytes + guided_h.nbytes
@@ -304,6 +326,10 @@ def main():
                          "flop_per_query": FLOP_PER_QUERY[args.workload]},
             "cpu_baseline": {"value": cpu_v, "unit": "queries/s", "cores": threads, "kind": "port",
                              "sample": f"{cpu_n} queries ({cpu_s:.1f} s) of the same workload"},
+            "train": {"metric": "train samples/s", "value": nb * world / (ms_train * 1e-3),
+                      "unit": "records/s", "batch": nb, "ms_per_step": ms_train,
+                      "achieved_tflops": TRAIN_FLOP_PER_RECORD[args.workload] * nb / (ms_train * 1e-3) / 1e12,
+                      "loss": last.loss, "launches_per_step": 6},
             "clocks": clk,
             "gpu_launches": args.steps,
         }

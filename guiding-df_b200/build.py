@@ -29,6 +29,7 @@ SOURCES = [
     ("kernels/df_fused.cu", ["-fmad=false"]),
     ("kernels/df_train.cu", ["-fmad=false"]),
     ("kernels/loss_static.cu", []),
+    ("kernels/nrc.cu", ["-fmad=false"]),
     ("host/api.cpp", []),
 ]
 

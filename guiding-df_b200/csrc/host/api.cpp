@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "../kernels/df_kernels.h"
+#include "../kernels/nrc_kernels.h"
 #include "../kernels/train_kernels.h"
 #include "context.h"
 
@@ -748,12 +749,76 @@ gdf_status gdf_set_optimizer_state(gdf_ctx* ctx, int32_t net, const float* m, co
   return GDF_OK;
 }
 
-gdf_status gdf_nrc_query(gdf_ctx*, const float*, float*, int64_t, void*) {
-  return fail(GDF_ERR_UNSUPPORTED, "gdf_nrc_query: not built yet");
+gdf_status gdf_nrc_query(gdf_ctx* ctx, const float* in, float* out, int64_t m, void* stream) {
+  if (!ctx) return fail(GDF_ERR_INVALID_ARG, "ctx is null");
+  Context& c = ctx->c;
+  if (!c.net[2].present) return fail(GDF_ERR_STATE, "NRC is disabled in this context");
+  if (m < 0) return fail(GDF_ERR_INVALID_ARG, "m < 0");
+  if (m == 0) return GDF_OK;
+  gdf_status s;
+  if ((s = check_ptr(in, "in")) || (s = check_ptr(out, "out"))) return s;
+  gdf::NrcParams p;
+  std::memset(&p, 0, sizeof(p));
+  p.in = in;
+  p.out = out;
+  p.n = m;
+  p.blob = c.net[2].blob_ema;
+  p.blob_bytes = c.net[2].blob_bytes;
+  p.hidden = c.net[2].hidden;
+  p.err = c.d_err;
+  cudaError_t e = gdf::launch_nrc_query(p, c.num_sms, static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cuda_fail(e, "nrc_query");
+  return GDF_OK;
 }
 
-gdf_status gdf_nrc_train_step(gdf_ctx*, const float*, const float*, int64_t, gdf_train_stats*, void*) {
-  return fail(GDF_ERR_UNSUPPORTED, "gdf_nrc_train_step: not built yet");
+gdf_status gdf_nrc_train_step(gdf_ctx* ctx, const float* in, const float* target, int64_t m,
+                              gdf_train_stats* stats, void* stream) {
+  if (!ctx) return fail(GDF_ERR_INVALID_ARG, "ctx is null");
+  Context& c = ctx->c;
+  if (!c.net[2].present) return fail(GDF_ERR_STATE, "NRC is disabled in this context");
+  if (m <= 0) return fail(GDF_ERR_INVALID_ARG, "m must be positive");
+  if (m > c.ws.capacity) return fail(GDF_ERR_INVALID_ARG, "m exceeds max_train_batch");
+  gdf_status s;
+  if ((s = check_ptr(in, "in")) || (s = check_ptr(target, "target"))) return s;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  Net& n = c.net[2];
+  GDF_CUDA(cudaMemsetAsync(c.ws.dropped, 0, sizeof(unsigned long long), st));
+  gdf::NrcTrainParams p;
+  std::memset(&p, 0, sizeof(p));
+  p.in = in;
+  p.target = target;
+  p.n = m;
+  p.blob = n.blob_w16;
+  p.blob_bytes = n.blob_bytes;
+  p.hidden = n.hidden;
+  p.wgrad_partial = c.ws.partial[2];
+  p.n_mlp = n.n_mlp;
+  p.loss_scale = c.cfg.nrc_loss_scale;
+  p.n_total = static_cast<float>(m * 3);
+  p.loss_out = c.ws.fwd;
+  p.n_dropped = c.ws.dropped;
+  p.err = c.d_err;
+  cudaError_t e = gdf::launch_nrc_train_bwd(p, c.num_sms, st);
+  if (e != cudaSuccess) return cuda_fail(e, "nrc_train_bwd");
+  gdf::AdamParams a = adam_params(c, 2, c.cfg.adam_nrc, c.cfg.nrc_loss_scale, c.ws.sq + 2 * gdf::kAdamBlocks);
+  a.grid_grad = nullptr;
+  e = gdf::launch_adam_ema(a, st);
+  if (e != cudaSuccess) return cuda_fail(e, "adam_ema (nrc)");
+  e = gdf::launch_train_stats(c.ws.fwd, m, c.ws.sq + 2 * gdf::kAdamBlocks, gdf::kAdamBlocks, c.ws.stats, st);
+  if (e != cudaSuccess) return cuda_fail(e, "train_stats (nrc)");
+  if (stats) {
+    double h[2];
+    unsigned long long dropped = 0;
+    GDF_CUDA(cudaMemcpyAsync(h, c.ws.stats, sizeof(h), cudaMemcpyDeviceToHost, st));
+    GDF_CUDA(cudaMemcpyAsync(&dropped, c.ws.dropped, sizeof(dropped), cudaMemcpyDeviceToHost, st));
+    GDF_CUDA(cudaStreamSynchronize(st));
+    // NRC::trainStep reports reduce(L) / batch (nrc.cpp:166)
+    stats->loss = h[0] / static_cast<double>(m);
+    stats->grad_norm = std::sqrt(h[1]);
+    stats->n_records = m;
+    stats->n_dropped = static_cast<int64_t>(dropped);
+  }
+  return GDF_OK;
 }
 
 gdf_status gdf_sync_status(gdf_ctx* ctx, void* stream) {

@@ -25,6 +25,7 @@
 #include "../device/df_math.cuh"
 #include "../device/df_tile.cuh"
 #include "../device/sm100.cuh"
+#include "../device/train_tile.cuh"
 #include "df_kernels.h"
 #include "train_kernels.h"
 
@@ -32,67 +33,9 @@ namespace gdf {
 namespace {
 
 using namespace sm100;
+using namespace train_tile;
 
 __host__ __device__ constexpr int pad16t(int v) { return (v + 15) / 16 * 16; }
-
-// MMA with arbitrary majors: D (+)= A * B over `ksteps` K=16 steps. a/b
-// descriptors advance by a_step / b_step bytes per step.
-__device__ __forceinline__ void mma_steps(uint32_t d, uint32_t a_s, uint32_t a_lbo, uint32_t a_sbo,
-                                          uint32_t a_step, uint32_t b_s, uint32_t b_lbo,
-                                          uint32_t b_sbo, uint32_t b_step, uint32_t idesc,
-                                          int ksteps, bool accumulate) {
-  for (int s = 0; s < ksteps; ++s) {
-    const uint64_t ad = smem_desc(a_s + s * a_step, a_lbo, a_sbo);
-    const uint64_t bd = smem_desc(b_s + s * b_step, b_lbo, b_sbo);
-    mma_f16_ss(d, ad, bd, idesc, (accumulate || s > 0) ? 1u : 0u);
-  }
-}
-
-// ReLU'(forward activation) * accumulator -> fp16 -> D tile (64 columns).
-__device__ __forceinline__ void dgrad_relu_to_tile(const tile::Wg& c, uint32_t taddr,
-                                                   const uint8_t* h_tile, uint8_t* d_tile) {
-#pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    uint32_t r[32];
-    tmem_ld32(taddr + h * 32, r);
-    tmem_ld_wait();
-#pragma unroll
-    for (int kc = 0; kc < 4; ++kc) {
-      const uint4 hv = *reinterpret_cast<const uint4*>(h_tile + tile::chunk_off(c.row, h * 4 + kc, 64));
-      const __half2* hh = reinterpret_cast<const __half2*>(&hv);
-      __half2 out[4];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const float2 f = __half22float2(hh[j]);
-        const float a = f.x > 0.f ? __uint_as_float(r[kc * 8 + 2 * j]) : 0.f;
-        const float b = f.y > 0.f ? __uint_as_float(r[kc * 8 + 2 * j + 1]) : 0.f;
-        out[j] = __floats2half2_rn(a, b);
-      }
-      *reinterpret_cast<uint4*>(d_tile + tile::chunk_off(c.row, h * 4 + kc, 64)) =
-          *reinterpret_cast<uint4*>(out);
-    }
-  }
-  tc_fence_before();
-}
-
-__device__ __forceinline__ void relu_to(const tile::Wg& c, uint32_t taddr, uint8_t* dst) {
-#pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    uint32_t r[32];
-    tmem_ld32(taddr + h * 32, r);
-    tmem_ld_wait();
-#pragma unroll
-    for (int kc = 0; kc < 4; ++kc) {
-      __half2 v[4];
-#pragma unroll
-      for (int j = 0; j < 4; ++j)
-        v[j] = __floats2half2_rn(fmaxf(__uint_as_float(r[kc * 8 + 2 * j]), 0.f),
-                                 fmaxf(__uint_as_float(r[kc * 8 + 2 * j + 1]), 0.f));
-      *reinterpret_cast<uint4*>(dst + tile::chunk_off(c.row, h * 4 + kc, 64)) = *reinterpret_cast<uint4*>(v);
-    }
-  }
-  tc_fence_before();
-}
 
 // dL/dlogits of one row into the D tile (fp16, 64 columns; first NB used).
 // compute_gradients_specialized_linear_interpolation / _nearest (AR.h:51-104).

@@ -344,3 +344,14 @@ def ref_lib():
             f.restype = res
         _ref = L
     return _ref
+
+
+def nrc_train_grads(nc: NrcCfg, w, inp, target, loss_scale=1024.0):
+    """NRC batch: per-record loss values and the FP64 gradient (scaled)."""
+    w16 = round_f16(w)
+    x, y = f32(inp), f32(target)
+    m = x.shape[0]
+    g = np.zeros(w16.size, np.float64)
+    loss = np.empty(m, np.float32)
+    lib().go_nrc_train_grads(C.byref(nc), _p(w16), _p(x), _p(y), m, loss_scale, _p(g), _p(loss))
+    return g, loss

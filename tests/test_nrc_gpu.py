@@ -1,0 +1,63 @@
+"""GPU parity of the Neural Radiance Cache: gdf_nrc_query and
+gdf_nrc_train_step against the oracle (NRC::inferenceStep / trainStep,
+src/render/guided/nrc.cpp:114-181)."""
+import numpy as np
+import pytest
+
+import oracle as O
+import pygdf
+from gdf_testutil import dev, gen_weights
+from pygdf import workload as W
+
+pytestmark = pytest.mark.gpu
+
+
+def _ctx(seed=1, gain=1.2):
+    cfg = pygdf.default_config(pygdf.PRESET_FULL)
+    ctx = pygdf.Context(cfg)
+    w = gen_weights(cfg, 2, seed, gain)
+    ctx.set_params(2, w)
+    return cfg, ctx, w
+
+
+@pytest.mark.parametrize("m", [1, 127, 129, 5000])
+def test_nrc_query_matches_oracle(m):
+    cfg, ctx, w = _ctx()
+    x, _ = W.nrc_batch(m, 3)
+    out = dev(np.zeros((m, 3), np.float32))
+    ctx.nrc_query(dev(x), out)
+    ctx.sync()
+    got = out.cpu().numpy()
+    ref = O.nrc_query(O.nrc_cfg_from(cfg), w, x)
+    scale = np.abs(ref).max() + 1e-6
+    assert np.abs(got - ref).max() <= 2e-3 * scale, (np.abs(got - ref).max(), scale)
+    ctx.close()
+
+
+def test_nrc_train_step_gradient_and_loss_match_oracle():
+    cfg, ctx, w = _ctx(seed=4)
+    m = 8192
+    x, y = W.nrc_batch(m, 5)
+    st = ctx.nrc_train_step(dev(x), dev(y))
+    ctx.sync()
+    g_ref, loss_ref = O.nrc_train_grads(O.nrc_cfg_from(cfg), w, x, y, cfg.nrc_loss_scale)
+    loss_ref = float(np.sum(loss_ref.astype(np.float64)) / m)
+    assert abs(st.loss - loss_ref) <= 1e-3 * abs(loss_ref), (st.loss, loss_ref)
+    mom, v, steps, k = ctx.get_optimizer_state(2)
+    g = mom.astype(np.float64) / (1.0 - np.float64(np.float32(cfg.adam_nrc.beta1)))
+    g -= np.float64(cfg.adam_nrc.l2_reg) * w
+    gref = g_ref / cfg.nrc_loss_scale
+    rel = np.linalg.norm(g - gref) / np.linalg.norm(gref)
+    assert rel < 5e-3, rel
+    assert k == 1 and np.all(steps == 1)
+    ctx.close()
+
+
+def test_nrc_training_reduces_loss():
+    cfg = pygdf.default_config(pygdf.PRESET_FULL)
+    ctx = pygdf.Context(cfg)
+    x, y = W.nrc_batch(65536, 8)
+    dx, dy = dev(x), dev(y)
+    losses = [ctx.nrc_train_step(dx, dy).loss for _ in range(40)]
+    assert losses[-1] < 0.7 * losses[0], losses
+    ctx.close()
