@@ -285,6 +285,35 @@ def main():
         e.synchronize()
         train_times.append(s.elapsed_time(e))
     last = ctx.train_step(da, db, dt, stream=stream, stats=True)
+    del da, db, dt
+    # ---- training-record producer (gdf_build_train_records) over one frame
+    import pygdf
+    n_px = n
+    fields, depth = W.path_state(n_px, 91 + rank)
+    fd = {k: torch.from_numpy(np.ascontiguousarray(v)).to(dev) for k, v in fields.items()}
+    cd = torch.from_numpy(depth.view(np.int32).copy()).to(dev)
+    st = pygdf.path_state(fd, cd)
+    box, px = pygdf.Aabb.of((-2.0, -1.0, -3.0), (4.0, 2.0, 1.0)), pygdf.TrainPixels(n_px, 0, 1)
+    cap = n_px * 5
+    ra, rb, rt = (torch.empty((cap, k), dtype=torch.float32, device=dev) for k in (9, 10, 9))
+    for _ in range(args.warmup):
+        n_rec = ctx.build_train_records(st, box, px, ra, rb, rt, stream=stream)
+    rec_times = []
+    for i in range(args.steps):
+        flush.zero_()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        n_rec = ctx.build_train_records(st, box, px, ra, rb, rt, stream=stream)
+        e.record(stream)
+        e.synchronize()
+        rec_times.append(s.elapsed_time(e))
+    # bytes every producer must move once: cur_depth, the delta flags of the
+    # visited vertices, the 84 B of fields of each non-delta vertex, and the
+    # 112 B of each record written
+    visit = np.arange(5)[:, None] < depth[None, :].astype(np.int64)
+    nondelta = visit & (fields["delta"] == 0)
+    rec_bytes = 4 * n_px + int(visit.sum()) + 84 * int(nondelta.sum()) + 112 * n_rec
+    del fd, cd, st, ra, rb, rt
     clk = clocks.stop()
     ctx.sync(stream)
 
@@ -330,6 +359,13 @@ def main():
                       "unit": "records/s", "batch": nb, "ms_per_step": ms_train,
                       "achieved_tflops": TRAIN_FLOP_PER_RECORD[args.workload] * nb / (ms_train * 1e-3) / 1e12,
                       "loss": last.loss, "launches_per_step": 6},
+            "records": {"metric": "training records/s (generate_training_data_AR)",
+                        "value": n_rec * world / (statistics.mean(rec_times) * 1e-3), "unit": "records/s",
+                        "pixels": n_px, "records": n_rec, "ms_per_step": statistics.mean(rec_times),
+                        "algorithmic_bytes": rec_bytes,
+                        "achieved_gbs": rec_bytes / (min(rec_times) * 1e-3) / 1e9,
+                        "frac_hbm": rec_bytes / (min(rec_times) * 1e-3) / 1e9 / peaks["hbm_gbs"],
+                        "launches_per_step": 3},
             "clocks": clk,
             "gpu_launches": args.steps,
         }

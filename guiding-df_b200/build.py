@@ -30,6 +30,7 @@ SOURCES = [
     ("kernels/df_train.cu", ["-fmad=false"]),
     ("kernels/loss_static.cu", []),
     ("kernels/nrc.cu", ["-fmad=false"]),
+    ("kernels/paths.cu", ["-fmad=false"]),
     ("host/api.cpp", []),
 ]
 

@@ -4,6 +4,8 @@
 // validation, parameter layout and initialisation, checkpoint files, and the
 // launches of the fused kernels. Nothing here computes a query on the CPU;
 // every compute entry point launches a CUDA kernel or fails.
+#include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -14,6 +16,7 @@
 
 #include "../kernels/df_kernels.h"
 #include "../kernels/nrc_kernels.h"
+#include "../kernels/paths_kernels.h"
 #include "../kernels/train_kernels.h"
 #include "context.h"
 
@@ -98,6 +101,12 @@ gdf_status validate(const gdf_config& c) {
     return fail(GDF_ERR_INVALID_ARG, "precision");
   if (c.max_queries < 0 || c.max_train_batch < 0)
     return fail(GDF_ERR_INVALID_ARG, "negative capacity");
+  const int64_t cap = c.max_train_batch > 0 ? c.max_train_batch : 65536;
+  if (c.df_batch_size < 128 || c.df_batch_size > cap || c.nrc_batch_size < 128 ||
+      c.nrc_batch_size > cap)
+    return fail(GDF_ERR_INVALID_ARG, "training batch sizes must be in [128, max_train_batch]");
+  if (c.min_train_batch < 1 || c.df_batches_per_frame < 0 || c.nrc_batches_per_frame < 0)
+    return fail(GDF_ERR_INVALID_ARG, "min_train_batch / batches_per_frame");
   gdf::DfShape s{c.grid_theta.n_levels, c.grid_theta.n_features_per_level, c.n_bins_theta,
                  c.n_bins_phi, c.pdf_interp == GDF_PDF_LINEAR};
   if (!gdf::df_shape_supported(s))
@@ -241,6 +250,24 @@ void free_ws(gdf::TrainWorkspace& w) {
   w = gdf::TrainWorkspace{};
 }
 
+void free_pw(gdf::PathWorkspace& w) {
+  cudaFree(w.mask);
+  cudaFree(w.block_counts);
+  cudaFree(w.block_offsets);
+  cudaFree(w.totals);
+  cudaFreeHost(w.totals_host);
+  cudaFree(w.df_in);
+  cudaFree(w.df_in_phi);
+  cudaFree(w.df_target);
+  cudaFree(w.nrc_query);
+  cudaFree(w.nrc_depth);
+  cudaFree(w.nrc_pixel);
+  cudaFree(w.nrc_out);
+  cudaFree(w.nrc_train_in);
+  cudaFree(w.nrc_train_target);
+  w = gdf::PathWorkspace{};
+}
+
 gdf_status alloc_ws(Context& c) {
   gdf::TrainWorkspace& w = c.ws;
   gdf_status s;
@@ -355,6 +382,9 @@ gdf_status gdf_default_config(int32_t preset, gdf_config* cfg) {
   c.precision = GDF_PREC_FP16;
   c.seed = 7272u;  // KRR_DEFAULT_RND_SEED (src/lib/src/core/config.in.h:15)
   gdf_grid_config hash{GDF_GRID_HASH, 8, 2, 16, 16, 2.0f, GDF_GRID_LINEAR};
+  c.min_train_batch = 65536;       // MIN_TRAIN_BATCH_SIZE (parameters.h:55)
+  c.df_batches_per_frame = 5;      // batchPerFrame (learnedDistribution.h:138)
+  c.nrc_batches_per_frame = 4;     // NRC_ITER_COUNT (parameters.h:65)
   switch (preset) {
     case GDF_PRESET_SMALL:
       c.n_bins_theta = c.n_bins_phi = 32;
@@ -363,6 +393,7 @@ gdf_status gdf_default_config(int32_t preset, gdf_config* cfg) {
       c.nrc_enable = 1;
       c.max_queries = 65536;
       c.max_train_batch = 65536;
+      c.df_batch_size = c.nrc_batch_size = 65536;
       break;
     case GDF_PRESET_FULL:
       c.n_bins_theta = c.n_bins_phi = 64;
@@ -372,7 +403,9 @@ gdf_status gdf_default_config(int32_t preset, gdf_config* cfg) {
       c.mlp_theta = c.mlp_phi = gdf_mlp_config{64, 4};
       c.nrc_enable = 1;
       c.max_queries = 1920 * 1080;
-      c.max_train_batch = 262144;
+      c.max_train_batch = 1048576;
+      c.df_batch_size = 262144;
+      c.nrc_batch_size = 1048576;  // TRAIN_BATCH_SIZE_NRC (parameters.h:66)
       break;
     case GDF_PRESET_REFERENCE: {
       // common/configs/nn/base_product_df.json + parameters.h:41,48.
@@ -383,7 +416,9 @@ gdf_status gdf_default_config(int32_t preset, gdf_config* cfg) {
       c.mlp_theta = c.mlp_phi = gdf_mlp_config{64, 3};
       c.nrc_enable = 1;
       c.max_queries = 1280 * 720;  // MAX_RESOLUTION (parameters.h:51)
-      c.max_train_batch = 65536 * 8;
+      c.max_train_batch = 1048576;
+      c.df_batch_size = 65536 * 8;   // TRAIN_BATCH_SIZE (parameters.h:54)
+      c.nrc_batch_size = 1048576;
       break;
     }
     default:
@@ -408,6 +443,7 @@ gdf_status gdf_create(const gdf_config* cfg, gdf_ctx** out) {
   auto cleanup = [&](gdf_status st) {
     for (Net& n : c.net) free_net(n);
     free_ws(c.ws);
+    free_pw(c.pw);
     cudaFree(c.d_err);
     delete h;
     return st;
@@ -433,6 +469,7 @@ gdf_status gdf_destroy(gdf_ctx* ctx) {
   cudaDeviceSynchronize();
   for (Net& n : ctx->c.net) free_net(n);
   free_ws(ctx->c.ws);
+  free_pw(ctx->c.pw);
   cudaFree(ctx->c.d_err);
   delete ctx;
   return GDF_OK;
@@ -562,6 +599,44 @@ gdf_status gdf_infer(gdf_ctx* ctx, const float* queries, const uint8_t* guided,
   p.n = n;
   p.philox_seed = philox_seed;
   p.philox_offset = philox_offset;
+  cudaError_t e = gdf::launch_df_fused(df_shape(ctx->c), gdf::kModeInfer, p, ctx->c.num_sms,
+                                       static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cuda_fail(e, "df_fused (infer)");
+  return GDF_OK;
+}
+
+gdf_status gdf_infer_ex(gdf_ctx* ctx, const gdf_infer_args* a, void* stream) {
+  if (!ctx || !a) return fail(GDF_ERR_INVALID_ARG, "null ctx / args");
+  const int64_t n = a->n;
+  if (n < 0) return fail(GDF_ERR_INVALID_ARG, "n < 0");
+  if (n == 0) return GDF_OK;
+  gdf_status s;
+  if ((s = check_ptr(a->wi_dev, "wi"))) return s;
+  if (a->shading) {
+    const gdf_shading& sh = *a->shading;
+    if ((s = check_ptr(sh.pos, "shading.pos")) || (s = check_ptr(sh.wo, "shading.wo")) ||
+        (s = check_ptr(sh.normal, "shading.normal")) || (s = check_ptr(sh.roughness, "shading.roughness")))
+      return s;
+  } else if ((s = check_ptr(a->queries_dev, "queries"))) {
+    return s;
+  }
+  if (ctx->c.cfg.max_queries > 0 && n > ctx->c.cfg.max_queries)
+    return fail(GDF_ERR_INVALID_ARG, "n exceeds max_queries");
+  if ((reinterpret_cast<uintptr_t>(a->wi_dev) & 15u) ||
+      (a->uniforms_dev && (reinterpret_cast<uintptr_t>(a->uniforms_dev) & 15u)) ||
+      (a->dir_pdf_dev && (reinterpret_cast<uintptr_t>(a->dir_pdf_dev) & 15u)))
+    return fail(GDF_ERR_INVALID_ARG, "wi, uniforms and dir_pdf must be 16-byte aligned");
+  gdf::DfKernelParams p = df_params(ctx->c);
+  p.queries = a->queries_dev;
+  if (a->shading) p.shading = *a->shading;
+  p.aabb = a->aabb;
+  p.guided = a->guided_dev;
+  p.uniforms = a->uniforms_dev;
+  p.wi = a->wi_dev;
+  p.dir_pdf = a->dir_pdf_dev;
+  p.n = n;
+  p.philox_seed = a->philox_seed;
+  p.philox_offset = a->philox_offset;
   cudaError_t e = gdf::launch_df_fused(df_shape(ctx->c), gdf::kModeInfer, p, ctx->c.num_sms,
                                        static_cast<cudaStream_t>(stream));
   if (e != cudaSuccess) return cuda_fail(e, "df_fused (infer)");
@@ -818,6 +893,351 @@ gdf_status gdf_nrc_train_step(gdf_ctx* ctx, const float* in, const float* target
     stats->n_records = m;
     stats->n_dropped = static_cast<int64_t>(dropped);
   }
+  return GDF_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------ records from the path tracer
+
+namespace {
+
+int64_t train_pixels(const gdf_train_pixels& px) {
+  return px.stride > 0 ? px.max_queue_size / px.stride : 0;
+}
+
+gdf_status check_px(const gdf_path_state* st, const gdf_aabb* aabb, const gdf_train_pixels* px) {
+  if (!st || !aabb || !px) return fail(GDF_ERR_INVALID_ARG, "null state / aabb / pixels");
+  if (px->stride == 0 || px->max_queue_size < 0)
+    return fail(GDF_ERR_INVALID_ARG, "train pixel stride must be >= 1 and queue size >= 0");
+  if (px->max_queue_size > INT32_MAX) return fail(GDF_ERR_INVALID_ARG, "max_queue_size > 2^31 - 1");
+  if (!st->cur_depth) return fail(GDF_ERR_INVALID_ARG, "cur_depth is null");
+  return GDF_OK;
+}
+
+// Scratch of the count/scan/emit passes for n training pixels.
+gdf_status ensure_scratch(Context& c, int64_t n) {
+  gdf::PathWorkspace& w = c.pw;
+  if (!w.totals) {
+    gdf_status s;
+    if ((s = dalloc(&w.totals, 2))) return s;
+    if (cudaMallocHost(&w.totals_host, 2 * sizeof(int64_t)) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(GDF_ERR_OOM_BUDGET, "pinned host allocation failed");
+    }
+  }
+  if (n <= w.pixels) return GDF_OK;
+  cudaFree(w.mask);
+  cudaFree(w.block_counts);
+  cudaFree(w.block_offsets);
+  w.mask = nullptr;
+  w.block_counts = nullptr;
+  w.block_offsets = nullptr;
+  w.pixels = 0;
+  const int64_t nb = gdf::produce_blocks(n);
+  gdf_status s;
+  if ((s = dalloc(&w.mask, static_cast<size_t>(n))) ||
+      (s = dalloc(&w.block_counts, static_cast<size_t>(2 * nb))) ||
+      (s = dalloc(&w.block_offsets, static_cast<size_t>(2 * nb))))
+    return s;
+  w.pixels = n;
+  return GDF_OK;
+}
+
+gdf_status ensure_df_records(Context& c, int64_t cap) {
+  gdf::PathWorkspace& w = c.pw;
+  if (cap <= w.df_cap) return GDF_OK;
+  cudaFree(w.df_in);
+  cudaFree(w.df_in_phi);
+  cudaFree(w.df_target);
+  w.df_in = w.df_in_phi = w.df_target = nullptr;
+  w.df_cap = 0;
+  gdf_status s;
+  if ((s = dalloc(&w.df_in, static_cast<size_t>(cap) * 9)) ||
+      (s = dalloc(&w.df_in_phi, static_cast<size_t>(cap) * 10)) ||
+      (s = dalloc(&w.df_target, static_cast<size_t>(cap) * 9)))
+    return s;
+  w.df_cap = cap;
+  return GDF_OK;
+}
+
+gdf_status ensure_nrc_rows(Context& c, int64_t cap) {
+  gdf::PathWorkspace& w = c.pw;
+  if (cap <= w.nrc_cap) return GDF_OK;
+  cudaFree(w.nrc_query);
+  cudaFree(w.nrc_depth);
+  cudaFree(w.nrc_pixel);
+  cudaFree(w.nrc_out);
+  cudaFree(w.nrc_train_in);
+  cudaFree(w.nrc_train_target);
+  w.nrc_query = w.nrc_out = w.nrc_train_in = w.nrc_train_target = nullptr;
+  w.nrc_depth = w.nrc_pixel = nullptr;
+  w.nrc_cap = 0;
+  w.nrc_rows = 0;
+  const size_t n = static_cast<size_t>(cap);
+  gdf_status s;
+  if ((s = dalloc(&w.nrc_query, n * 15)) || (s = dalloc(&w.nrc_depth, n)) ||
+      (s = dalloc(&w.nrc_pixel, n)) || (s = dalloc(&w.nrc_out, n * 3)) ||
+      (s = dalloc(&w.nrc_train_in, n * 15)) || (s = dalloc(&w.nrc_train_target, n * 3)))
+    return s;
+  w.nrc_cap = cap;
+  return GDF_OK;
+}
+
+// One producer pass; counts[] receive the full list sizes (synchronises).
+gdf_status produce(Context& c, const gdf_path_state& st, const gdf_aabb& aabb,
+                   const gdf_train_pixels& px, int kind, gdf::ProduceParams p,
+                   int64_t counts[2], cudaStream_t s) {
+  const int64_t n = train_pixels(px);
+  gdf_status rc = ensure_scratch(c, n);
+  if (rc) return rc;
+  p.st = st;
+  p.aabb = aabb;
+  p.n_train = n;
+  p.offset = px.offset;
+  p.stride = px.stride;
+  p.bins_theta = c.cfg.n_bins_theta;
+  p.linear = c.cfg.pdf_interp == GDF_PDF_LINEAR;
+  p.mask = c.pw.mask;
+  p.block_counts = c.pw.block_counts;
+  p.block_offsets = c.pw.block_offsets;
+  p.totals = c.pw.totals;
+  cudaError_t e = gdf::launch_produce(p, kind, s);
+  if (e != cudaSuccess) return cuda_fail(e, "record producer");
+  GDF_CUDA(cudaMemcpyAsync(c.pw.totals_host, c.pw.totals, 2 * sizeof(int64_t),
+                           cudaMemcpyDeviceToHost, s));
+  GDF_CUDA(cudaStreamSynchronize(s));
+  counts[0] = c.pw.totals_host[0];
+  counts[1] = c.pw.totals_host[1];
+  return GDF_OK;
+}
+
+gdf_status nrc_query_rows(Context& c, const float* in, float* out, int64_t m, cudaStream_t s) {
+  if (m == 0) return GDF_OK;
+  gdf::NrcParams q;
+  std::memset(&q, 0, sizeof(q));
+  q.in = in;
+  q.out = out;
+  q.n = m;
+  q.blob = c.net[2].blob_ema;
+  q.blob_bytes = c.net[2].blob_bytes;
+  q.hidden = c.net[2].hidden;
+  q.err = c.d_err;
+  cudaError_t e = gdf::launch_nrc_query(q, c.num_sms, s);
+  if (e != cudaSuccess) return cuda_fail(e, "nrc_query");
+  return GDF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+gdf_status gdf_prepare_queries(const gdf_shading* sh, const gdf_aabb* aabb, float* queries,
+                               int64_t n, void* stream) {
+  if (!sh || !aabb) return fail(GDF_ERR_INVALID_ARG, "null shading / aabb");
+  if (n < 0) return fail(GDF_ERR_INVALID_ARG, "n < 0");
+  if (n == 0) return GDF_OK;
+  gdf_status s;
+  if ((s = check_ptr(sh->pos, "shading.pos")) || (s = check_ptr(sh->wo, "shading.wo")) ||
+      (s = check_ptr(sh->normal, "shading.normal")) || (s = check_ptr(sh->roughness, "shading.roughness")) ||
+      (s = check_ptr(queries, "queries")))
+    return s;
+  cudaError_t e = gdf::launch_prepare_queries(*sh, *aabb, queries, n, static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cuda_fail(e, "prepare_queries");
+  return GDF_OK;
+}
+
+gdf_status gdf_build_train_records(gdf_ctx* ctx, const gdf_path_state* state, const gdf_aabb* aabb,
+                                   const gdf_train_pixels* px, float* in_theta, float* in_phi,
+                                   float* target, int64_t capacity, int64_t* count_host,
+                                   void* stream) {
+  if (!ctx) return fail(GDF_ERR_INVALID_ARG, "ctx is null");
+  gdf_status s;
+  if ((s = check_px(state, aabb, px))) return s;
+  if (capacity < 0) return fail(GDF_ERR_INVALID_ARG, "capacity < 0");
+  if (capacity > 0 && ((s = check_ptr(in_theta, "in_theta")) || (s = check_ptr(in_phi, "in_phi")) ||
+                       (s = check_ptr(target, "target"))))
+    return s;
+  gdf::ProduceParams p;
+  std::memset(&p, 0, sizeof(p));
+  p.out_a0 = in_theta;
+  p.out_a1 = in_phi;
+  p.out_a2 = target;
+  p.cap_a = capacity;
+  int64_t counts[2];
+  if ((s = produce(ctx->c, *state, *aabb, *px, gdf::kRecordsDf, p, counts,
+                   static_cast<cudaStream_t>(stream))))
+    return s;
+  if (count_host) *count_host = counts[0];
+  if (counts[0] > capacity) return fail(GDF_ERR_INVALID_ARG, "more records than capacity");
+  return GDF_OK;
+}
+
+gdf_status gdf_build_nrc_records(gdf_ctx* ctx, gdf_path_state* state, const gdf_aabb* aabb,
+                                 const gdf_train_pixels* px, int32_t with_training,
+                                 float* query_in, int32_t* query_depth, int32_t* query_pixel,
+                                 int64_t query_capacity, float* train_in, float* train_target,
+                                 int64_t train_capacity, int64_t* counts_host, void* stream) {
+  if (!ctx) return fail(GDF_ERR_INVALID_ARG, "ctx is null");
+  gdf_status s;
+  if ((s = check_px(state, aabb, px))) return s;
+  if (query_capacity < 0 || train_capacity < 0) return fail(GDF_ERR_INVALID_ARG, "capacity < 0");
+  if (query_capacity > 0 && ((s = check_ptr(query_in, "query_in")) ||
+                             (s = check_ptr(query_depth, "query_depth")) ||
+                             (s = check_ptr(query_pixel, "query_pixel"))))
+    return s;
+  if (with_training && train_capacity > 0 &&
+      ((s = check_ptr(train_in, "train_in")) || (s = check_ptr(train_target, "train_target"))))
+    return s;
+  gdf::ProduceParams p;
+  std::memset(&p, 0, sizeof(p));
+  p.out_a0 = query_in;
+  p.a_depth = query_depth;
+  p.a_pixel = query_pixel;
+  p.cap_a = query_capacity;
+  p.out_b0 = train_in;
+  p.out_b1 = train_target;
+  p.cap_b = with_training ? train_capacity : 0;
+  int64_t counts[2];
+  if ((s = produce(ctx->c, *state, *aabb, *px,
+                   with_training ? gdf::kRecordsNrcTrain : gdf::kRecordsNrcQuery, p, counts,
+                   static_cast<cudaStream_t>(stream))))
+    return s;
+  if (counts_host) {
+    counts_host[0] = counts[0];
+    counts_host[1] = counts[1];
+  }
+  if (counts[0] > query_capacity || counts[1] > p.cap_b)
+    return fail(GDF_ERR_INVALID_ARG, "more rows than capacity");
+  return GDF_OK;
+}
+
+gdf_status gdf_apply_nrc(gdf_ctx* ctx, gdf_path_state* state, const float* nrc_out,
+                         const int32_t* depth, const int32_t* pixel, int64_t m, void* stream) {
+  if (!ctx || !state) return fail(GDF_ERR_INVALID_ARG, "null ctx / state");
+  if (m < 0) return fail(GDF_ERR_INVALID_ARG, "m < 0");
+  if (m == 0) return GDF_OK;
+  gdf_status s;
+  if ((s = check_ptr(nrc_out, "nrc_out")) || (s = check_ptr(depth, "depth")) ||
+      (s = check_ptr(pixel, "pixel")) || (s = check_ptr(state->cur_depth, "cur_depth")))
+    return s;
+  cudaError_t e = gdf::launch_apply_nrc(*state, nrc_out, depth, pixel, m, static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cuda_fail(e, "apply_nrc");
+  return GDF_OK;
+}
+
+gdf_status gdf_nrc_train_paths(gdf_ctx* ctx, gdf_path_state* state, const gdf_aabb* aabb,
+                               const gdf_train_pixels* px, float* loss_host,
+                               int64_t* n_samples_host, void* stream) {
+  if (!ctx) return fail(GDF_ERR_INVALID_ARG, "ctx is null");
+  Context& c = ctx->c;
+  if (!c.net[2].present) return fail(GDF_ERR_STATE, "NRC is disabled in this context");
+  gdf_status s;
+  if ((s = check_px(state, aabb, px))) return s;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int64_t cap = train_pixels(*px) * GDF_MAX_TRAIN_DEPTH;
+  if ((s = ensure_nrc_rows(c, cap))) return s;
+  gdf::ProduceParams p;
+  std::memset(&p, 0, sizeof(p));
+  p.out_a0 = c.pw.nrc_query;
+  p.a_depth = c.pw.nrc_depth;
+  p.a_pixel = c.pw.nrc_pixel;
+  p.cap_a = c.pw.nrc_cap;
+  p.out_b0 = c.pw.nrc_train_in;
+  p.out_b1 = c.pw.nrc_train_target;
+  p.cap_b = c.pw.nrc_cap;
+  int64_t counts[2];
+  if ((s = produce(c, *state, *aabb, *px, gdf::kRecordsNrcTrain, p, counts, st))) return s;
+  c.pw.nrc_rows = counts[0];
+  const int64_t n = counts[1];
+  if (n_samples_host) *n_samples_host = n;
+  // NRC::trainStep batch loop (nrc.cpp:129-168), including its use of the
+  // rounded local batch size as the row offset.
+  const int64_t bs = c.cfg.nrc_batch_size;
+  const int64_t batches = std::max<int64_t>(n / bs + 1, c.cfg.nrc_batches_per_frame);
+  const int64_t eff = std::min<int64_t>(n / batches, bs);
+  double loss_sum = 0.0;
+  for (int64_t it = 0; it < batches; ++it) {
+    int64_t local = std::min<int64_t>(n - it * eff, eff);
+    local -= local % 128;
+    if (local < c.cfg.min_train_batch) break;
+    gdf_train_stats ts;
+    if ((s = gdf_nrc_train_step(ctx, c.pw.nrc_train_in + it * local * 15,
+                                c.pw.nrc_train_target + it * local * 3, local, &ts, stream)))
+      return s;
+    loss_sum += ts.loss;
+  }
+  if (loss_host) *loss_host = static_cast<float>(loss_sum / static_cast<double>(batches));
+  return GDF_OK;
+}
+
+gdf_status gdf_nrc_substitute_paths(gdf_ctx* ctx, gdf_path_state* state, const gdf_aabb* aabb,
+                                    const gdf_train_pixels* px, int32_t skip_generation,
+                                    void* stream) {
+  if (!ctx) return fail(GDF_ERR_INVALID_ARG, "ctx is null");
+  Context& c = ctx->c;
+  if (!c.net[2].present) return fail(GDF_ERR_STATE, "NRC is disabled in this context");
+  gdf_status s;
+  if ((s = check_px(state, aabb, px))) return s;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (!skip_generation) {
+    const int64_t cap = train_pixels(*px) * GDF_MAX_TRAIN_DEPTH;
+    if ((s = ensure_nrc_rows(c, cap))) return s;
+    gdf::ProduceParams p;
+    std::memset(&p, 0, sizeof(p));
+    p.out_a0 = c.pw.nrc_query;
+    p.a_depth = c.pw.nrc_depth;
+    p.a_pixel = c.pw.nrc_pixel;
+    p.cap_a = c.pw.nrc_cap;
+    int64_t counts[2];
+    if ((s = produce(c, *state, *aabb, *px, gdf::kRecordsNrcQuery, p, counts, st))) return s;
+    c.pw.nrc_rows = counts[0];
+  }
+  const int64_t m = c.pw.nrc_rows;
+  if ((s = nrc_query_rows(c, c.pw.nrc_query, c.pw.nrc_out, m, st))) return s;
+  if ((s = gdf_apply_nrc(ctx, state, c.pw.nrc_out, c.pw.nrc_depth, c.pw.nrc_pixel, m, stream)))
+    return s;
+  c.pw.nrc_rows = 0;  // inferenceBuffer clear() (nrc.cpp:216)
+  GDF_CUDA(cudaStreamSynchronize(st));
+  return GDF_OK;
+}
+
+gdf_status gdf_train_paths(gdf_ctx* ctx, const gdf_path_state* state, const gdf_aabb* aabb,
+                           const gdf_train_pixels* px, float* loss_host, int64_t* n_samples_host,
+                           void* stream) {
+  if (!ctx) return fail(GDF_ERR_INVALID_ARG, "ctx is null");
+  Context& c = ctx->c;
+  gdf_status s;
+  if ((s = check_px(state, aabb, px))) return s;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int64_t cap = train_pixels(*px) * GDF_MAX_TRAIN_DEPTH;
+  if ((s = ensure_df_records(c, cap))) return s;
+  gdf::ProduceParams p;
+  std::memset(&p, 0, sizeof(p));
+  p.out_a0 = c.pw.df_in;
+  p.out_a1 = c.pw.df_in_phi;
+  p.out_a2 = c.pw.df_target;
+  p.cap_a = c.pw.df_cap;
+  int64_t counts[2];
+  if ((s = produce(c, *state, *aabb, *px, gdf::kRecordsDf, p, counts, st))) return s;
+  const int64_t n = counts[0];
+  if (n_samples_host) *n_samples_host = n;
+  // LearnedDistribution::trainStep batch loop (learnedDistribution.cpp:227-290).
+  const int64_t bs = c.cfg.df_batch_size;
+  const int64_t batches = std::min<int64_t>(n / bs + 1, c.cfg.df_batches_per_frame);
+  double loss = 0.0;
+  for (int64_t it = 0; it < batches; ++it) {
+    int64_t local = std::min<int64_t>(n - it * bs, bs);
+    local -= local % 128;
+    if (local < c.cfg.min_train_batch) break;
+    gdf_train_stats ts;
+    const int64_t o = it * bs;
+    if ((s = gdf_train_step(ctx, c.pw.df_in + o * 9, c.pw.df_in_phi + o * 10, c.pw.df_target + o * 9,
+                            local, &ts, stream)))
+      return s;
+    loss += ts.loss;
+  }
+  if (loss_host) *loss_host = batches > 0 ? static_cast<float>(loss / static_cast<double>(batches)) : 0.f;
   return GDF_OK;
 }
 

@@ -49,6 +49,28 @@ struct TrainWorkspace {
 
 constexpr int kAdamBlocks = 1184;  // 8 x 148 SMs
 
+// Buffers of the frame-level record producers, grown on demand.
+struct PathWorkspace {
+  int64_t pixels = 0;               // training-pixel capacity of the scratch
+  uint16_t* mask = nullptr;         // [pixels]
+  int32_t* block_counts = nullptr;  // [blocks x 2]
+  int64_t* block_offsets = nullptr; // [blocks x 2]
+  int64_t* totals = nullptr;        // [2] device
+  int64_t* totals_host = nullptr;   // [2] pinned
+  int64_t df_cap = 0;               // DF records
+  float* df_in = nullptr;           // [df_cap x 9]
+  float* df_in_phi = nullptr;       // [df_cap x 10]
+  float* df_target = nullptr;       // [df_cap x 9]
+  int64_t nrc_cap = 0;              // NRC query / training rows
+  float* nrc_query = nullptr;       // [nrc_cap x 15]
+  int32_t* nrc_depth = nullptr;     // [nrc_cap]
+  int32_t* nrc_pixel = nullptr;     // [nrc_cap]
+  float* nrc_out = nullptr;         // [nrc_cap x 3]
+  float* nrc_train_in = nullptr;    // [nrc_cap x 15]
+  float* nrc_train_target = nullptr;// [nrc_cap x 3]
+  int64_t nrc_rows = 0;             // query rows of the last NRC build
+};
+
 struct Context {
   gdf_config cfg{};
   int device = 0;
@@ -56,6 +78,7 @@ struct Context {
   Net net[3];  // theta, phi, nrc
   uint32_t* d_err = nullptr;  // device error word of bounded waits
   TrainWorkspace ws;
+  PathWorkspace pw;
 };
 
 // Sets the thread-local message returned by gdf_last_error().

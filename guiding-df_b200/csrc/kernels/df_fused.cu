@@ -22,6 +22,7 @@
 
 #include "../device/df_math.cuh"
 #include "../device/df_tile.cuh"
+#include "../device/records.cuh"
 #include "../device/sm100.cuh"
 #include "df_kernels.h"
 
@@ -117,8 +118,24 @@ __global__ void __launch_bounds__(128 * WGS, 1) df_fused_kernel(const __grid_con
     const int64_t row = t * 128 + c.row;
     const bool valid = row < p.n;
     float q[9], qp[10];
+    if (MODE == kModeInfer && p.shading.pos != nullptr) {
+      // generate_inference_data_AR (train.cu:344-361) in registers
 #pragma unroll
-    for (int i = 0; i < 9; ++i) q[i] = valid ? __ldg(p.queries + row * 9 + i) : 0.5f;
+      for (int i = 0; i < 9; ++i) q[i] = 0.5f;
+      if (valid) {
+        float pos[3], wo[3], nrm[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          pos[k] = __ldg(p.shading.pos + row * 3 + k);
+          wo[k] = __ldg(p.shading.wo + row * 3 + k);
+          nrm[k] = __ldg(p.shading.normal + row * 3 + k);
+        }
+        rec::shading_to_query(pos, wo, nrm, __ldg(p.shading.roughness + row), rec::scene_frame(p.aabb), q);
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < 9; ++i) q[i] = valid ? __ldg(p.queries + row * 9 + i) : 0.5f;
+    }
     bool record_ok = true;
     float tg[9];
     if constexpr (MODE == kModeTrainFwd) {
@@ -228,9 +245,15 @@ __global__ void __launch_bounds__(128 * WGS, 1) df_fused_kernel(const __grid_con
     const tile::RowResult rp = tile::row_epilogue<NBP, LINEAR>(
         c.tmem + c.lane_base, MODE == kModeInfer && guided, u_phi_given, u[2], u[3]);
     if constexpr (MODE == kModeInfer) {
-      if (valid)
-        *reinterpret_cast<float4*>(p.wi + row * 4) =
-            make_float4(u_theta, rp.u, wi.z * pdf_theta, wi.w * rp.pdf);
+      const float4 o = make_float4(u_theta, rp.u, wi.z * pdf_theta, wi.w * rp.pdf);
+      if (valid) *reinterpret_cast<float4*>(p.wi + row * 4) = o;
+      if (valid && p.dir_pdf != nullptr) {
+        // AutoRegressive over the guiding data (AR.h:25-48)
+        float d[3];
+        rec::square_to_uniform_sphere(o.x, o.y, d);
+        const float pdf = fabsf(o.z) * fabsf(o.w) * rec::kInv4Pi;
+        *reinterpret_cast<float4*>(p.dir_pdf + row * 4) = make_float4(d[0], d[1], d[2], pdf);
+      }
     } else {
       if (valid) *reinterpret_cast<float2*>(p.pdf_out + row * 2) = make_float2(pdf_theta, rp.pdf);
     }

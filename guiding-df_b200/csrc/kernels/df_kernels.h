@@ -6,6 +6,7 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include "../../../include/gdf.h"
 #include "../device/grid_levels.h"
 
 namespace gdf {
@@ -39,6 +40,10 @@ struct DfKernelParams {
   unsigned long long* n_dropped;     // records rejected by the validity filter
   float loss_scale_per_record;       // TRAIN_LOSS_SCALE / n
   GridLevels gl_theta, gl_phi;
+  // inference options (gdf_infer_ex)
+  gdf_shading shading;               // raw shading points when shading.pos != nullptr
+  gdf_aabb aabb;
+  float* dir_pdf;                    // n x 4 world direction + solid-angle pdf, nullable
 };
 
 struct DfShape {

@@ -13,7 +13,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.dirname(HERE)
 LIB_PATH = os.path.join(PKG, "lib", "libgdf_b200.so")
 
-GDF_ABI_VERSION = 1
+GDF_ABI_VERSION = 2
+MAX_TRAIN_DEPTH = 5
 GDF_OK = 0
 STATUS = {0: "OK", 1: "INVALID_ARG", 2: "OOM_BUDGET", 3: "CUDA", 4: "TIMEOUT", 5: "NUMERIC",
           6: "UNSUPPORTED", 7: "STATE"}
@@ -45,7 +46,68 @@ class Config(C.Structure):
                 ("loss_scale", C.c_float), ("nrc_enable", C.c_int32), ("nrc_frequencies", C.c_int32),
                 ("nrc_oneblob_bins", C.c_int32), ("mlp_nrc", MlpConfig), ("adam_nrc", AdamConfig),
                 ("nrc_loss_scale", C.c_float), ("precision", C.c_int32), ("seed", C.c_uint32),
-                ("max_queries", C.c_int64), ("max_train_batch", C.c_int64)]
+                ("max_queries", C.c_int64), ("max_train_batch", C.c_int64),
+                ("df_batch_size", C.c_int64), ("nrc_batch_size", C.c_int64),
+                ("min_train_batch", C.c_int64), ("df_batches_per_frame", C.c_int32),
+                ("nrc_batches_per_frame", C.c_int32)]
+
+
+class Aabb(C.Structure):
+    _fields_ = [("lo", C.c_float * 3), ("hi", C.c_float * 3)]
+
+    @staticmethod
+    def of(lo, hi) -> "Aabb":
+        a = Aabb()
+        for k in range(3):
+            a.lo[k] = float(lo[k])
+            a.hi[k] = float(hi[k])
+        return a
+
+
+class Shading(C.Structure):
+    _fields_ = [("pos", C.c_void_p), ("wo", C.c_void_p), ("normal", C.c_void_p),
+                ("roughness", C.c_void_p)]
+
+
+# gdf_record_fields member order, with components per pixel and element type
+RECORD_FIELDS = [("L", 3, "f4"), ("thp", 3, "f4"), ("Le", 3, "f4"), ("pos", 3, "f4"),
+                 ("dir", 2, "f4"), ("wi_pdf", 1, "f4"), ("mis_weight", 1, "f4"),
+                 ("delta", 1, "u1"), ("miss", 1, "u1"), ("bsdf_val", 3, "f4"), ("wo", 2, "f4"),
+                 ("normal", 2, "f4"), ("roughness", 1, "f4"), ("diffuse", 3, "f4"),
+                 ("specular", 3, "f4")]
+
+
+class RecordFields(C.Structure):
+    _fields_ = [(name, C.c_void_p) for name, _, _ in RECORD_FIELDS]
+
+
+class PathState(C.Structure):
+    _fields_ = [("depth", RecordFields * MAX_TRAIN_DEPTH), ("cur_depth", C.c_void_p)]
+
+
+class TrainPixels(C.Structure):
+    _fields_ = [("max_queue_size", C.c_int64), ("offset", C.c_uint32), ("stride", C.c_uint32)]
+
+
+class InferArgs(C.Structure):
+    _fields_ = [("queries_dev", C.c_void_p), ("shading", C.POINTER(Shading)), ("aabb", Aabb),
+                ("guided_dev", C.c_void_p), ("uniforms_dev", C.c_void_p),
+                ("philox_seed", C.c_uint64), ("philox_offset", C.c_uint64),
+                ("wi_dev", C.c_void_p), ("dir_pdf_dev", C.c_void_p), ("n", C.c_int64)]
+
+
+def path_state(fields: dict, cur_depth) -> PathState:
+    """gdf_path_state over device tensors: fields[name] is [depth, pixel(, k)]
+    contiguous, cur_depth is [pixel] uint32 (int32 storage)."""
+    st = PathState()
+    for name, k, _ in RECORD_FIELDS:
+        t = fields[name]
+        per_depth = t[0].numel() * t.element_size()
+        for d in range(MAX_TRAIN_DEPTH):
+            setattr(st.depth[d], name, t.data_ptr() + d * per_depth)
+    st.cur_depth = cur_depth.data_ptr()
+    st._keep = (fields, cur_depth)  # the struct holds raw pointers into these tensors
+    return st
 
 
 class TrainStats(C.Structure):
@@ -90,6 +152,20 @@ def lib() -> C.CDLL:
             "gdf_get_optimizer_state": [P, C.c_int32, P, P, P, C.c_int64, P],
             "gdf_set_optimizer_state": [P, C.c_int32, P, P, P, C.c_int64, C.c_uint32],
             "gdf_train_loss_static": [P, P, P, P, C.c_int64, P, P, P],
+            "gdf_infer_ex": [P, C.POINTER(InferArgs), P],
+            "gdf_prepare_queries": [C.POINTER(Shading), C.POINTER(Aabb), P, C.c_int64, P],
+            "gdf_build_train_records": [P, C.POINTER(PathState), C.POINTER(Aabb), C.POINTER(TrainPixels),
+                                        P, P, P, C.c_int64, C.POINTER(C.c_int64), P],
+            "gdf_build_nrc_records": [P, C.POINTER(PathState), C.POINTER(Aabb), C.POINTER(TrainPixels),
+                                      C.c_int32, P, P, P, C.c_int64, P, P, C.c_int64,
+                                      C.POINTER(C.c_int64 * 2), P],
+            "gdf_apply_nrc": [P, C.POINTER(PathState), P, P, P, C.c_int64, P],
+            "gdf_nrc_train_paths": [P, C.POINTER(PathState), C.POINTER(Aabb), C.POINTER(TrainPixels),
+                                    C.POINTER(C.c_float), C.POINTER(C.c_int64), P],
+            "gdf_nrc_substitute_paths": [P, C.POINTER(PathState), C.POINTER(Aabb),
+                                         C.POINTER(TrainPixels), C.c_int32, P],
+            "gdf_train_paths": [P, C.POINTER(PathState), C.POINTER(Aabb), C.POINTER(TrainPixels),
+                                C.POINTER(C.c_float), C.POINTER(C.c_int64), P],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -125,6 +201,17 @@ def _ptr(x):
     if hasattr(x, "ctypes"):
         return x.ctypes.data
     raise TypeError(type(x))
+
+
+def shading(pos, wo, normal, roughness) -> Shading:
+    sh = Shading(_ptr(pos), _ptr(wo), _ptr(normal), _ptr(roughness))
+    sh._keep = (pos, wo, normal, roughness)  # raw pointers into these tensors
+    return sh
+
+
+def prepare_queries(sh: Shading, aabb: Aabb, queries, n=None, stream=None):
+    n = queries.shape[0] if n is None else n
+    check(lib().gdf_prepare_queries(C.byref(sh), C.byref(aabb), _ptr(queries), n, _stream(stream)))
 
 
 def _stream(s):
@@ -214,6 +301,68 @@ class Context:
         check(lib().gdf_nrc_train_step(self.h, _ptr(inp), _ptr(target), n,
                                        C.byref(st) if stats else None, _stream(stream)))
         return st
+
+    def infer_ex(self, wi, n=None, queries=None, shading: "Shading | None" = None, aabb=None,
+                 guided=None, uniforms=None, seed=0, offset=0, dir_pdf=None, stream=None):
+        n = wi.shape[0] if n is None else n
+        a = InferArgs()
+        a.queries_dev = _ptr(queries)
+        a.shading = C.pointer(shading) if shading is not None else None
+        a._keep = shading
+        if aabb is not None:
+            a.aabb = aabb
+        a.guided_dev = _ptr(guided)
+        a.uniforms_dev = _ptr(uniforms)
+        a.philox_seed = seed
+        a.philox_offset = offset
+        a.wi_dev = _ptr(wi)
+        a.dir_pdf_dev = _ptr(dir_pdf)
+        a.n = n
+        check(lib().gdf_infer_ex(self.h, C.byref(a), _stream(stream)))
+
+    def build_train_records(self, st: PathState, aabb: Aabb, px: TrainPixels, in_theta, in_phi,
+                            target, capacity=None, stream=None) -> int:
+        cap = in_theta.shape[0] if capacity is None else capacity
+        cnt = C.c_int64()
+        check(lib().gdf_build_train_records(self.h, C.byref(st), C.byref(aabb), C.byref(px),
+                                            _ptr(in_theta), _ptr(in_phi), _ptr(target), cap,
+                                            C.byref(cnt), _stream(stream)))
+        return cnt.value
+
+    def build_nrc_records(self, st: PathState, aabb: Aabb, px: TrainPixels, with_training: bool,
+                          q_in, q_depth, q_pixel, t_in=None, t_target=None, stream=None):
+        counts = (C.c_int64 * 2)()
+        qcap = q_in.shape[0]
+        tcap = t_in.shape[0] if t_in is not None else 0
+        check(lib().gdf_build_nrc_records(self.h, C.byref(st), C.byref(aabb), C.byref(px),
+                                          int(with_training), _ptr(q_in), _ptr(q_depth),
+                                          _ptr(q_pixel), qcap, _ptr(t_in), _ptr(t_target), tcap,
+                                          C.byref(counts), _stream(stream)))
+        return counts[0], counts[1]
+
+    def apply_nrc(self, st: PathState, nrc_out, depth, pixel, m=None, stream=None):
+        m = depth.shape[0] if m is None else m
+        check(lib().gdf_apply_nrc(self.h, C.byref(st), _ptr(nrc_out), _ptr(depth), _ptr(pixel), m,
+                                  _stream(stream)))
+
+    def nrc_train_paths(self, st: PathState, aabb: Aabb, px: TrainPixels, stream=None):
+        loss = C.c_float()
+        n = C.c_int64()
+        check(lib().gdf_nrc_train_paths(self.h, C.byref(st), C.byref(aabb), C.byref(px),
+                                        C.byref(loss), C.byref(n), _stream(stream)))
+        return loss.value, n.value
+
+    def nrc_substitute_paths(self, st: PathState, aabb: Aabb, px: TrainPixels,
+                             skip_generation=False, stream=None):
+        check(lib().gdf_nrc_substitute_paths(self.h, C.byref(st), C.byref(aabb), C.byref(px),
+                                             int(skip_generation), _stream(stream)))
+
+    def train_paths(self, st: PathState, aabb: Aabb, px: TrainPixels, stream=None):
+        loss = C.c_float()
+        n = C.c_int64()
+        check(lib().gdf_train_paths(self.h, C.byref(st), C.byref(aabb), C.byref(px),
+                                    C.byref(loss), C.byref(n), _stream(stream)))
+        return loss.value, n.value
 
     def get_optimizer_state(self, net: int):
         import numpy as np

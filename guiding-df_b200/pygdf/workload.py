@@ -165,3 +165,64 @@ def nrc_batch(n: int, seed: int):
     field = VmfField(seed)
     y = field.radiance(rec["pos"], wo)
     return x, y
+
+
+def path_state(n_pixels: int, seed: int, aabb=((-2.0, -1.0, -3.0), (4.0, 2.0, 1.0)),
+               defects: bool = True) -> tuple[dict, np.ndarray]:
+    """Per-pixel vertex records of one frame, laid out like
+    GuidedPixelStateBuffer (workqueue.h:16-145, RadianceRecordItem in
+    guideditem.h:23-44): fields[name] is [MAX_TRAIN_DEPTH, n_pixels(, k)].
+
+    Path lengths follow a survival of 0.7 per bounce; about 15 % of the
+    vertices are delta-lobe samples and 5 % NRC alignment records of misses.
+    With `defects`, a few per mille of positions, directions and radiances
+    are NaN, some throughputs are below M_EPSILON and some pdfs are zero, so
+    the producers' filters are exercised."""
+    rng = np.random.default_rng(seed)
+    d, n = 5, n_pixels
+    lo = np.asarray(aabb[0], np.float32)
+    hi = np.asarray(aabb[1], np.float32)
+    f32 = np.float32
+
+    def sph(shape):
+        t = np.arccos(1.0 - 2.0 * rng.random(shape)).astype(f32)
+        p = (2.0 * np.pi * rng.random(shape)).astype(f32)
+        return np.stack([t, p], axis=-1)
+
+    thp = (0.05 + 0.95 * rng.random((d, n, 3))).astype(f32)
+    fields = {
+        # accumulated radiance carries the vertex throughput (recordRadiance,
+        # workqueue.h:84-92), so L / thp is a local radiance of order one
+        "L": (thp * rng.exponential(1.0, (d, n, 3))).astype(f32),
+        "thp": thp,
+        "Le": (0.1 * rng.random((d, n, 3))).astype(f32),
+        "pos": (lo + (hi - lo) * rng.random((d, n, 3))).astype(f32),
+        "dir": sph((d, n)),
+        "wi_pdf": (0.05 + 2.0 * rng.random((d, n))).astype(f32),
+        "mis_weight": rng.random((d, n), dtype=f32),
+        "delta": (rng.random((d, n)) < 0.15).astype(np.uint8),
+        "miss": (rng.random((d, n)) < 0.05).astype(np.uint8),
+        "bsdf_val": rng.random((d, n, 3), dtype=f32),
+        "wo": sph((d, n)),
+        "normal": sph((d, n)),
+        "roughness": rng.random((d, n), dtype=f32),
+        "diffuse": rng.random((d, n, 3), dtype=f32),
+        "specular": rng.random((d, n, 3), dtype=f32),
+    }
+    depth = np.zeros(n, np.uint32)
+    alive = np.ones(n, bool)
+    for k in range(d):
+        depth += alive
+        alive &= rng.random(n) < 0.7
+    if defects:
+        def poke(name, frac, value):
+            a = fields[name]
+            m = rng.random(a.shape[:2]) < frac
+            a[m] = value
+        poke("pos", 0.004, np.nan)
+        poke("dir", 0.003, np.nan)
+        poke("wo", 0.002, np.nan)
+        poke("L", 0.004, np.nan)
+        poke("thp", 0.02, 1e-6)
+        poke("wi_pdf", 0.01, 0.0)
+    return fields, depth

@@ -35,8 +35,10 @@
 extern "C" {
 #endif
 
-#define GDF_ABI_VERSION 1
+#define GDF_ABI_VERSION 2
 #define GDF_MAX_GRID_LEVELS 24
+/* MAX_TRAIN_DEPTH (parameters.h:24): path vertices recorded per pixel. */
+#define GDF_MAX_TRAIN_DEPTH 5
 
 typedef enum gdf_status {
   GDF_OK = 0,
@@ -106,6 +108,15 @@ typedef struct gdf_config {
   uint32_t seed;            /* parameter initialisation seed (7272)          */
   int64_t max_queries;      /* capacity of one inference call                */
   int64_t max_train_batch;  /* capacity of one training call                 */
+  /* Frame-level training loops (gdf_train_paths, gdf_nrc_train_paths):
+   * LearnedDistribution batchSize / batchPerFrame (learnedDistribution.h:138-139),
+   * NRC batchSize / batchPerFrame (nrc.h:80-81), MIN_TRAIN_BATCH_SIZE
+   * (parameters.h:55). Batch sizes must not exceed max_train_batch. */
+  int64_t df_batch_size;
+  int64_t nrc_batch_size;
+  int64_t min_train_batch;
+  int32_t df_batches_per_frame;
+  int32_t nrc_batches_per_frame;
 } gdf_config;
 
 typedef enum gdf_preset {
@@ -189,6 +200,45 @@ gdf_status gdf_infer(gdf_ctx* ctx, const float* queries_dev, const uint8_t* guid
                      const float* uniforms_dev, uint64_t philox_seed, uint64_t philox_offset,
                      float* wi_dev, int64_t n, void* stream);
 
+/* Scene bounds (krr AABB, aabb.h:11-33): positions are normalised by
+ * normalizeSpatialCoord (train.h:272-276) against this box inflated by
+ * 0.005 x its diagonal length. */
+typedef struct gdf_aabb {
+  float lo[3];
+  float hi[3];
+} gdf_aabb;
+
+/* Raw shading points of a wavefront (the ShadingData fields that
+ * generate_inference_data_AR, train.cu:334-362, reads). Device arrays. */
+typedef struct gdf_shading {
+  const float* pos;       /* [n x 3] world-space position (sd.pos)        */
+  const float* wo;        /* [n x 3] outgoing direction (sd.wo, any length) */
+  const float* normal;    /* [n x 3] shading normal (sd.frame.N)          */
+  const float* roughness; /* [n]     (sd.roughness)                        */
+} gdf_shading;
+
+/* gdf_infer with the optional stages either side of it:
+ *   - shading != NULL: the queries are built in-kernel from raw shading
+ *     points and `aabb` (generate_inference_data_AR, train.cu:334-362), so
+ *     the 9-float rows never reach memory; queries_dev is then ignored;
+ *   - dir_pdf_dev != NULL: also writes, per query, the consumer view of
+ *     the result (AutoRegressive, AR.h:25-48): the unit direction
+ *     squareToUniformSphere(u_theta, u_phi) (math_utils.h:226-231) and the
+ *     solid-angle pdf |wi[2]| * |wi[3]| / (4 pi), as [x, y, z, pdf]. */
+typedef struct gdf_infer_args {
+  const float* queries_dev;
+  const gdf_shading* shading;
+  gdf_aabb aabb;
+  const uint8_t* guided_dev;
+  const float* uniforms_dev;
+  uint64_t philox_seed;
+  uint64_t philox_offset;
+  float* wi_dev;
+  float* dir_pdf_dev;
+  int64_t n;
+} gdf_infer_args;
+gdf_status gdf_infer_ex(gdf_ctx* ctx, const gdf_infer_args* args, void* stream);
+
 /* compute_AR_pdf_combined_F (train.h:730-751) for given square directions:
  * pdf_out_dev[i] = {pdf_theta(u[i].x), pdf_phi(u[i].y)} of the learned
  * distribution at query i (the phi net is conditioned on u[i].x). */
@@ -261,6 +311,110 @@ gdf_status gdf_nrc_query(gdf_ctx* ctx, const float* in_dev, float* out_dev, int6
  * Adam + EMA. target [m x 3] fp32. */
 gdf_status gdf_nrc_train_step(gdf_ctx* ctx, const float* in_dev, const float* target_dev,
                               int64_t m, gdf_train_stats* stats_host, void* stream);
+
+/* ------------------------------------------- records from the path tracer */
+
+/* One depth of GuidedPixelStateBuffer (workqueue.h:16-145): the
+ * RadianceRecordItem fields (guideditem.h:23-44) as device arrays indexed
+ * by pixel id. Angles are (theta, phi) in radians as the reference stores
+ * them. L is read and written (NRC target substitution); the rest is read. */
+typedef struct gdf_record_fields {
+  float* L;                 /* [n x 3] accumulated radiance               */
+  const float* thp;         /* [n x 3] throughput                          */
+  const float* Le;          /* [n x 3] emission at the vertex              */
+  const float* pos;         /* [n x 3] world-space vertex position         */
+  const float* dir;         /* [n x 2] scattered direction wi              */
+  const float* wi_pdf;      /* [n]     pdf of wi                            */
+  const float* mis_weight;  /* [n]                                          */
+  const uint8_t* delta;     /* [n]     sampled from a delta lobe           */
+  const uint8_t* miss;      /* [n]     NRC alignment record of a miss      */
+  const float* bsdf_val;    /* [n x 3]                                      */
+  const float* wo;          /* [n x 2] outgoing direction                  */
+  const float* normal;      /* [n x 2] shading normal                      */
+  const float* roughness;   /* [n]                                          */
+  const float* diffuse;     /* [n x 3]                                      */
+  const float* specular;    /* [n x 3]                                      */
+} gdf_record_fields;
+
+typedef struct gdf_path_state {
+  gdf_record_fields depth[GDF_MAX_TRAIN_DEPTH];
+  uint32_t* cur_depth;      /* [n] curDepth; NRC record building decrements it */
+} gdf_path_state;
+
+/* The training pixels of a frame: pixel = offset + i * stride for
+ * i < max_queue_size / stride (learnedDistribution.cpp:218-222). */
+typedef struct gdf_train_pixels {
+  int64_t max_queue_size;
+  uint32_t offset;  /* trainPixelOffset */
+  uint32_t stride;  /* trainPixelStride, >= 1 */
+} gdf_train_pixels;
+
+/* generate_inference_data_AR (train.cu:334-362) alone: shading points ->
+ * the 9-float query rows described at the top of this file. */
+gdf_status gdf_prepare_queries(const gdf_shading* shading, const gdf_aabb* aabb,
+                               float* queries_dev, int64_t n, void* stream);
+
+/* generate_training_data_AR (train.cu:6-96): one GuidedInput,
+ * GuidedInputPhi and GuidedOutput per non-delta, finite vertex of each
+ * training pixel. Records are ordered by training pixel, then depth (the
+ * reference appends them atomically in no fixed order). At most `capacity`
+ * records are written; *count_host receives the full count and
+ * GDF_ERR_INVALID_ARG is returned when it exceeds capacity. Synchronises. */
+gdf_status gdf_build_train_records(gdf_ctx* ctx, const gdf_path_state* state, const gdf_aabb* aabb,
+                                   const gdf_train_pixels* px, float* in_theta_dev,
+                                   float* in_phi_dev, float* target_dev, int64_t capacity,
+                                   int64_t* count_host, void* stream);
+
+/* NRC record building, ordered like gdf_build_train_records:
+ *   with_training = 1: generate_training_data_nrc_with_inference
+ *     (train.cu:156-214): query rows for every non-delta, non-miss vertex and
+ *     training rows (GuidedInputNRC + RGB target) for all but the last;
+ *   with_training = 0: generate_NRCinput_from_training_data
+ *     (train.cu:216-262): query rows only.
+ * Both decrement cur_depth of every training pixel, like the reference.
+ * query_depth/query_pixel receive each query row's depth and pixel id.
+ * counts_host[0] = query rows, counts_host[1] = training rows. Synchronises. */
+gdf_status gdf_build_nrc_records(gdf_ctx* ctx, gdf_path_state* state, const gdf_aabb* aabb,
+                                 const gdf_train_pixels* px, int32_t with_training,
+                                 float* query_in_dev, int32_t* query_depth_dev,
+                                 int32_t* query_pixel_dev, int64_t query_capacity,
+                                 float* train_in_dev, float* train_target_dev,
+                                 int64_t train_capacity, int64_t* counts_host, void* stream);
+
+/* apply_NRCoutput_to_training_data + divide_training_data_by_NRCoutput
+ * (train.cu:265-308) for OPTIMIZE_ON_NRC 4 (parameters.h:19): for every
+ * query row (depth d, pixel p, NRC output o), first
+ *   replaceIndirectRadianceSkipDelta(p, d-1, o)   (workqueue.h:122-129)
+ * for all rows, then divideRadiance(p, d, o) (workqueue.h:104-111). Rows
+ * may come in any order. */
+gdf_status gdf_apply_nrc(gdf_ctx* ctx, gdf_path_state* state, const float* nrc_out_dev,
+                         const int32_t* query_depth_dev, const int32_t* query_pixel_dev,
+                         int64_t m, void* stream);
+
+/* NRC::trainStep (nrc.cpp:114-170): builds the NRC query and training rows
+ * into library buffers (with_training = 1 above, cur_depth decremented),
+ * then runs its batch loop of gdf_nrc_train_step. *loss_host = the mean of
+ * the batch losses over the loop's batch count; *n_samples_host = training
+ * rows. The query rows are kept for gdf_nrc_substitute_paths. Synchronises. */
+gdf_status gdf_nrc_train_paths(gdf_ctx* ctx, gdf_path_state* state, const gdf_aabb* aabb,
+                               const gdf_train_pixels* px, float* loss_host,
+                               int64_t* n_samples_host, void* stream);
+
+/* NRC::inferenceStepFromTrainingData (nrc.cpp:183-217): builds the query
+ * rows unless skip_generation (then the rows of the last
+ * gdf_nrc_train_paths are used), queries the NRC and substitutes the
+ * targets in state (gdf_apply_nrc). Synchronises. */
+gdf_status gdf_nrc_substitute_paths(gdf_ctx* ctx, gdf_path_state* state, const gdf_aabb* aabb,
+                                    const gdf_train_pixels* px, int32_t skip_generation,
+                                    void* stream);
+
+/* LearnedDistribution::trainStep (learnedDistribution.cpp:208-293): builds
+ * the records (gdf_build_train_records) into library buffers and runs the
+ * batch loop of gdf_train_step. *loss_host = sum of batch losses / batch
+ * count; *n_samples_host = records built. Synchronises. */
+gdf_status gdf_train_paths(gdf_ctx* ctx, const gdf_path_state* state, const gdf_aabb* aabb,
+                           const gdf_train_pixels* px, float* loss_host, int64_t* n_samples_host,
+                           void* stream);
 
 /* ----------------------------------------------------------------- errors */
 

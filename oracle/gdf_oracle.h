@@ -132,6 +132,29 @@ void go_df_pdf_tables(const go_df_config* c, const float* p_theta, const float* 
 void go_nrc_query(const go_nrc_config* c, const float* params16, const float* in15, float* out3,
                   int64_t m, int n_threads);
 
+
+/* ---- path records (gdf_oracle_paths.c) ---------------------------------- */
+/* Host copy of GuidedPixelStateBuffer: each field is [5][n][k] (depth-major). */
+typedef struct go_paths {
+  int64_t n; /* pixels */
+  float *L, *thp, *Le, *pos, *dir, *wi_pdf, *mis_weight;
+  uint8_t *delta, *miss;
+  float *bsdf_val, *wo, *normal, *roughness, *diffuse, *specular;
+  uint32_t* cur_depth;
+} go_paths;
+
+void go_prepare_queries(const float* pos, const float* wo, const float* nrm, const float* rough,
+                        const float aabb[6], float* q, int64_t n);
+int64_t go_build_df_records(const go_paths* s, const float aabb[6], int64_t n_train, uint32_t offset,
+                            uint32_t stride, int bins, int linear, float* in, float* in_phi,
+                            float* target, int64_t cap);
+void go_build_nrc_records(go_paths* s, const float aabb[6], int64_t n_train, uint32_t offset,
+                          uint32_t stride, int with_training, float* q_in, int32_t* q_depth,
+                          int32_t* q_pixel, int64_t q_cap, float* t_in, float* t_target,
+                          int64_t t_cap, int64_t* counts);
+void go_apply_nrc(go_paths* s, const float* out, const int32_t* depth, const int32_t* pixel,
+                  int64_t m);
+
 #ifdef __cplusplus
 }
 #endif

@@ -16,7 +16,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 BUILD = os.path.join(HERE, "_build")
 SO = os.path.join(BUILD, "libgdf_oracle.so")
-SRCS = [os.path.join(HERE, "gdf_oracle.c"), os.path.join(HERE, "gdf_oracle_train.c")]
+SRCS = [os.path.join(HERE, "gdf_oracle.c"), os.path.join(HERE, "gdf_oracle_train.c"),
+        os.path.join(HERE, "gdf_oracle_paths.c")]
 HDR = os.path.join(HERE, "gdf_oracle.h")
 
 
@@ -355,3 +356,83 @@ def nrc_train_grads(nc: NrcCfg, w, inp, target, loss_scale=1024.0):
     loss = np.empty(m, np.float32)
     lib().go_nrc_train_grads(C.byref(nc), _p(w16), _p(x), _p(y), m, loss_scale, _p(g), _p(loss))
     return g, loss
+
+
+# ---- path records (gdf_oracle_paths.c) ------------------------------------
+
+PATH_FIELDS = ["L", "thp", "Le", "pos", "dir", "wi_pdf", "mis_weight", "delta", "miss", "bsdf_val",
+               "wo", "normal", "roughness", "diffuse", "specular"]
+
+
+class GoPaths(C.Structure):
+    _fields_ = [("n", C.c_int64)] + [(f, C.c_void_p) for f in PATH_FIELDS] + [("cur_depth", C.c_void_p)]
+
+
+def _paths(fields: dict, cur_depth: np.ndarray):
+    """go_paths over numpy arrays (modified in place by the oracle)."""
+    s = GoPaths()
+    s.n = cur_depth.shape[0]
+    for f in PATH_FIELDS:
+        a = fields[f]
+        assert a.flags.c_contiguous
+        setattr(s, f, a.ctypes.data)
+    s.cur_depth = cur_depth.ctypes.data
+    return s
+
+
+def _aabb6(aabb):
+    return (C.c_float * 6)(*[float(x) for x in list(aabb[0]) + list(aabb[1])])
+
+
+def prepare_queries(pos, wo, nrm, rough, aabb):
+    n = pos.shape[0]
+    q = np.empty((n, 9), np.float32)
+    L = lib()
+    L.go_prepare_queries.argtypes = [C.c_void_p] * 4 + [C.c_void_p, C.c_void_p, C.c_int64]
+    p, w, m, r = f32(pos), f32(wo), f32(nrm), f32(rough)
+    L.go_prepare_queries(_p(p), _p(w), _p(m), _p(r), _aabb6(aabb), _p(q), n)
+    return q
+
+
+def build_df_records(fields, cur_depth, aabb, n_train, offset, stride, bins, linear):
+    cap = n_train * 5
+    a = np.empty((cap, 9), np.float32)
+    b = np.empty((cap, 10), np.float32)
+    t = np.empty((cap, 9), np.float32)
+    L = lib()
+    L.go_build_df_records.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_uint32, C.c_uint32,
+                                      C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64]
+    L.go_build_df_records.restype = C.c_int64
+    s = _paths(fields, cur_depth)
+    k = L.go_build_df_records(C.byref(s), _aabb6(aabb), n_train, offset, stride, bins, int(linear),
+                              _p(a), _p(b), _p(t), cap)
+    return a[:k], b[:k], t[:k]
+
+
+def build_nrc_records(fields, cur_depth, aabb, n_train, offset, stride, with_training):
+    """Returns dict(q_in, q_depth, q_pixel, t_in, t_target); decrements cur_depth in place."""
+    cap = n_train * 5
+    q = np.empty((cap, 15), np.float32)
+    qd = np.empty(cap, np.int32)
+    qp = np.empty(cap, np.int32)
+    ti = np.empty((cap, 15), np.float32)
+    tt = np.empty((cap, 3), np.float32)
+    counts = (C.c_int64 * 2)()
+    L = lib()
+    L.go_build_nrc_records.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_uint32, C.c_uint32,
+                                       C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
+                                       C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]
+    s = _paths(fields, cur_depth)
+    L.go_build_nrc_records(C.byref(s), _aabb6(aabb), n_train, offset, stride, int(with_training),
+                           _p(q), _p(qd), _p(qp), cap, _p(ti), _p(tt), cap, counts)
+    kq, kt = counts[0], counts[1]
+    return dict(q_in=q[:kq], q_depth=qd[:kq], q_pixel=qp[:kq], t_in=ti[:kt], t_target=tt[:kt])
+
+
+def apply_nrc(fields, cur_depth, out, depth, pixel):
+    """Modifies fields['L'] in place."""
+    L = lib()
+    L.go_apply_nrc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64]
+    s = _paths(fields, cur_depth)
+    o, d, p = f32(out), np.ascontiguousarray(depth, np.int32), np.ascontiguousarray(pixel, np.int32)
+    L.go_apply_nrc(C.byref(s), _p(o), _p(d), _p(p), o.shape[0])
