@@ -160,7 +160,10 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="CPU-baseline sample length; 0 skips it (profiling runs)")
     ap.add_argument("--skip-e2e", action="store_true", help="profiling runs: kernel timing only")
+    ap.add_argument("--stages", default="infer,train,records",
+                    help="comma list of infer, train, records (profiling runs select one)")
     args = ap.parse_args()
+    stages = set(args.stages.split(","))
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -270,6 +273,22 @@ def main():
             e2e_times.append(s.elapsed_time(e))
     # ---- training step (gdf_train_step on one batch of synthetic records)
     nb = TRAIN_BATCH[args.workload]
+    train_times, rec_times, last, n_rec, rec_bytes = [], [], None, 0, 0
+    if "train" in stages:
+        train_times, last = time_train(ctx, cfg, W, nb, rank, dev, stream, flush, args)
+    if "records" in stages:
+        rec_times, n_rec, rec_bytes = time_records(ctx, W, n, rank, dev, stream, flush, args)
+    clk = clocks.stop()
+    ctx.sync(stream)
+    _report(args, rank, world, dist, dev, n, cfg, params, times, e2e_times, train_times, rec_times,
+            last, n_rec, rec_bytes, clk, nb, workload_name, threads, q_h, wi_h, guided_h)
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+def time_train(ctx, cfg, W, nb, rank, dev, stream, flush, args):
+    import torch
     ta, tb, tt = W.training_batch(nb, 77 + rank, cfg.n_bins_theta)
     da, db, dt = (torch.from_numpy(x).to(dev) for x in (ta, tb, tt))
     for _ in range(args.warmup):
@@ -285,8 +304,12 @@ def main():
         e.synchronize()
         train_times.append(s.elapsed_time(e))
     last = ctx.train_step(da, db, dt, stream=stream, stats=True)
-    del da, db, dt
-    # ---- training-record producer (gdf_build_train_records) over one frame
+    return train_times, last
+
+
+def time_records(ctx, W, n, rank, dev, stream, flush, args):
+    """training-record producer (gdf_build_train_records) over one frame"""
+    import torch
     import pygdf
     n_px = n
     fields, depth = W.path_state(n_px, 91 + rank)
@@ -313,17 +336,20 @@ def main():
     visit = np.arange(5)[:, None] < depth[None, :].astype(np.int64)
     nondelta = visit & (fields["delta"] == 0)
     rec_bytes = 4 * n_px + int(visit.sum()) + 84 * int(nondelta.sum()) + 112 * n_rec
-    del fd, cd, st, ra, rb, rt
-    clk = clocks.stop()
-    ctx.sync(stream)
+    return rec_times, n_rec, rec_bytes
 
+
+def _report(args, rank, world, dist, dev, n, cfg, params, times, e2e_times, train_times, rec_times,
+            last, n_rec, rec_bytes, clk, nb, workload_name, threads, q_h, wi_h, guided_h):
+    import torch
     ms = statistics.mean(times)
     ms_e2e = statistics.mean(e2e_times) if e2e_times else float("nan")
-    ms_train = statistics.mean(train_times)
+    ms_train = statistics.mean(train_times) if train_times else float("nan")
+    ms_rec = statistics.mean(rec_times) if rec_times else float("nan")
     if dist:
-        t = torch.tensor([ms, ms_e2e, ms_train], dtype=torch.float64, device=dev)
+        t = torch.tensor([ms, ms_e2e, ms_train, ms_rec], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, ms_e2e, ms_train = float(t[0]), float(t[1]), float(t[2])
+        ms, ms_e2e, ms_train, ms_rec = (float(x) for x in t)
     value = n * world / (ms * 1e-3)
     e2e_value = n * world / (ms_e2e * 1e-3)
     h2d = q_h.nbytes + wi_h.nbytes + guided_h.nbytes
@@ -332,7 +358,7 @@ def main():
     if rank == 0:
         peaks = load_peaks()
         flops = FLOP_PER_QUERY[args.workload] * n
-        achieved = flops / (min(times) * 1e-3) / 1e12
+        achieved = flops / (ms * 1e-3) / 1e12  # average launch duration
         traffic = None
         prof = os.path.join(ROOT, "profiles", f"df_fused_{args.workload}.json")
         if os.path.exists(prof):
@@ -355,24 +381,26 @@ def main():
                          "flop_per_query": FLOP_PER_QUERY[args.workload]},
             "cpu_baseline": {"value": cpu_v, "unit": "queries/s", "cores": threads, "kind": "port",
                              "sample": f"{cpu_n} queries ({cpu_s:.1f} s) of the same workload"},
-            "train": {"metric": "train samples/s", "value": nb * world / (ms_train * 1e-3),
-                      "unit": "records/s", "batch": nb, "ms_per_step": ms_train,
-                      "achieved_tflops": TRAIN_FLOP_PER_RECORD[args.workload] * nb / (ms_train * 1e-3) / 1e12,
-                      "loss": last.loss, "launches_per_step": 6},
-            "records": {"metric": "training records/s (generate_training_data_AR)",
-                        "value": n_rec * world / (statistics.mean(rec_times) * 1e-3), "unit": "records/s",
-                        "pixels": n_px, "records": n_rec, "ms_per_step": statistics.mean(rec_times),
-                        "algorithmic_bytes": rec_bytes,
-                        "achieved_gbs": rec_bytes / (min(rec_times) * 1e-3) / 1e9,
-                        "frac_hbm": rec_bytes / (min(rec_times) * 1e-3) / 1e9 / peaks["hbm_gbs"],
-                        "launches_per_step": 3},
-            "clocks": clk,
-            "gpu_launches": args.steps,
         }
+        if train_times:
+            line["train"] = {
+                "metric": "train samples/s", "value": nb * world / (ms_train * 1e-3),
+                "unit": "records/s", "batch": nb, "ms_per_step": ms_train,
+                "achieved_tflops": TRAIN_FLOP_PER_RECORD[args.workload] * nb / (ms_train * 1e-3) / 1e12,
+                "loss": last.loss, "launches_per_step": 6}
+        if rec_times:
+            line["records"] = {
+                "metric": "training records/s (generate_training_data_AR)",
+                "value": n_rec * world / (ms_rec * 1e-3), "unit": "records/s",
+                "pixels": n, "records": n_rec, "ms_per_step": ms_rec, "algorithmic_bytes": rec_bytes,
+                "achieved_gbs": rec_bytes / (ms_rec * 1e-3) / 1e9,
+                "frac_hbm": rec_bytes / (ms_rec * 1e-3) / 1e9 / peaks["hbm_gbs"],
+                "launches_per_step": 3}
+        line.update({
+            "clocks": clk,
+            "gpu_launches": 2 * args.steps,  # grid features + fused kernel per step
+        })
         print(json.dumps(line), flush=True)
-    ctx.close()
-    if dist:
-        dist.destroy_process_group()
 
 
 if __name__ == "__main__":

@@ -27,6 +27,7 @@ COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-I", os.path
 # (source, extra flags)
 SOURCES = [
     ("kernels/df_fused.cu", ["-fmad=false"]),
+    ("kernels/grid_features.cu", ["-fmad=false"]),
     ("kernels/df_train.cu", ["-fmad=false"]),
     ("kernels/loss_static.cu", []),
     ("kernels/nrc.cu", ["-fmad=false"]),

@@ -428,6 +428,59 @@ gdf_status gdf_default_config(int32_t preset, gdf_config* cfg) {
   return GDF_OK;
 }
 
+}  // extern "C"
+
+static gdf::DfShape df_shape(const Context& c) {
+  return gdf::DfShape{c.cfg.grid_theta.n_levels, c.cfg.grid_theta.n_features_per_level,
+                      c.cfg.n_bins_theta, c.cfg.n_bins_phi, c.cfg.pdf_interp == GDF_PDF_LINEAR};
+}
+
+static int64_t feat_row_halves(const Context& c) {
+  return static_cast<int64_t>(c.cfg.grid_theta.n_levels) * c.cfg.grid_theta.n_features_per_level;
+}
+
+// Grows the grid-feature buffer to n_tiles 128-row tiles per network.
+static gdf_status ensure_features(Context& c, int64_t n_tiles) {
+  if (n_tiles <= c.feat_tiles) return GDF_OK;
+  cudaFree(c.feat);
+  c.feat = nullptr;
+  c.feat_tiles = 0;
+  gdf_status s = dalloc(&c.feat, static_cast<size_t>(2 * n_tiles * 128 * feat_row_halves(c)));
+  if (s) return s;
+  c.feat_tiles = n_tiles;
+  return GDF_OK;
+}
+
+// Both grids' features of n queries (query rows, or shading positions with
+// aabb) into the context's buffer; points p at them.
+static gdf_status grid_features(Context& c, const float* queries, const gdf_shading* sh,
+                                const gdf_aabb& aabb, int64_t n, gdf::DfKernelParams& p,
+                                cudaStream_t st) {
+  const int64_t tiles = (n + 127) / 128;
+  gdf_status s = ensure_features(c, tiles);
+  if (s) return s;
+  gdf::GridFeatParams g;
+  std::memset(&g, 0, sizeof(g));
+  g.queries = queries;
+  g.shading_pos = sh ? sh->pos : nullptr;
+  g.aabb = aabb;
+  g.n = n;
+  g.n_tiles = tiles;
+  g.grid_theta = p.grid_theta;
+  g.grid_phi = p.grid_phi;
+  g.gl_theta = p.gl_theta;
+  g.gl_phi = p.gl_phi;
+  g.feat_theta = c.feat;
+  g.feat_phi = c.feat + c.feat_tiles * 128 * feat_row_halves(c);
+  cudaError_t e = gdf::launch_grid_features(df_shape(c), g, st);
+  if (e != cudaSuccess) return cuda_fail(e, "grid_features");
+  p.feat_theta = g.feat_theta;
+  p.feat_phi = g.feat_phi;
+  return GDF_OK;
+}
+
+extern "C" {
+
 gdf_status gdf_create(const gdf_config* cfg, gdf_ctx** out) {
   if (!cfg || !out) return fail(GDF_ERR_INVALID_ARG, "null argument");
   *out = nullptr;
@@ -444,6 +497,7 @@ gdf_status gdf_create(const gdf_config* cfg, gdf_ctx** out) {
     for (Net& n : c.net) free_net(n);
     free_ws(c.ws);
     free_pw(c.pw);
+    cudaFree(c.feat);
     cudaFree(c.d_err);
     delete h;
     return st;
@@ -455,6 +509,8 @@ gdf_status gdf_create(const gdf_config* cfg, gdf_ctx** out) {
     if (n.present && (s = alloc_net(n))) return cleanup(s);
   if ((s = dalloc(&c.d_err, 1))) return cleanup(s);
   if ((s = alloc_ws(c))) return cleanup(s);
+  if (c.cfg.max_queries > 0 && (s = ensure_features(c, (c.cfg.max_queries + 127) / 128)))
+    return cleanup(s);
   e = cudaMemset(c.d_err, 0, 4);
   if (e != cudaSuccess) return cleanup(cuda_fail(e, "cudaMemset"));
   for (int i = 0; i < 3; ++i)
@@ -470,6 +526,7 @@ gdf_status gdf_destroy(gdf_ctx* ctx) {
   for (Net& n : ctx->c.net) free_net(n);
   free_ws(ctx->c.ws);
   free_pw(ctx->c.pw);
+  cudaFree(ctx->c.feat);
   cudaFree(ctx->c.d_err);
   delete ctx;
   return GDF_OK;
@@ -574,10 +631,7 @@ static gdf::DfKernelParams df_params(Context& c) {
   return p;
 }
 
-static gdf::DfShape df_shape(const Context& c) {
-  return gdf::DfShape{c.cfg.grid_theta.n_levels, c.cfg.grid_theta.n_features_per_level,
-                      c.cfg.n_bins_theta, c.cfg.n_bins_phi, c.cfg.pdf_interp == GDF_PDF_LINEAR};
-}
+
 
 gdf_status gdf_infer(gdf_ctx* ctx, const float* queries, const uint8_t* guided,
                      const float* uniforms, uint64_t philox_seed, uint64_t philox_offset,
@@ -599,6 +653,8 @@ gdf_status gdf_infer(gdf_ctx* ctx, const float* queries, const uint8_t* guided,
   p.n = n;
   p.philox_seed = philox_seed;
   p.philox_offset = philox_offset;
+  if ((s = grid_features(ctx->c, queries, nullptr, gdf_aabb{}, n, p, static_cast<cudaStream_t>(stream))))
+    return s;
   cudaError_t e = gdf::launch_df_fused(df_shape(ctx->c), gdf::kModeInfer, p, ctx->c.num_sms,
                                        static_cast<cudaStream_t>(stream));
   if (e != cudaSuccess) return cuda_fail(e, "df_fused (infer)");
@@ -637,6 +693,9 @@ gdf_status gdf_infer_ex(gdf_ctx* ctx, const gdf_infer_args* a, void* stream) {
   p.n = n;
   p.philox_seed = a->philox_seed;
   p.philox_offset = a->philox_offset;
+  if ((s = grid_features(ctx->c, a->queries_dev, a->shading, a->aabb, n, p,
+                         static_cast<cudaStream_t>(stream))))
+    return s;
   cudaError_t e = gdf::launch_df_fused(df_shape(ctx->c), gdf::kModeInfer, p, ctx->c.num_sms,
                                        static_cast<cudaStream_t>(stream));
   if (e != cudaSuccess) return cuda_fail(e, "df_fused (infer)");
@@ -657,6 +716,8 @@ gdf_status gdf_eval_pdf(gdf_ctx* ctx, const float* queries, const float* u, floa
   p.u_eval = u;
   p.pdf_out = pdf_out;
   p.n = n;
+  if ((s = grid_features(ctx->c, queries, nullptr, gdf_aabb{}, n, p, static_cast<cudaStream_t>(stream))))
+    return s;
   cudaError_t e = gdf::launch_df_fused(df_shape(ctx->c), gdf::kModeEval, p, ctx->c.num_sms,
                                        static_cast<cudaStream_t>(stream));
   if (e != cudaSuccess) return cuda_fail(e, "df_fused (eval)");

@@ -41,6 +41,11 @@ struct DfWidths {
   static constexpr int kTheta = pad16c(kGrid + 16 + 12);
   static constexpr int kPhi = pad16c(kGrid + 16 + 12 + 12);
   static constexpr int kMax = kPhi > 64 ? kPhi : 64;
+  // columns of the per-warpgroup A tile: first-layer segment(s) and the
+  // 64-wide hidden activations
+  __host__ __device__ static constexpr uint32_t tile_a(uint32_t a, uint32_t b) {
+    return a > 64u ? (a > b ? a : b) : (64u > b ? 64u : b);
+  }
 };
 
 // ---------------------------------------------------------------------------
@@ -58,8 +63,13 @@ __global__ void __launch_bounds__(128 * WGS, 1) df_fused_kernel(const __grid_con
   constexpr uint32_t LF = L * F;
   constexpr uint32_t KT = Wd::kTheta;            // theta input width
   constexpr uint32_t KR = Wd::kPhi - LF;         // phi input minus its grid part
-  constexpr uint32_t KA = KT > 64 ? (KT > KR ? KT : KR) : (64 > KR ? 64 : KR);
-  static_assert(LF % 16 == 0 && KT % 16 == 0 && KR % 16 == 0, "K segments must be multiples of 16");
+  constexpr uint32_t KTR = KT - LF;              // theta input minus its grid part
+  // Inference and pdf evaluation read both grids' features precomputed
+  // (launch_grid_features); the training forward gathers them itself.
+  constexpr bool kFeat = MODE != kModeTrainFwd;
+  constexpr uint32_t KA = kFeat ? DfWidths<L, F>::tile_a(KTR, KR) : DfWidths<L, F>::tile_a(KT, KR);
+  static_assert(LF % 16 == 0 && KT % 16 == 0 && KR % 16 == 0 && KTR % 16 == 0,
+                "K segments must be multiples of 16");
   extern __shared__ __align__(1024) uint8_t smem[];
   const uint32_t tid = threadIdx.x;
   const uint32_t wg = tid >> 7;
@@ -68,9 +78,11 @@ __global__ void __launch_bounds__(128 * WGS, 1) df_fused_kernel(const __grid_con
   const uint32_t off_phi = (p.blob_theta_bytes + 127u) & ~127u;
   const uint32_t off_tiles = (off_phi + p.blob_phi_bytes + 127u) & ~127u;
   constexpr uint32_t kTileA = 128u * KA * 2u, kTileP = 128u * LF * 2u;
-  const uint32_t off_bars = off_tiles + WGS * (kTileA + kTileP);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + off_bars);  // [0] weights, [1+g] MMA
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + off_bars + 8 * (WGS + 1));
+  constexpr uint32_t kWgBytes = kTileA + (kFeat ? 2u : 1u) * kTileP;
+  const uint32_t off_bars = off_tiles + WGS * kWgBytes;
+  // [0] weights, [1+g] MMA of warpgroup g, [1+WGS+g] its feature tiles
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + off_bars);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + off_bars + 8 * (2 * WGS + 1));
   constexpr uint32_t kTmemCols = 64 * WGS <= 128 ? 128 : (64 * WGS <= 256 ? 256 : 512);
 
   if (warp == 0) {
@@ -78,7 +90,7 @@ __global__ void __launch_bounds__(128 * WGS, 1) df_fused_kernel(const __grid_con
     tmem_relinquish();
   }
   if (tid == 0) {
-    for (int i = 0; i <= WGS; ++i) mbar_init(&bars[i], 1);
+    for (int i = 0; i <= 2 * WGS; ++i) mbar_init(&bars[i], 1);
     fence_mbar_init();
     mbar_arrive_expect_tx(&bars[0], p.blob_theta_bytes + p.blob_phi_bytes);
     for (uint32_t o = 0; o < p.blob_theta_bytes; o += 32768u)
@@ -95,10 +107,14 @@ __global__ void __launch_bounds__(128 * WGS, 1) df_fused_kernel(const __grid_con
   mbar_wait(&bars[0], 0, p.err, kErrWeightLoad);
 
   tile::Wg c;
-  c.tile_a = smem + off_tiles + wg * (kTileA + kTileP);
+  c.tile_a = smem + off_tiles + wg * kWgBytes;
   c.tile_a_s = smem_addr(c.tile_a);
   c.tile_p = c.tile_a + kTileA;
   c.tile_p_s = c.tile_a_s + kTileA;
+  uint8_t* const tile_gt = c.tile_p + kTileP;  // theta grid features (kFeat)
+  const uint32_t tile_gt_s = c.tile_p_s + kTileP;
+  uint64_t* const fbar = &bars[1 + WGS + wg];
+  uint32_t fphase = 0;
   c.tmem = tmem_base + wg * 64u;
   c.lane_base = ((warp & 3u) * 32u) << 16;
   c.bar = &bars[1 + wg];
@@ -113,6 +129,17 @@ __global__ void __launch_bounds__(128 * WGS, 1) df_fused_kernel(const __grid_con
   const uint32_t w_phi_hidden = w_phi + 64u * (LF + KR) * 2u;
 
   const int64_t n_tiles = (p.n + 127) / 128;
+  // Both feature tiles of tile t, one bulk copy each, completing on fbar.
+  auto fetch_features = [&](int64_t t) {
+    if (!c.leader) return;
+    mbar_arrive_expect_tx(fbar, 2u * kTileP);
+    bulk_g2s(tile_gt, p.feat_theta + t * (128 * LF), kTileP, fbar);
+    bulk_g2s(c.tile_p, p.feat_phi + t * (128 * LF), kTileP, fbar);
+  };
+  if constexpr (kFeat) {
+    const int64_t t0 = static_cast<int64_t>(blockIdx.x) * WGS + wg;
+    if (t0 < n_tiles) fetch_features(t0);
+  }
   for (int64_t t = static_cast<int64_t>(blockIdx.x) * WGS + wg; t < n_tiles;
        t += static_cast<int64_t>(gridDim.x) * WGS) {
     const int64_t row = t * 128 + c.row;
@@ -160,13 +187,22 @@ __global__ void __launch_bounds__(128 * WGS, 1) df_fused_kernel(const __grid_con
       for (int i = 0; i < 9; ++i) qp[i] = q[i];
     }
 
-    // ---- 1. both grids (theta -> tile A, phi -> tile P), theta input rest, layer 0
-    tile::grids_to_tiles<L, F>(p.gl_theta, p.grid_theta, p.gl_phi, p.grid_phi, q, qp, c.tile_a, KT,
-                               c.tile_p, c.row);
-    tile::sh_ob_to_tile(q, c.tile_a, c.row, LF, KT);
-    tile::ones_to_tile(c.tile_a, c.row, LF + 28, KT, KT);
-    tile::publish(c);
-    {
+    // ---- 1. theta input (grid features | SH | OneBlob | 1-pad), layer 0
+    if constexpr (kFeat) {
+      tile::sh_ob_to_tile(q, c.tile_a, c.row, 0, KTR);
+      tile::ones_to_tile(c.tile_a, c.row, 28, KTR, KTR);
+      mbar_wait(fbar, fphase, p.err, kErrMbarTimeout);
+      fphase ^= 1u;
+      tile::publish(c);
+      const tile::ASeg a[2] = {{tile_gt_s, LF, static_cast<int>(LF / 16)},
+                               {c.tile_a_s, KTR, static_cast<int>(KTR / 16)}};
+      tile::issue(c, a, 2, w_theta, KT, 64);
+    } else {
+      tile::grids_to_tiles<L, F>(p.gl_theta, p.grid_theta, p.gl_phi, p.grid_phi, q, qp, c.tile_a, KT,
+                                 c.tile_p, c.row);
+      tile::sh_ob_to_tile(q, c.tile_a, c.row, LF, KT);
+      tile::ones_to_tile(c.tile_a, c.row, LF + 28, KT, KT);
+      tile::publish(c);
       const tile::ASeg a{c.tile_a_s, KT, static_cast<int>(KT / 16)};
       tile::issue(c, &a, 1, w_theta, KT, 64);
     }
@@ -223,6 +259,11 @@ __global__ void __launch_bounds__(128 * WGS, 1) df_fused_kernel(const __grid_con
     }
     // ---- 6. phi layers and epilogue
     tile::mlp_tail(c, w_phi_hidden, p.hidden_phi, NBP);
+    if constexpr (kFeat) {
+      // every MMA that read this tile's feature tiles has completed
+      const int64_t next = t + static_cast<int64_t>(gridDim.x) * WGS;
+      if (next < n_tiles) fetch_features(next);
+    }
     if constexpr (MODE == kModeTrainFwd) {
       const float pdf_phi = tile::row_pdf_train<NBP, LINEAR>(c.tmem + c.lane_base, tg[1]);
       // combine_AR_pdf_and_dl_doutput (train.h:956-963): AutoRegressive takes
@@ -321,22 +362,24 @@ bool df_shape_supported(const DfShape& s) {
   return a || b || c;
 }
 
-size_t df_fused_smem_bytes(const DfShape& s, uint32_t bt, uint32_t bp) {
-  const int lf = s.levels * s.features;
-  const int kt = pad16c(lf + 28);
-  const int kr = pad16c(lf + 40) - lf;
-  int ka = kt > 64 ? kt : 64;
-  ka = ka > kr ? ka : kr;
+size_t df_fused_smem_bytes(const DfShape& s, int mode, uint32_t bt, uint32_t bp) {
+  const uint32_t lf = static_cast<uint32_t>(s.levels * s.features);
+  const uint32_t kt = static_cast<uint32_t>(pad16c(static_cast<int>(lf) + 28));
+  const uint32_t kr = static_cast<uint32_t>(pad16c(static_cast<int>(lf) + 40)) - lf;
+  const bool feat = mode != kModeTrainFwd;
+  const uint32_t ka = feat ? DfWidths<8, 2>::tile_a(kt - lf, kr) : DfWidths<8, 2>::tile_a(kt, kr);
   const size_t off_phi = (bt + 127u) & ~127u;
   const size_t off_tiles = (off_phi + bp + 127u) & ~size_t(127);
-  return off_tiles + static_cast<size_t>(kDfWarpgroups) * 128u * (ka + lf) * 2u +
-         8u * (kDfWarpgroups + 1) + 16u;
+  return off_tiles + static_cast<size_t>(kDfWarpgroups) * 128u * (ka + (feat ? 2u : 1u) * lf) * 2u +
+         8u * (2 * kDfWarpgroups + 1) + 16u;
 }
 
 cudaError_t launch_df_fused(const DfShape& s, int mode, const DfKernelParams& p, int num_sms,
                             cudaStream_t st) {
   if (p.n <= 0) return cudaSuccess;
-  const size_t smem = df_fused_smem_bytes(s, p.blob_theta_bytes, p.blob_phi_bytes);
+  const size_t smem = df_fused_smem_bytes(s, mode, p.blob_theta_bytes, p.blob_phi_bytes);
+  if (mode != kModeTrainFwd && (p.feat_theta == nullptr || p.feat_phi == nullptr))
+    return cudaErrorInvalidValue;
 #define GDF_DISPATCH(L, F, NBT, NBP)                                                  \
   if (s.levels == L && s.features == F && s.bins_theta == NBT && s.bins_phi == NBP) { \
     return s.linear ? launch_t<L, F, NBT, NBP, true>(mode, p, smem, num_sms, st)      \

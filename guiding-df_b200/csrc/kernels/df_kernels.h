@@ -40,10 +40,26 @@ struct DfKernelParams {
   unsigned long long* n_dropped;     // records rejected by the validity filter
   float loss_scale_per_record;       // TRAIN_LOSS_SCALE / n
   GridLevels gl_theta, gl_phi;
+  // grid features of both networks, precomputed by launch_grid_features
+  // (inference and pdf evaluation): 128-row tiles, canonical layout
+  const __half* feat_theta;
+  const __half* feat_phi;
   // inference options (gdf_infer_ex)
   gdf_shading shading;               // raw shading points when shading.pos != nullptr
   gdf_aabb aabb;
   float* dir_pdf;                    // n x 4 world direction + solid-angle pdf, nullable
+};
+
+struct GridFeatParams {
+  const float* queries;      // n x 9 query rows (positions in columns 0-2), or
+  const float* shading_pos;  // n x 3 world positions normalised against aabb
+  gdf_aabb aabb;
+  int64_t n, n_tiles;        // rows, 128-row tiles written (padding rows use 0.5)
+  const __half* grid_theta;
+  const __half* grid_phi;
+  GridLevels gl_theta, gl_phi;
+  __half* feat_theta;        // [n_tiles][128 x L*F] canonical
+  __half* feat_phi;
 };
 
 struct DfShape {
@@ -54,8 +70,11 @@ struct DfShape {
 // Returns cudaErrorNotSupported when no kernel is built for the shape.
 cudaError_t launch_df_fused(const DfShape& s, int mode, const DfKernelParams& p, int num_sms,
                             cudaStream_t stream);
-size_t df_fused_smem_bytes(const DfShape& s, uint32_t blob_theta_bytes, uint32_t blob_phi_bytes);
+size_t df_fused_smem_bytes(const DfShape& s, int mode, uint32_t blob_theta_bytes, uint32_t blob_phi_bytes);
 bool df_shape_supported(const DfShape& s);
+
+// Both grids' features for inference / pdf evaluation.
+cudaError_t launch_grid_features(const DfShape& s, const GridFeatParams& p, cudaStream_t st);
 
 // Epilogue-only kernel (gdf_post_inference).
 cudaError_t launch_df_post(int bins_theta, int bins_phi, bool linear, const float* logits_theta,
