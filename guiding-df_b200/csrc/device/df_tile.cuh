@@ -48,10 +48,16 @@ __device__ __forceinline__ void store_run(uint8_t* t, uint32_t row, uint32_t col
 // fp32 accumulation. interp: 0 linear, 1 smoothstep, 2 nearest.
 // The level tables are read from the kernel's __grid_constant__ parameters
 // with a warp-uniform dynamic level index (indexed constant-bank loads).
-template <int F>
-__device__ __forceinline__ void grid_level(const GridLevels& s, int l, int interp,
-                                           const __half* __restrict__ table, float px, float py,
-                                           float pz, float* out) {
+// Corner entries and per-axis weights of one level at one position
+// (tcnn kernel_grid, encodings/grid.h:220-330; grid_index :165-188 with the
+// CoherentPrime hash of :112-129 for hashed levels).
+struct LevelCorners {
+  uint32_t e[8];   // entry of corner c (bit 0: x, bit 1: y, bit 2: z), within the level
+  float w[3][2];   // per-axis weight of the lower (0) and upper (1) corner
+};
+
+__device__ __forceinline__ LevelCorners level_corners(const GridLevels& s, int l, int interp, float px,
+                                                      float py, float pz) {
   const float scale = s.scale[l];
   const float pin[3] = {px, py, pz};
   float fr[3];
@@ -79,54 +85,122 @@ __device__ __forceinline__ void grid_level(const GridLevels& s, int l, int inter
     ty[0] = mode > 1 ? pg[1] * r : 0u; ty[1] = mode > 1 ? ty[0] + r : 0u;
     tz[0] = mode > 2 ? pg[2] * r * r : 0u; tz[1] = mode > 2 ? tz[0] + r * r : 0u;
   }
-  const __half* tab = table + static_cast<size_t>(s.offset[l]) * F;
-  auto entry = [&](int c) -> uint32_t {
-    const uint32_t x = tx[c & 1], y = ty[(c >> 1) & 1], z = tz[(c >> 2) & 1];
+  LevelCorners c;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const uint32_t x = tx[k & 1], y = ty[(k >> 1) & 1], z = tz[(k >> 2) & 1];
     const uint32_t idx = mode == 0 ? (x ^ y ^ z) : (x + y + z);
-    return hmask ? (idx & hmask) : (idx % hsize);
-  };
+    c.e[k] = hmask ? (idx & hmask) : (idx % hsize);
+  }
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    c.w[d][0] = 1.f - fr[d];
+    c.w[d][1] = fr[d];
+  }
+  return c;
+}
+
+// weight of corner k = (x-term * y-term) * z-term, as kernel_grid's dim loop
+__device__ __forceinline__ float corner_weight(const LevelCorners& c, int k) {
+  return (1.f * c.w[0][k & 1]) * c.w[1][(k >> 1) & 1] * c.w[2][(k >> 2) & 1];
+}
+
+template <int F>
+__device__ __forceinline__ void grid_level(const GridLevels& s, int l, int interp,
+                                           const __half* __restrict__ table, float px, float py,
+                                           float pz, float* out) {
+  const LevelCorners c = level_corners(s, l, interp, px, py, pz);
+  const __half* tab = table + static_cast<size_t>(s.offset[l]) * F;
   float acc[F];
 #pragma unroll
   for (int f = 0; f < F; ++f) acc[f] = 0.f;
   if (interp == 2) {
-    const uint32_t e = entry(0);
 #pragma unroll
-    for (int f = 0; f < F; ++f) acc[f] = __half2float(tab[static_cast<size_t>(e) * F + f]);
+    for (int f = 0; f < F; ++f) acc[f] = __half2float(tab[static_cast<size_t>(c.e[0]) * F + f]);
+  } else if constexpr (F == 2) {
+    uint32_t raw[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) raw[k] = __ldg(reinterpret_cast<const unsigned int*>(tab) + c.e[k]);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const float w = corner_weight(c, k);
+      const float2 v = __half22float2(*reinterpret_cast<const __half2*>(&raw[k]));
+      acc[0] += w * v.x;
+      acc[1] += w * v.y;
+    }
   } else {
-    const float wx[2] = {1.f - fr[0], fr[0]}, wy[2] = {1.f - fr[1], fr[1]}, wz[2] = {1.f - fr[2], fr[2]};
-    uint32_t e[8];
+    uint2 raw[8];
 #pragma unroll
-    for (int c = 0; c < 8; ++c) e[c] = entry(c);
-    if constexpr (F == 2) {
-      uint32_t raw[8];
+    for (int k = 0; k < 8; ++k) raw[k] = __ldg(reinterpret_cast<const uint2*>(tab) + c.e[k]);
 #pragma unroll
-      for (int c = 0; c < 8; ++c) raw[c] = __ldg(reinterpret_cast<const unsigned int*>(tab) + e[c]);
-#pragma unroll
-      for (int c = 0; c < 8; ++c) {
-        // weight = (x-term * y-term) * z-term, as kernel_grid's dim loop
-        const float w = (1.f * wx[c & 1]) * wy[(c >> 1) & 1] * wz[(c >> 2) & 1];
-        const float2 v = __half22float2(*reinterpret_cast<const __half2*>(&raw[c]));
-        acc[0] += w * v.x;
-        acc[1] += w * v.y;
-      }
-    } else {
-      uint2 raw[8];
-#pragma unroll
-      for (int c = 0; c < 8; ++c) raw[c] = __ldg(reinterpret_cast<const uint2*>(tab) + e[c]);
-#pragma unroll
-      for (int c = 0; c < 8; ++c) {
-        const float w = (1.f * wx[c & 1]) * wy[(c >> 1) & 1] * wz[(c >> 2) & 1];
-        const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&raw[c].x));
-        const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&raw[c].y));
-        acc[0] += w * a.x;
-        acc[1] += w * a.y;
-        acc[2] += w * b.x;
-        acc[3] += w * b.y;
-      }
+    for (int k = 0; k < 8; ++k) {
+      const float w = corner_weight(c, k);
+      const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&raw[k].x));
+      const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&raw[k].y));
+      acc[0] += w * a.x;
+      acc[1] += w * a.y;
+      acc[2] += w * b.x;
+      acc[3] += w * b.y;
     }
   }
 #pragma unroll
   for (int f = 0; f < F; ++f) out[f] = acc[f];
+}
+
+// One level of both DF grids at the same position, from the interleaved
+// table il: entry e holds [theta features (F) | phi features (F)], so each
+// corner is one 2F-half gather for both networks. Same arithmetic as
+// grid_level (shared corners and weights, accumulation in corner order).
+template <int F>
+__device__ __forceinline__ void grid_level_pair(const GridLevels& s, int l, int interp,
+                                                const __half* __restrict__ il, float px, float py,
+                                                float pz, float* out_t, float* out_p) {
+  const LevelCorners c = level_corners(s, l, interp, px, py, pz);
+  const __half* tab = il + static_cast<size_t>(s.offset[l]) * (2 * F);
+  float at[F], ap[F];
+#pragma unroll
+  for (int f = 0; f < F; ++f) { at[f] = 0.f; ap[f] = 0.f; }
+  if (interp == 2) {
+#pragma unroll
+    for (int f = 0; f < F; ++f) {
+      at[f] = __half2float(tab[static_cast<size_t>(c.e[0]) * 2 * F + f]);
+      ap[f] = __half2float(tab[static_cast<size_t>(c.e[0]) * 2 * F + F + f]);
+    }
+  } else if constexpr (F == 2) {
+    uint2 raw[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) raw[k] = __ldg(reinterpret_cast<const uint2*>(tab) + c.e[k]);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const float w = corner_weight(c, k);
+      const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&raw[k].x));
+      const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&raw[k].y));
+      at[0] += w * a.x;
+      at[1] += w * a.y;
+      ap[0] += w * b.x;
+      ap[1] += w * b.y;
+    }
+  } else {
+    uint4 raw[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) raw[k] = __ldg(reinterpret_cast<const uint4*>(tab) + c.e[k]);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const float w = corner_weight(c, k);
+      const uint32_t h[4] = {raw[k].x, raw[k].y, raw[k].z, raw[k].w};
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&h[j]));
+        const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&h[2 + j]));
+        at[2 * j] += w * a.x;
+        at[2 * j + 1] += w * a.y;
+        ap[2 * j] += w * b.x;
+        ap[2 * j + 1] += w * b.y;
+      }
+    }
+  }
+#pragma unroll
+  for (int f = 0; f < F; ++f) { out_t[f] = at[f]; out_p[f] = ap[f]; }
 }
 
 // All levels of one grid, written as fp16 into columns [0, L*F) of a tile

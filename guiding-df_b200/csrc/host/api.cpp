@@ -81,9 +81,9 @@ gdf_status validate(const gdf_config& c) {
     return fail(GDF_ERR_INVALID_ARG, "pdf_interp");
   if (!valid_grid(c.grid_theta) || !valid_grid(c.grid_phi))
     return fail(GDF_ERR_INVALID_ARG, "grid config out of range");
-  if (c.grid_theta.n_levels != c.grid_phi.n_levels ||
-      c.grid_theta.n_features_per_level != c.grid_phi.n_features_per_level)
-    return fail(GDF_ERR_UNSUPPORTED, "theta and phi grids must share levels and features");
+  if (std::memcmp(&c.grid_theta, &c.grid_phi, sizeof(gdf_grid_config)) != 0)
+    return fail(GDF_ERR_UNSUPPORTED,
+                "theta and phi grids must share one configuration (inference gathers both at once)");
   if (c.sh_degree != 4 || c.oneblob_bins != 4 || c.tw_frequencies != 12)
     return fail(GDF_ERR_UNSUPPORTED, "built encodings: SH degree 4, OneBlob 4 bins, TriangleWave 12");
   if (c.mlp_theta.n_neurons != 64 || c.mlp_phi.n_neurons != 64)
@@ -451,6 +451,17 @@ static gdf_status ensure_features(Context& c, int64_t n_tiles) {
   return GDF_OK;
 }
 
+// Rebuilds the interleaved inference grid from both networks' EMA copies.
+static gdf_status refresh_grid_il(Context& c) {
+  const Net& t = c.net[0];
+  const Net& f = c.net[1];
+  cudaError_t e = gdf::launch_interleave_grids(t.ema16 + t.n_mlp, f.ema16 + f.n_mlp, c.grid_il,
+                                               t.n_grid / t.features, t.features, nullptr);
+  if (e != cudaSuccess) return cuda_fail(e, "interleave grids");
+  GDF_CUDA(cudaDeviceSynchronize());
+  return GDF_OK;
+}
+
 // Both grids' features of n queries (query rows, or shading positions with
 // aabb) into the context's buffer; points p at them.
 static gdf_status grid_features(Context& c, const float* queries, const gdf_shading* sh,
@@ -466,10 +477,8 @@ static gdf_status grid_features(Context& c, const float* queries, const gdf_shad
   g.aabb = aabb;
   g.n = n;
   g.n_tiles = tiles;
-  g.grid_theta = p.grid_theta;
-  g.grid_phi = p.grid_phi;
-  g.gl_theta = p.gl_theta;
-  g.gl_phi = p.gl_phi;
+  g.grid_il = c.grid_il;
+  g.gl = c.net[0].gl;
   g.feat_theta = c.feat;
   g.feat_phi = c.feat + c.feat_tiles * 128 * feat_row_halves(c);
   cudaError_t e = gdf::launch_grid_features(df_shape(c), g, st);
@@ -498,6 +507,7 @@ gdf_status gdf_create(const gdf_config* cfg, gdf_ctx** out) {
     free_ws(c.ws);
     free_pw(c.pw);
     cudaFree(c.feat);
+    cudaFree(c.grid_il);
     cudaFree(c.d_err);
     delete h;
     return st;
@@ -511,11 +521,13 @@ gdf_status gdf_create(const gdf_config* cfg, gdf_ctx** out) {
   if ((s = alloc_ws(c))) return cleanup(s);
   if (c.cfg.max_queries > 0 && (s = ensure_features(c, (c.cfg.max_queries + 127) / 128)))
     return cleanup(s);
+  if ((s = dalloc(&c.grid_il, static_cast<size_t>(2 * c.net[0].n_grid)))) return cleanup(s);
   e = cudaMemset(c.d_err, 0, 4);
   if (e != cudaSuccess) return cleanup(cuda_fail(e, "cudaMemset"));
   for (int i = 0; i < 3; ++i)
     if (c.net[i].present && (s = init_params(c.net[i], c.cfg.seed, static_cast<uint32_t>(i))))
       return cleanup(s);
+  if ((s = refresh_grid_il(c))) return cleanup(s);
   *out = h;
   return GDF_OK;
 }
@@ -527,6 +539,7 @@ gdf_status gdf_destroy(gdf_ctx* ctx) {
   free_ws(ctx->c.ws);
   free_pw(ctx->c.pw);
   cudaFree(ctx->c.feat);
+  cudaFree(ctx->c.grid_il);
   cudaFree(ctx->c.d_err);
   delete ctx;
   return GDF_OK;
@@ -540,7 +553,7 @@ gdf_status gdf_reset_training(gdf_ctx* ctx, uint32_t seed) {
     gdf_status s = init_params(n, seed, static_cast<uint32_t>(i));
     if (s) return s;
   }
-  return GDF_OK;
+  return refresh_grid_il(ctx->c);
 }
 
 gdf_status gdf_n_params(const gdf_ctx* ctx, int32_t net, int64_t* n_params) {
@@ -555,7 +568,9 @@ gdf_status gdf_set_params(gdf_ctx* ctx, int32_t net, const float* params_host, i
   if (!nt || !params_host) return fail(GDF_ERR_INVALID_ARG, "bad ctx / net id / params");
   if (n != nt->n_params) return fail(GDF_ERR_INVALID_ARG, "parameter count mismatch");
   std::vector<float> h(params_host, params_host + n);
-  return upload_params(*nt, h);
+  gdf_status s = upload_params(*nt, h);
+  if (s || net == GDF_NET_NRC) return s;
+  return refresh_grid_il(ctx->c);
 }
 
 gdf_status gdf_get_params(const gdf_ctx* ctx, int32_t net, float* params_host, int64_t n) {
@@ -609,7 +624,7 @@ gdf_status gdf_load_network(gdf_ctx* ctx, const char* prefix) {
     gdf_status s = upload_params(n, h);
     if (s) return s;
   }
-  return GDF_OK;
+  return refresh_grid_il(ctx->c);
 }
 
 static gdf::DfKernelParams df_params(Context& c) {
@@ -779,6 +794,11 @@ static gdf::AdamParams adam_params(Context& c, int id, const gdf_adam_config& a,
   p.debias_new = 1.0f / (1.0f - static_cast<float>(std::pow(static_cast<double>(a.ema_decay), static_cast<double>(step))));
   p.sq_partial = sq;
   p.n_blocks = gdf::kAdamBlocks;
+  if (id < 2) {
+    p.grid_il = c.grid_il;
+    p.il_net = id;
+    p.il_features = n.features;
+  }
   return p;
 }
 

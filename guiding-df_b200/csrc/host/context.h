@@ -79,6 +79,9 @@ struct Context {
   uint32_t* d_err = nullptr;  // device error word of bounded waits
   TrainWorkspace ws;
   PathWorkspace pw;
+  // the two DF networks' EMA grids interleaved per entry for inference:
+  // [grid entries][theta F halves | phi F halves]
+  __half* grid_il = nullptr;
   // grid features of both networks for inference: [2][feat_tiles][128 x L*F]
   __half* feat = nullptr;
   int64_t feat_tiles = 0;

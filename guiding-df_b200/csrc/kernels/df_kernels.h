@@ -55,9 +55,8 @@ struct GridFeatParams {
   const float* shading_pos;  // n x 3 world positions normalised against aabb
   gdf_aabb aabb;
   int64_t n, n_tiles;        // rows, 128-row tiles written (padding rows use 0.5)
-  const __half* grid_theta;
-  const __half* grid_phi;
-  GridLevels gl_theta, gl_phi;
+  const __half* grid_il;     // interleaved EMA tables: [entries][theta F | phi F]
+  GridLevels gl;             // the grid configuration both networks share
   __half* feat_theta;        // [n_tiles][128 x L*F] canonical
   __half* feat_phi;
 };
@@ -75,6 +74,9 @@ bool df_shape_supported(const DfShape& s);
 
 // Both grids' features for inference / pdf evaluation.
 cudaError_t launch_grid_features(const DfShape& s, const GridFeatParams& p, cudaStream_t st);
+// (Re)builds the interleaved inference table from the two EMA grids.
+cudaError_t launch_interleave_grids(const __half* theta, const __half* phi, __half* il,
+                                    int64_t n_entries, int features, cudaStream_t st);
 
 // Epilogue-only kernel (gdf_post_inference).
 cudaError_t launch_df_post(int bins_theta, int bins_phi, bool linear, const float* logits_theta,

@@ -406,6 +406,10 @@ __global__ void adam_ema_kernel(const __grid_constant__ AdamParams p) {
     const __half e = __float2half_rn((__half2float(p.ema16[i]) * p.ema_decay * p.debias_old +
                                       w16 * (1 - p.ema_decay)) * p.debias_new);
     p.ema16[i] = e;
+    if (i >= p.n_mlp && p.grid_il != nullptr) {
+      const int64_t j = i - p.n_mlp, F = p.il_features;
+      p.grid_il[(j / F) * 2 * F + p.il_net * F + j % F] = e;
+    }
     if (i < p.n_mlp) {
       // re-layout for the tensor cores (canonical K-major per matrix)
       int l = 0;

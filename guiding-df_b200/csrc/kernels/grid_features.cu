@@ -2,15 +2,18 @@
 // a batch of queries, written in the tensor-core tile layout.
 //
 // The grid gathers (tcnn kernel_grid, encodings/grid.h:220-330: 8 corner
-// reads per level) dominate inference. Inside the fused kernel they ran at
-// one 128-thread warpgroup per tile between the MMA and epilogue phases,
-// which left L2 mostly idle. Here every thread computes one 16-byte chunk of
-// one row's features -- 8/F levels of one network, 8x that many independent
-// 4- or 8-byte gathers -- at full occupancy, and stores it where the fused
-// kernel's bulk copy expects it: tiles of 128 rows x L*F fp16 columns in the
-// canonical no-swizzle K-major layout (8x8 core matrices), tile t at
-// feat + t * 128 * L*F. A warp covers 32 consecutive rows of one chunk, so
-// each group of 8 rows writes one contiguous 128-byte line.
+// reads per level and network) dominate inference, and with random query
+// positions their cost is the number of L1 misses sent to L2 (about 4
+// random sectors per level). Both networks use the same grid configuration
+// at the same position, so their corner indices coincide: inference reads
+// an interleaved copy of the two EMA tables (entry e = [theta F halves |
+// phi F halves]) and one 4F-byte gather serves both networks, halving the
+// requests. Every thread computes one 16-byte chunk (8/F levels) of one
+// row for both networks at full occupancy and stores the two chunks where
+// the fused kernel's bulk copies expect them: tiles of 128 rows x L*F fp16
+// columns in the canonical no-swizzle K-major layout (8x8 core matrices),
+// tile t at feat + t * 128 * L*F. A warp covers 32 consecutive rows of one
+// chunk, so each group of 8 rows writes one contiguous 128-byte line.
 #include <cuda_fp16.h>
 
 #include "../device/df_tile.cuh"
@@ -28,11 +31,9 @@ __global__ void __launch_bounds__(256, 4) grid_features_kernel(const __grid_cons
   constexpr uint32_t LF = L * F;
   const int64_t rows = p.n_tiles * 128;
   const int64_t gid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (gid >= rows * NCH * 2) return;
+  if (gid >= rows * NCH) return;
   const int64_t row = gid % rows;
-  const int64_t rest = gid / rows;
-  const int chunk = static_cast<int>(rest % NCH);
-  const int net = static_cast<int>(rest / NCH);
+  const int chunk = static_cast<int>(gid / rows);
   float pos[3] = {0.5f, 0.5f, 0.5f};
   if (row < p.n) {
     if (p.shading_pos != nullptr) {
@@ -45,28 +46,41 @@ __global__ void __launch_bounds__(256, 4) grid_features_kernel(const __grid_cons
       for (int k = 0; k < 3; ++k) pos[k] = __ldg(p.queries + row * 9 + k);
     }
   }
-  const GridLevels& gl = net ? p.gl_phi : p.gl_theta;
-  const __half* tab = net ? p.grid_phi : p.grid_theta;
-  uint32_t packed[4];
+  const GridLevels& gl = p.gl;
+  uint32_t pt[4], pp[4];
 #pragma unroll
   for (int j = 0; j < LPC; ++j) {
-    float f[F];
-    tile::grid_level<F>(gl, chunk * LPC + j, gl.interp, tab, pos[0], pos[1], pos[2], f);
+    float ft[F], fp[F];
+    tile::grid_level_pair<F>(gl, chunk * LPC + j, gl.interp, p.grid_il, pos[0], pos[1], pos[2], ft, fp);
 #pragma unroll
     for (int k = 0; k < F; k += 2) {
-      const __half2 h = __floats2half2_rn(f[k], f[k + 1]);
-      packed[(j * F + k) / 2] = *reinterpret_cast<const uint32_t*>(&h);
+      const __half2 a = __floats2half2_rn(ft[k], ft[k + 1]);
+      const __half2 b = __floats2half2_rn(fp[k], fp[k + 1]);
+      pt[(j * F + k) / 2] = *reinterpret_cast<const uint32_t*>(&a);
+      pp[(j * F + k) / 2] = *reinterpret_cast<const uint32_t*>(&b);
     }
   }
-  __half* out = (net ? p.feat_phi : p.feat_theta) + (row >> 7) * (128 * LF) +
-                sm100::canon_offset(static_cast<uint32_t>(row & 127), static_cast<uint32_t>(chunk * 8), LF);
-  *reinterpret_cast<uint4*>(out) = make_uint4(packed[0], packed[1], packed[2], packed[3]);
+  const int64_t off = (row >> 7) * (128 * LF) +
+                      sm100::canon_offset(static_cast<uint32_t>(row & 127), static_cast<uint32_t>(chunk * 8), LF);
+  *reinterpret_cast<uint4*>(p.feat_theta + off) = make_uint4(pt[0], pt[1], pt[2], pt[3]);
+  *reinterpret_cast<uint4*>(p.feat_phi + off) = make_uint4(pp[0], pp[1], pp[2], pp[3]);
+}
+
+// il[e][0..F) = theta[e][..], il[e][F..2F) = phi[e][..]
+__global__ void interleave_grids_kernel(const __half* __restrict__ t, const __half* __restrict__ ph,
+                                        __half* __restrict__ il, int64_t n_entries, int F) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n_entries * F) return;
+  const int64_t e = i / F;
+  const int f = static_cast<int>(i % F);
+  il[e * 2 * F + f] = t[i];
+  il[e * 2 * F + F + f] = ph[i];
 }
 
 template <int L, int F>
 cudaError_t launch_l(const GridFeatParams& p, cudaStream_t st) {
   constexpr int NCH = L * F / 8;
-  const int64_t threads = p.n_tiles * 128 * NCH * 2;
+  const int64_t threads = p.n_tiles * 128 * NCH;
   grid_features_kernel<L, F><<<static_cast<unsigned>((threads + 255) / 256), 256, 0, st>>>(p);
   return cudaGetLastError();
 }
@@ -79,6 +93,15 @@ cudaError_t launch_grid_features(const DfShape& s, const GridFeatParams& p, cuda
   if (s.levels == 16 && s.features == 2) return launch_l<16, 2>(p, st);
   if (s.levels == 8 && s.features == 4) return launch_l<8, 4>(p, st);
   return cudaErrorNotSupported;
+}
+
+cudaError_t launch_interleave_grids(const __half* theta, const __half* phi, __half* il,
+                                    int64_t n_entries, int features, cudaStream_t st) {
+  const int64_t n = n_entries * features;
+  if (n == 0) return cudaSuccess;
+  interleave_grids_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, st>>>(theta, phi, il, n_entries,
+                                                                                  features);
+  return cudaGetLastError();
 }
 
 }  // namespace gdf

@@ -48,6 +48,10 @@ struct AdamParams {
   float loss_scale, lr, beta1, beta2, eps, l2_reg, ema_decay, debias_old, debias_new;
   double* sq_partial;       // [n_blocks]
   int32_t n_blocks;
+  // interleaved inference copy of the EMA grid ([entries][theta F | phi F]),
+  // nullable; this network's half is at il_net * F
+  __half* grid_il;
+  int32_t il_net, il_features;
 };
 
 cudaError_t launch_df_train_bwd(const DfShape& s, bool phi, const DfBwdParams& p, int ctas,
