@@ -18,6 +18,13 @@ namespace gdf {
 
 constexpr float kEps = 1e-5f;  // M_EPSILON (krrmath/constants.h:19)
 
+// 2^x by the SFU (ex2.approx.ftz.f32; subnormal results flush to zero).
+__device__ __forceinline__ float ex2_approx(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 // grid_index (grid.h:165-188) with the CoherentPrime hash (grid.h:112-129).
 __device__ __forceinline__ uint32_t grid_entry(const GridLevels& g, int l, uint32_t x,
                                                uint32_t y, uint32_t z) {
@@ -333,6 +340,134 @@ __device__ __forceinline__ float sample_dir(const float (&pdf)[N], float u, floa
     const float d = (static_cast<float>(seg) + w) / static_cast<float>(N);
     return fminf(d, 1.f - kEps);
   }
+}
+
+// Inversion inside the segment found by the CDF walk (train.h:453-519):
+// seg is the index of the first boundary above u (0 = the leading half-bin,
+// N = the trailing one), cm1/ci the CDF at the segment's ends, lo/hi the pdf
+// at its ends.
+template <int N, bool LINEAR>
+__device__ __forceinline__ float invert_segment(int seg, float cm1, float ci, float lo, float hi, float u,
+                                                float u2) {
+  const float inv_n = 1.f / static_cast<float>(N);
+  if constexpr (LINEAR) {
+    int idx_m1 = seg - 1;
+    float v = static_cast<float>(idx_m1) + 0.5f;
+    float ecm = 1.f, v_off = 0.f;
+    if (idx_m1 < 0) { v_off = 0.5f; ecm = 0.5f; }
+    else if (seg > N - 1) { ecm = 0.5f; }
+    const float m = (hi - lo) * static_cast<float>(N);
+    const float B = lo * (1 + v) - hi * v;
+    v += v_off;
+    const float A = m * 0.5f;
+    float d;
+    if (fabsf(A) < kEps) {
+      const float v_diff = u - cm1;
+      const float v_cdf_diff = ci - cm1;
+      const float w = v_cdf_diff > kEps ? v_diff / v_cdf_diff : u2;
+      d = (v + w * ecm) * inv_n;
+    } else {
+      const float C = -(m * 0.5f) * (v * v * inv_n * inv_n) - (B * v * inv_n) + cm1 - u;
+      const float delta = B * B - 4 * A * C;
+      if (delta < kEps) {
+        d = (v + u2 * ecm) * inv_n;
+      } else {
+        const float sq = sqrtf(delta);
+        const float s0 = (-B + sq) / (2 * A);
+        const float s1 = (-B - sq) / (2 * A);
+        d = A >= 0 ? fmaxf(s0, s1) : fminf(s0, s1);
+      }
+    }
+    return fminf(d, 1.f - kEps);
+  } else {
+    const float v_diff = u - cm1;
+    const float v_cdf_diff = ci - cm1;
+    const float w = v_cdf_diff > kEps ? v_diff / v_cdf_diff : u2;
+    const float d = (static_cast<float>(seg) + w) / static_cast<float>(N);
+    return fminf(d, 1.f - kEps);
+  }
+}
+
+struct SampleResult {
+  float u;    // sampled (guided) or given square coordinate
+  float pdf;  // interpolated pdf at u
+};
+
+// sample_dir_guided_inputs_F (train.h:416-520) followed by sample_pdf
+// (train.h:655-681) in one pass over the bins.
+//
+// The CDF is non-decreasing, so the reference's early-exit search for the
+// first boundary above u equals counting the boundaries b_i <= u; the walk
+// latches the values of the last counted boundary (its index, CDF, and the
+// pdf at both ends of the next segment) without a "found" flag. Rows that
+// are not guided count bins up to the given direction's floor(N u - 1/2)
+// instead, so the same latched pair serves the pdf interpolation of every
+// row; a guided sample whose rounding puts it outside its segment falls back
+// to indexed reads.
+template <int N, bool LINEAR>
+__device__ __forceinline__ SampleResult sample_and_pdf(const float (&pdf)[N], bool guided, float u_given,
+                                                       float u, float u2) {
+  const float nf = static_cast<float>(N);
+  SampleResult r;
+  if constexpr (LINEAR) {
+    const int f_given = safe_floor<N>(u_given * nf - 0.5f);
+    int seg = 0;
+    float cm1 = 0.f, lo = pdf[0], hi = pdf[0];
+    float b = pdf[0] * 0.5f / nf;  // b_0: end of the leading half-bin
+    const float b0 = b;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      if (i > 0) b = b + (pdf[i - 1] + pdf[i]) / static_cast<float>(2 * N);
+      const bool cond = guided ? (b <= u) : (i <= f_given);
+      if (cond) {
+        seg = i + 1;
+        cm1 = b;
+        lo = pdf[i];
+        hi = pdf[i + 1 < N ? i + 1 : N - 1];
+      }
+    }
+    float d = u_given;
+    if (guided) {
+      const float ci = seg == 0 ? b0 : (seg < N ? cm1 + (lo + hi) / static_cast<float>(2 * N)
+                                                : cm1 + pdf[N - 1] * 0.5f / nf);
+      d = invert_segment<N, true>(seg, cm1, ci, lo, hi, u, u2);
+    }
+    r.u = d;
+    // sample_pdf (train.h:656-676): bins f = floor(N d - 1/2) and f + 1,
+    // the leading half-bin reads pdf[0], the trailing one pdf[N-1]
+    const float x = d * nf - 0.5f;
+    const int f = safe_floor<N>(x);
+    if (f == seg - 1) {
+      r.pdf = f < 0 ? lo : (f + 1 > N - 1 ? lo : (1.0f - (x - static_cast<float>(f))) * lo +
+                                                     (x - static_cast<float>(f)) * hi);
+    } else {
+      r.pdf = sample_pdf<N, true>(pdf, d);
+    }
+  } else {
+    const int f_given = safe_floor<N>(u_given * nf);
+    int seg = 0;
+    float cm1 = 0.f, cur = pdf[0];
+    float c = 0.f;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      c = c + pdf[i] / nf;
+      const bool cond = guided ? (c <= u) : (i < f_given);
+      if (cond) {
+        seg = i + 1;
+        cm1 = c;
+        cur = pdf[i + 1 < N ? i + 1 : N - 1];
+      }
+    }
+    float d = u_given;
+    if (guided) {
+      const float ci = seg < N ? cm1 + cur / nf : cm1;
+      d = invert_segment<N, false>(seg, cm1, ci, 0.f, 0.f, u, u2);
+    }
+    r.u = d;
+    const int f = safe_floor<N>(d * nf);  // sample_pdf, nearest (train.h:679)
+    r.pdf = (f == (seg < N ? seg : N - 1)) ? cur : select_bin<N>(pdf, f);
+  }
+  return r;
 }
 
 // ------------------------------------------------------------ Philox RNG

@@ -331,10 +331,13 @@ __device__ __forceinline__ void relu_to_tile(Wg& c) {
 #pragma unroll
     for (int kc = 0; kc < 4; ++kc) {
       __half2 v[4];
+      // ReLU after rounding: max(round(x), 0) = round(max(x, 0)), and
+      // __hmax2 maps NaN to 0 like tcnn's relu (x > 0 ? x : 0)
 #pragma unroll
       for (int j = 0; j < 4; ++j)
-        v[j] = __floats2half2_rn(fmaxf(__uint_as_float(r[kc * 8 + 2 * j]), 0.f),
-                                 fmaxf(__uint_as_float(r[kc * 8 + 2 * j + 1]), 0.f));
+        v[j] = __hmax2(__floats2half2_rn(__uint_as_float(r[kc * 8 + 2 * j]),
+                                         __uint_as_float(r[kc * 8 + 2 * j + 1])),
+                       __float2half2_rn(0.f));
       *reinterpret_cast<uint4*>(c.tile_a + chunk_off(c.row, h * 4 + kc, 64)) =
           *reinterpret_cast<uint4*>(v);
     }
@@ -509,19 +512,27 @@ __device__ __noinline__ RowResult row_epilogue(uint32_t taddr, bool guided, floa
     for (int i = 0; i < NB; ++i) v[i] = __uint_as_float(r[i]);
   }
   tc_fence_before();
-  // softmax2 (train.h:845-862): max from 0, exp(z - m - log(sum)), x N
+  // softmax2 (train.h:845-862): p_i = N exp(z_i - m - log sum_j exp(z_j - m))
+  // with m = max(0, max z), evaluated as e_i = 2^(z_i log2 e - m log2 e),
+  // p_i = e_i * (N / sum e): one exponential per bin instead of two.
   float m = 0.0f;
 #pragma unroll
   for (int i = 0; i < NB; ++i) m = fmaxf(m, v[i]);
+  constexpr float kLog2e = 1.4426950408889634074f;
+  const float ml = m * kLog2e;
   float s = 0.0f;
 #pragma unroll
-  for (int i = 0; i < NB; ++i) s += __expf(v[i] - m);
-  const float ls = __logf(s);
+  for (int i = 0; i < NB; ++i) {
+    v[i] = ex2_approx(fmaf(v[i], kLog2e, -ml));
+    s += v[i];
+  }
+  const float k = static_cast<float>(NB) / s;
 #pragma unroll
-  for (int i = 0; i < NB; ++i) v[i] = __expf(v[i] - m - ls) * static_cast<float>(NB);
+  for (int i = 0; i < NB; ++i) v[i] *= k;
+  const SampleResult sr = sample_and_pdf<NB, LINEAR>(v, guided, u_given, u_main, u_fallback);
   RowResult r;
-  r.u = guided ? sample_dir<NB, LINEAR>(v, u_main, u_fallback) : u_given;
-  r.pdf = sample_pdf<NB, LINEAR>(v, r.u);
+  r.u = sr.u;
+  r.pdf = sr.pdf;
   return r;
 }
 
