@@ -250,6 +250,26 @@ void free_ws(gdf::TrainWorkspace& w) {
   w = gdf::TrainWorkspace{};
 }
 
+void free_host_stage(Context& c) {
+  cudaFree(c.host_q);
+  cudaFree(c.host_g);
+  cudaFree(c.host_u);
+  cudaFree(c.host_wi);
+  c.host_q = nullptr;
+  c.host_g = nullptr;
+  c.host_u = nullptr;
+  c.host_wi = nullptr;
+  c.host_cap = 0;
+  for (cudaStream_t& s : c.pipe) {
+    if (s) cudaStreamDestroy(s);
+    s = nullptr;
+  }
+  for (cudaEvent_t& e : c.pipe_ev) {
+    if (e) cudaEventDestroy(e);
+    e = nullptr;
+  }
+}
+
 void free_pw(gdf::PathWorkspace& w) {
   cudaFree(w.mask);
   cudaFree(w.block_counts);
@@ -466,9 +486,9 @@ static gdf_status refresh_grid_il(Context& c) {
 // aabb) into the context's buffer; points p at them.
 static gdf_status grid_features(Context& c, const float* queries, const gdf_shading* sh,
                                 const gdf_aabb& aabb, int64_t n, gdf::DfKernelParams& p,
-                                cudaStream_t st) {
+                                cudaStream_t st, int64_t tile_base = 0) {
   const int64_t tiles = (n + 127) / 128;
-  gdf_status s = ensure_features(c, tiles);
+  gdf_status s = ensure_features(c, tile_base + tiles);
   if (s) return s;
   gdf::GridFeatParams g;
   std::memset(&g, 0, sizeof(g));
@@ -479,8 +499,8 @@ static gdf_status grid_features(Context& c, const float* queries, const gdf_shad
   g.n_tiles = tiles;
   g.grid_il = c.grid_il;
   g.gl = c.net[0].gl;
-  g.feat_theta = c.feat;
-  g.feat_phi = c.feat + c.feat_tiles * 128 * feat_row_halves(c);
+  g.feat_theta = c.feat + tile_base * 128 * feat_row_halves(c);
+  g.feat_phi = c.feat + (c.feat_tiles + tile_base) * 128 * feat_row_halves(c);
   cudaError_t e = gdf::launch_grid_features(df_shape(c), g, st);
   if (e != cudaSuccess) return cuda_fail(e, "grid_features");
   p.feat_theta = g.feat_theta;
@@ -508,6 +528,7 @@ gdf_status gdf_create(const gdf_config* cfg, gdf_ctx** out) {
     free_pw(c.pw);
     cudaFree(c.feat);
     cudaFree(c.grid_il);
+    free_host_stage(c);
     cudaFree(c.d_err);
     delete h;
     return st;
@@ -540,6 +561,7 @@ gdf_status gdf_destroy(gdf_ctx* ctx) {
   free_pw(ctx->c.pw);
   cudaFree(ctx->c.feat);
   cudaFree(ctx->c.grid_il);
+  free_host_stage(ctx->c);
   cudaFree(ctx->c.d_err);
   delete ctx;
   return GDF_OK;
@@ -714,6 +736,78 @@ gdf_status gdf_infer_ex(gdf_ctx* ctx, const gdf_infer_args* a, void* stream) {
   cudaError_t e = gdf::launch_df_fused(df_shape(ctx->c), gdf::kModeInfer, p, ctx->c.num_sms,
                                        static_cast<cudaStream_t>(stream));
   if (e != cudaSuccess) return cuda_fail(e, "df_fused (infer)");
+  return GDF_OK;
+}
+
+gdf_status gdf_infer_host(gdf_ctx* ctx, const float* queries_h, const uint8_t* guided_h,
+                          const float* uniforms_h, uint64_t philox_seed, uint64_t philox_offset,
+                          const float* wi_in_h, float* wi_out_h, int64_t n, void* stream) {
+  if (!ctx) return fail(GDF_ERR_INVALID_ARG, "ctx is null");
+  if (n < 0) return fail(GDF_ERR_INVALID_ARG, "n < 0");
+  if (n == 0) return GDF_OK;
+  gdf_status s;
+  if ((s = check_ptr(queries_h, "queries")) || (s = check_ptr(wi_in_h, "wi_in")) ||
+      (s = check_ptr(wi_out_h, "wi_out")))
+    return s;
+  Context& c = ctx->c;
+  if (c.cfg.max_queries > 0 && n > c.cfg.max_queries)
+    return fail(GDF_ERR_INVALID_ARG, "n exceeds max_queries");
+  if (n > c.host_cap) {
+    cudaFree(c.host_q);
+    cudaFree(c.host_g);
+    cudaFree(c.host_u);
+    cudaFree(c.host_wi);
+    c.host_q = c.host_u = c.host_wi = nullptr;
+    c.host_g = nullptr;
+    c.host_cap = 0;
+    const size_t m = static_cast<size_t>(n);
+    if ((s = dalloc(&c.host_q, m * 9)) || (s = dalloc(&c.host_g, m)) || (s = dalloc(&c.host_u, m * 4)) ||
+        (s = dalloc(&c.host_wi, m * 4)))
+      return s;
+    c.host_cap = n;
+  }
+  if (!c.pipe[0]) {
+    for (cudaStream_t& ps : c.pipe) GDF_CUDA(cudaStreamCreateWithFlags(&ps, cudaStreamNonBlocking));
+    for (cudaEvent_t& e : c.pipe_ev) GDF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  if ((s = ensure_features(c, (n + 127) / 128))) return s;
+  cudaStream_t user = static_cast<cudaStream_t>(stream);
+  GDF_CUDA(cudaEventRecord(c.pipe_ev[2], user));
+  for (cudaStream_t ps : c.pipe) GDF_CUDA(cudaStreamWaitEvent(ps, c.pipe_ev[2], 0));
+  // Chunks of 1024 tiles alternate between two streams, so the copy engines
+  // move chunk k+1 in and chunk k-1 out while chunk k computes.
+  constexpr int64_t kChunk = 1024 * 128;
+  for (int64_t b = 0, k = 0; b < n; b += kChunk, ++k) {
+    const int64_t m = std::min(kChunk, n - b);
+    cudaStream_t ps = c.pipe[k & 1];
+    GDF_CUDA(cudaMemcpyAsync(c.host_q + b * 9, queries_h + b * 9, static_cast<size_t>(m) * 36,
+                             cudaMemcpyHostToDevice, ps));
+    GDF_CUDA(cudaMemcpyAsync(c.host_wi + b * 4, wi_in_h + b * 4, static_cast<size_t>(m) * 16,
+                             cudaMemcpyHostToDevice, ps));
+    if (guided_h)
+      GDF_CUDA(cudaMemcpyAsync(c.host_g + b, guided_h + b, static_cast<size_t>(m), cudaMemcpyHostToDevice, ps));
+    if (uniforms_h)
+      GDF_CUDA(cudaMemcpyAsync(c.host_u + b * 4, uniforms_h + b * 4, static_cast<size_t>(m) * 16,
+                               cudaMemcpyHostToDevice, ps));
+    gdf::DfKernelParams p = df_params(c);
+    p.queries = c.host_q + b * 9;
+    p.guided = guided_h ? c.host_g + b : nullptr;
+    p.uniforms = uniforms_h ? c.host_u + b * 4 : nullptr;
+    p.wi = c.host_wi + b * 4;
+    p.n = m;
+    p.philox_seed = philox_seed;
+    p.philox_offset = philox_offset;
+    p.philox_row_base = b;
+    if ((s = grid_features(c, p.queries, nullptr, gdf_aabb{}, m, p, ps, b / 128))) return s;
+    cudaError_t e = gdf::launch_df_fused(df_shape(c), gdf::kModeInfer, p, c.num_sms, ps);
+    if (e != cudaSuccess) return cuda_fail(e, "df_fused (infer_host)");
+    GDF_CUDA(cudaMemcpyAsync(wi_out_h + b * 4, c.host_wi + b * 4, static_cast<size_t>(m) * 16,
+                             cudaMemcpyDeviceToHost, ps));
+  }
+  for (int i = 0; i < 2; ++i) {
+    GDF_CUDA(cudaEventRecord(c.pipe_ev[i], c.pipe[i]));
+    GDF_CUDA(cudaStreamWaitEvent(user, c.pipe_ev[i], 0));
+  }
   return GDF_OK;
 }
 

@@ -85,6 +85,14 @@ struct Context {
   // grid features of both networks for inference: [2][feat_tiles][128 x L*F]
   __half* feat = nullptr;
   int64_t feat_tiles = 0;
+  // device copies of host inputs for gdf_infer_host, two pipeline streams
+  int64_t host_cap = 0;
+  float* host_q = nullptr;       // [host_cap x 9]
+  uint8_t* host_g = nullptr;     // [host_cap]
+  float* host_u = nullptr;       // [host_cap x 4]
+  float* host_wi = nullptr;      // [host_cap x 4]
+  cudaStream_t pipe[2] = {nullptr, nullptr};
+  cudaEvent_t pipe_ev[3] = {nullptr, nullptr, nullptr};
 };
 
 // Sets the thread-local message returned by gdf_last_error().

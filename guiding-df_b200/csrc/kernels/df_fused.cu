@@ -221,7 +221,8 @@ __global__ void __launch_bounds__(128 * WGS, 1) df_fused_kernel(const __grid_con
           u[0] = uu.x; u[1] = uu.y; u[2] = uu.z; u[3] = uu.w;
         } else {
           uint32_t r[4];
-          philox4x32_10(static_cast<uint32_t>(row), static_cast<uint32_t>(static_cast<uint64_t>(row) >> 32),
+          const uint64_t ctr = static_cast<uint64_t>(row + p.philox_row_base);
+          philox4x32_10(static_cast<uint32_t>(ctr), static_cast<uint32_t>(ctr >> 32),
                         static_cast<uint32_t>(p.philox_offset), static_cast<uint32_t>(p.philox_offset >> 32),
                         static_cast<uint32_t>(p.philox_seed), static_cast<uint32_t>(p.philox_seed >> 32), r);
 #pragma unroll

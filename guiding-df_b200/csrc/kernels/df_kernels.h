@@ -26,6 +26,7 @@ struct DfKernelParams {
   float* pdf_out;            // n x 2 (eval)
   int64_t n;
   uint64_t philox_seed, philox_offset;
+  int64_t philox_row_base;   // Philox counter of row r is row_base + r (chunked calls)
   const __half* grid_theta;  // grid tables (entries x F halfs), inference copy
   const __half* grid_phi;
   const __half* blob_theta;  // MLP weights in the canonical tensor-core layout

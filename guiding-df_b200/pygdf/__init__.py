@@ -153,6 +153,7 @@ def lib() -> C.CDLL:
             "gdf_set_optimizer_state": [P, C.c_int32, P, P, P, C.c_int64, C.c_uint32],
             "gdf_train_loss_static": [P, P, P, P, C.c_int64, P, P, P],
             "gdf_infer_ex": [P, C.POINTER(InferArgs), P],
+            "gdf_infer_host": [P, P, P, P, C.c_uint64, C.c_uint64, P, P, C.c_int64, P],
             "gdf_prepare_queries": [C.POINTER(Shading), C.POINTER(Aabb), P, C.c_int64, P],
             "gdf_build_train_records": [P, C.POINTER(PathState), C.POINTER(Aabb), C.POINTER(TrainPixels),
                                         P, P, P, C.c_int64, C.POINTER(C.c_int64), P],
@@ -274,6 +275,12 @@ class Context:
         n = queries.shape[0] if n is None else n
         check(lib().gdf_infer(self.h, _ptr(queries), _ptr(guided), _ptr(uniforms), seed, offset,
                               _ptr(wi), n, _stream(stream)))
+
+    def infer_host(self, queries, wi_in, wi_out, guided=None, uniforms=None, seed=0, offset=0,
+                   n=None, stream=None):
+        n = queries.shape[0] if n is None else n
+        check(lib().gdf_infer_host(self.h, _ptr(queries), _ptr(guided), _ptr(uniforms), seed, offset,
+                                   _ptr(wi_in), _ptr(wi_out), n, _stream(stream)))
 
     def eval_pdf(self, queries, u, pdf_out, n=None, stream=None):
         n = queries.shape[0] if n is None else n

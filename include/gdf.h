@@ -195,7 +195,10 @@ gdf_status gdf_load_network(gdf_ctx* ctx, const char* path_prefix);
  *   wi_dev       [n x 4] fp32 in/out: slots 0,1 hold the BSDF-sampled square
  *                direction of non-guided rows; slots 2,3 hold the caller's
  *                sign (+1/-1) that the pdfs multiply into.
- * Inference uses the EMA weights, like tcnn's inference params. */
+ * Inference uses the EMA weights, like tcnn's inference params. The
+ * context's inference workspace is shared by its calls: calls on one
+ * context must be ordered (one stream); concurrent streams need separate
+ * contexts. */
 gdf_status gdf_infer(gdf_ctx* ctx, const float* queries_dev, const uint8_t* guided_dev,
                      const float* uniforms_dev, uint64_t philox_seed, uint64_t philox_offset,
                      float* wi_dev, int64_t n, void* stream);
@@ -238,6 +241,20 @@ typedef struct gdf_infer_args {
   int64_t n;
 } gdf_infer_args;
 gdf_status gdf_infer_ex(gdf_ctx* ctx, const gdf_infer_args* args, void* stream);
+
+/* gdf_infer on HOST buffers, for callers whose queries live in host memory:
+ * the inputs are copied in, inferred and the guiding data copied back in
+ * chunks of 131,072 queries pipelined over two internal streams, so the
+ * transfers overlap the kernels. Results are identical to gdf_infer on the
+ * same data (the in-kernel Philox counter continues across chunks).
+ *   queries_h [n x 9], guided_h [n] (nullable), uniforms_h [n x 4]
+ *   (nullable), wi_in_h / wi_out_h [n x 4] (may alias); page-locked host
+ *   memory lets the copies run asynchronously.
+ * Ordered after prior work on `stream`; work on `stream` issued afterwards
+ * runs after it. The host buffers must stay valid until then. */
+gdf_status gdf_infer_host(gdf_ctx* ctx, const float* queries_h, const uint8_t* guided_h,
+                          const float* uniforms_h, uint64_t philox_seed, uint64_t philox_offset,
+                          const float* wi_in_h, float* wi_out_h, int64_t n, void* stream);
 
 /* compute_AR_pdf_combined_F (train.h:730-751) for given square directions:
  * pdf_out_dev[i] = {pdf_theta(u[i].x), pdf_phi(u[i].y)} of the learned
