@@ -32,6 +32,7 @@ SOURCES = [
     ("kernels/loss_static.cu", []),
     ("kernels/nrc.cu", ["-fmad=false"]),
     ("kernels/paths.cu", ["-fmad=false"]),
+    ("kernels/tools.cu", ["-fmad=false"]),
     ("host/api.cpp", []),
 ]
 

@@ -17,6 +17,7 @@
 #include "../kernels/df_kernels.h"
 #include "../kernels/nrc_kernels.h"
 #include "../kernels/paths_kernels.h"
+#include "../kernels/tools_kernels.h"
 #include "../kernels/train_kernels.h"
 #include "context.h"
 
@@ -97,6 +98,9 @@ gdf_status validate(const gdf_config& c) {
     if (c.nrc_frequencies != 12 || c.nrc_oneblob_bins != 4)
       return fail(GDF_ERR_UNSUPPORTED, "built NRC encoding: Frequency 12, OneBlob 4");
   }
+  for (const gdf_adam_config* a : {&c.adam_df, &c.adam_nrc})
+    if (!(a->beta1 >= 0.f && a->beta1 < 1.f && a->beta2 >= 0.f && a->beta2 < 1.f))
+      return fail(GDF_ERR_INVALID_ARG, "Adam betas must lie in [0, 1)");
   if (c.precision < GDF_PREC_FP16 || c.precision > GDF_PREC_FP8)
     return fail(GDF_ERR_INVALID_ARG, "precision");
   if (c.max_queries < 0 || c.max_train_batch < 0)
@@ -251,6 +255,10 @@ void free_ws(gdf::TrainWorkspace& w) {
 }
 
 void free_host_stage(Context& c) {
+  for (float*& t : c.lr_table) {
+    cudaFree(t);
+    t = nullptr;
+  }
   cudaFree(c.host_q);
   cudaFree(c.host_g);
   cudaFree(c.host_u);
@@ -260,6 +268,11 @@ void free_host_stage(Context& c) {
   c.host_u = nullptr;
   c.host_wi = nullptr;
   c.host_cap = 0;
+  cudaFree(c.tool_q);
+  cudaFree(c.tool_uv);
+  cudaFree(c.tool_out);
+  c.tool_q = c.tool_uv = c.tool_out = nullptr;
+  c.tool_cap = 0;
   for (cudaStream_t& s : c.pipe) {
     if (s) cudaStreamDestroy(s);
     s = nullptr;
@@ -543,6 +556,18 @@ gdf_status gdf_create(const gdf_config* cfg, gdf_ctx** out) {
   if (c.cfg.max_queries > 0 && (s = ensure_features(c, (c.cfg.max_queries + 127) / 128)))
     return cleanup(s);
   if ((s = dalloc(&c.grid_il, static_cast<size_t>(2 * c.net[0].n_grid)))) return cleanup(s);
+  for (int t = 0; t < 2; ++t) {
+    const gdf_adam_config& a = t == 0 ? c.cfg.adam_df : c.cfg.adam_nrc;
+    // past k with beta^k < 2^-27 for both betas, 1 - beta^k is 1.0f and the
+    // step size is lr exactly; the table stops two entries after that
+    double k = 1.0;
+    for (double b : {static_cast<double>(a.beta1), static_cast<double>(a.beta2)})
+      if (b > 0.0) k = std::max(k, std::ceil(std::log(std::ldexp(1.0, -27)) / std::log(b)));
+    c.lr_table_n[t] = static_cast<int32_t>(std::min(k + 2.0, static_cast<double>(1 << 22)));
+    if ((s = dalloc(&c.lr_table[t], static_cast<size_t>(c.lr_table_n[t])))) return cleanup(s);
+    e = gdf::launch_adam_lr_table(a.learning_rate, a.beta1, a.beta2, c.lr_table[t], c.lr_table_n[t], nullptr);
+    if (e != cudaSuccess) return cleanup(cuda_fail(e, "adam lr table"));
+  }
   e = cudaMemset(c.d_err, 0, 4);
   if (e != cudaSuccess) return cleanup(cuda_fail(e, "cudaMemset"));
   for (int i = 0; i < 3; ++i)
@@ -811,6 +836,91 @@ gdf_status gdf_infer_host(gdf_ctx* ctx, const float* queries_h, const uint8_t* g
   return GDF_OK;
 }
 
+}  // extern "C"
+
+static gdf_status ensure_tools(Context& c, int64_t n) {
+  if (n <= c.tool_cap) return GDF_OK;
+  cudaFree(c.tool_q);
+  cudaFree(c.tool_uv);
+  cudaFree(c.tool_out);
+  c.tool_q = c.tool_uv = c.tool_out = nullptr;
+  c.tool_cap = 0;
+  const size_t m = static_cast<size_t>(n);
+  gdf_status s;
+  if ((s = dalloc(&c.tool_q, m * 9)) || (s = dalloc(&c.tool_uv, m * 2)) || (s = dalloc(&c.tool_out, m * 4)))
+    return s;
+  c.tool_cap = n;
+  return GDF_OK;
+}
+
+static gdf::QueryRow query_row(const float* q) {
+  gdf::QueryRow r;
+  for (int k = 0; k < 9; ++k) r.v[k] = q[k];
+  return r;
+}
+
+extern "C" {
+
+gdf_status gdf_pdf_image(gdf_ctx* ctx, const float* query_h, int32_t width, int32_t height,
+                         float* image_dev, void* stream) {
+  if (!ctx) return fail(GDF_ERR_INVALID_ARG, "ctx is null");
+  gdf_status s;
+  if ((s = check_ptr(query_h, "query")) || (s = check_ptr(image_dev, "image"))) return s;
+  if (width < 1 || height < 1 || static_cast<int64_t>(width) * height > (int64_t{1} << 26))
+    return fail(GDF_ERR_INVALID_ARG, "image size must be 1 .. 2^26 pixels");
+  Context& c = ctx->c;
+  const int64_t n = static_cast<int64_t>(width) * height;
+  if ((s = ensure_tools(c, n))) return s;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaError_t e = gdf::launch_replicate(query_row(query_h), c.tool_q, c.tool_uv, nullptr, width, height, n, st);
+  if (e != cudaSuccess) return cuda_fail(e, "replicate");
+  gdf::DfKernelParams p = df_params(c);
+  p.queries = c.tool_q;
+  p.u_eval = c.tool_uv;
+  p.pdf_out = c.tool_out;
+  p.n = n;
+  if ((s = grid_features(c, c.tool_q, nullptr, gdf_aabb{}, n, p, st))) return s;
+  e = gdf::launch_df_fused(df_shape(c), gdf::kModeEval, p, c.num_sms, st);
+  if (e != cudaSuccess) return cuda_fail(e, "df_fused (pdf image)");
+  e = gdf::launch_pdf_image(c.tool_out, image_dev, n, st);
+  if (e != cudaSuccess) return cuda_fail(e, "pdf image");
+  return GDF_OK;
+}
+
+gdf_status gdf_sample_histogram(gdf_ctx* ctx, const float* query_h, int64_t n_samples, uint64_t seed,
+                                int32_t width, int32_t height, uint32_t* counts_dev, float* dirs_dev,
+                                void* stream) {
+  if (!ctx) return fail(GDF_ERR_INVALID_ARG, "ctx is null");
+  gdf_status s;
+  if ((s = check_ptr(query_h, "query")) || (s = check_ptr(counts_dev, "counts"))) return s;
+  if (n_samples < 0) return fail(GDF_ERR_INVALID_ARG, "n_samples < 0");
+  if (width < 1 || height < 1 || static_cast<int64_t>(width) * height > (int64_t{1} << 26))
+    return fail(GDF_ERR_INVALID_ARG, "image size must be 1 .. 2^26 pixels");
+  Context& c = ctx->c;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  GDF_CUDA(cudaMemsetAsync(counts_dev, 0, static_cast<size_t>(width) * height * 4, st));
+  constexpr int64_t kChunk = int64_t{1} << 20;
+  if ((s = ensure_tools(c, std::min(n_samples, kChunk)))) return s;
+  for (int64_t b = 0; b < n_samples; b += kChunk) {
+    const int64_t m = std::min(kChunk, n_samples - b);
+    cudaError_t e = gdf::launch_replicate(query_row(query_h), c.tool_q, nullptr, c.tool_out, width, height, m, st);
+    if (e != cudaSuccess) return cuda_fail(e, "replicate");
+    gdf::DfKernelParams p = df_params(c);
+    p.queries = c.tool_q;
+    p.wi = c.tool_out;
+    p.n = m;
+    p.philox_seed = seed;
+    p.philox_offset = 0;
+    p.philox_row_base = b;
+    if ((s = grid_features(c, c.tool_q, nullptr, gdf_aabb{}, m, p, st))) return s;
+    e = gdf::launch_df_fused(df_shape(c), gdf::kModeInfer, p, c.num_sms, st);
+    if (e != cudaSuccess) return cuda_fail(e, "df_fused (sampling)");
+    e = gdf::launch_histogram(c.tool_out, m, width, height, counts_dev, dirs_dev ? dirs_dev + b * 2 : nullptr, st);
+    if (e != cudaSuccess) return cuda_fail(e, "histogram");
+  }
+  return GDF_OK;
+}
+
 gdf_status gdf_eval_pdf(gdf_ctx* ctx, const float* queries, const float* u, float* pdf_out,
                         int64_t n, void* stream) {
   if (!ctx) return fail(GDF_ERR_INVALID_ARG, "ctx is null");
@@ -893,6 +1003,8 @@ static gdf::AdamParams adam_params(Context& c, int id, const gdf_adam_config& a,
     p.il_net = id;
     p.il_features = n.features;
   }
+  p.lr_table = c.lr_table[id < 2 ? 0 : 1];
+  p.lr_table_n = c.lr_table_n[id < 2 ? 0 : 1];
   return p;
 }
 

@@ -92,6 +92,14 @@ struct Context {
   float* host_u = nullptr;       // [host_cap x 4]
   float* host_wi = nullptr;      // [host_cap x 4]
   cudaStream_t pipe[2] = {nullptr, nullptr};
+  // Adam step sizes by per-parameter step counter: [0] DF optimizer, [1] NRC
+  float* lr_table[2] = {nullptr, nullptr};
+  int32_t lr_table_n[2] = {0, 0};
+  // inputs and outputs of the distribution-inspection tools
+  int64_t tool_cap = 0;
+  float* tool_q = nullptr;       // [tool_cap x 9]
+  float* tool_uv = nullptr;      // [tool_cap x 2]
+  float* tool_out = nullptr;     // [tool_cap x 4]
   cudaEvent_t pipe_ev[3] = {nullptr, nullptr, nullptr};
 };
 

@@ -369,56 +369,128 @@ cudaError_t launch_bwd_t(const DfBwdParams& p, int ctas, cudaStream_t st) {
 }
 
 // ----------------------------------------------------------------- Adam
+// One parameter of AdamOptimizer::step (tcnn optimizers/adam.h:48-117)
+// followed by EmaOptimizer's update (ema.h:102-130). The step size for a
+// parameter whose own step counter is k, lr sqrt(1 - beta2^k) / (1 - beta1^k),
+// comes from a table filled by adam_lr_table_kernel with the same float
+// expression; past the table's end the value is lr exactly.
+__device__ __forceinline__ void adam_param(const AdamParams& p, bool matrix, float graw, float& wf,
+                                           float& m1, float& m2, uint32_t& step, __half& w16h,
+                                           __half& emah, double& sq) {
+  float g = graw / p.loss_scale;
+  sq += static_cast<double>(g) * g;
+  float w16;
+  if (matrix || g != 0.0f) {  // non-matrix parameters with a zero gradient are skipped
+    if (matrix) g += p.l2_reg * wf;
+    m1 = p.beta1 * m1 + (1 - p.beta1) * g;
+    m2 = p.beta2 * m2 + (1 - p.beta2) * (g * g);
+    const uint32_t cs = ++step;
+    const float lr = p.lr_table[cs < static_cast<uint32_t>(p.lr_table_n) ? cs : p.lr_table_n - 1];
+    const float eff = fminf(fmaxf(lr / (sqrtf(m2) + p.eps), 0.0f), 3.402823466e38f);
+    wf = wf - eff * m1;
+    w16h = __float2half_rn(wf);
+    w16 = __half2float(w16h);
+  } else {
+    w16 = __half2float(w16h);
+  }
+  emah = __float2half_rn((__half2float(emah) * p.ema_decay * p.debias_old + w16 * (1 - p.ema_decay)) *
+                         p.debias_new);
+}
+
+__global__ void adam_lr_table_kernel(float lr, float beta1, float beta2, float* table, int32_t n) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const float cs = static_cast<float>(k);
+  table[k] = lr * sqrtf(1 - powf(beta2, cs)) / (1 - powf(beta1, cs));
+}
+
 __global__ void adam_ema_kernel(const __grid_constant__ AdamParams p) {
   double local_sq = 0.0;
-  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < p.n;
-       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    float graw;
-    if (i < p.n_mlp) {
-      float s = 0.f;
-      for (int cta = 0; cta < p.n_partials; ++cta) s += p.partials[static_cast<size_t>(cta) * p.n_mlp + i];
-      graw = s;
-    } else {
-      graw = p.grid_grad[i - p.n_mlp];
-      p.grid_grad[i - p.n_mlp] = 0.f;
+  const int64_t tid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t nth = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  // MLP matrices: gradient = the per-CTA partials reduced in CTA order
+  for (int64_t i = tid; i < p.n_mlp; i += nth) {
+    float graw = 0.f;
+#pragma unroll 8
+    for (int cta = 0; cta < p.n_partials; ++cta) graw += p.partials[static_cast<size_t>(cta) * p.n_mlp + i];
+    float wf = p.master[i], m1 = p.m[i], m2 = p.v[i];
+    uint32_t step = p.step[i];
+    __half w16h = p.w16[i], emah = p.ema16[i];
+    adam_param(p, true, graw, wf, m1, m2, step, w16h, emah, local_sq);
+    p.master[i] = wf;
+    p.m[i] = m1;
+    p.v[i] = m2;
+    p.step[i] = step;
+    p.w16[i] = w16h;
+    p.ema16[i] = emah;
+    // re-layout for the tensor cores (canonical K-major per matrix)
+    int l = 0;
+    while (l + 1 < p.n_layers && i >= p.layer_off[l + 1]) ++l;
+    const uint32_t k = static_cast<uint32_t>(i - p.layer_off[l]);
+    const uint32_t cols = static_cast<uint32_t>(p.layer_cols[l]);
+    const uint32_t off = static_cast<uint32_t>(p.layer_off[l]) + canon_offset(k / cols, k % cols, cols);
+    p.blob_w16[off] = w16h;
+    p.blob_ema[off] = emah;
+  }
+  // grid tables: 4 parameters per thread and step, 16-byte accesses (the
+  // grid part starts at a multiple of 1024 parameters and has a multiple of
+  // 8 entries per level); the gradient is read and re-zeroed
+  const int64_t ng = p.n - p.n_mlp;
+  const int64_t ng4 = ng >> 2;
+  for (int64_t q = tid; q < ng4; q += nth) {
+    const int64_t j = q * 4, i = p.n_mlp + j;
+    const float4 g4 = *reinterpret_cast<const float4*>(p.grid_grad + j);
+    *reinterpret_cast<float4*>(p.grid_grad + j) = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 w4 = *reinterpret_cast<const float4*>(p.master + i);
+    float4 m4 = *reinterpret_cast<const float4*>(p.m + i);
+    float4 v4 = *reinterpret_cast<const float4*>(p.v + i);
+    uint4 s4 = *reinterpret_cast<const uint4*>(p.step + i);
+    uint2 h4 = *reinterpret_cast<const uint2*>(p.w16 + i);
+    uint2 e4 = *reinterpret_cast<const uint2*>(p.ema16 + i);
+    __half* hh = reinterpret_cast<__half*>(&h4);
+    __half* ee = reinterpret_cast<__half*>(&e4);
+    const float gg[4] = {g4.x, g4.y, g4.z, g4.w};
+    float* ww = &w4.x;
+    float* mm = &m4.x;
+    float* vv = &v4.x;
+    uint32_t* ss = &s4.x;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) adam_param(p, false, gg[t], ww[t], mm[t], vv[t], ss[t], hh[t], ee[t], local_sq);
+    *reinterpret_cast<float4*>(p.master + i) = w4;
+    *reinterpret_cast<float4*>(p.m + i) = m4;
+    *reinterpret_cast<float4*>(p.v + i) = v4;
+    *reinterpret_cast<uint4*>(p.step + i) = s4;
+    *reinterpret_cast<uint2*>(p.w16 + i) = h4;
+    *reinterpret_cast<uint2*>(p.ema16 + i) = e4;
+    if (p.grid_il != nullptr) {
+      // interleaved inference copy: entry e = [theta F | phi F]
+      if (p.il_features == 2) {
+        const int64_t e = j >> 1;
+        *reinterpret_cast<uint32_t*>(p.grid_il + e * 4 + p.il_net * 2) = e4.x;
+        *reinterpret_cast<uint32_t*>(p.grid_il + (e + 1) * 4 + p.il_net * 2) = e4.y;
+      } else {
+        const int64_t e = j >> 2;
+        *reinterpret_cast<uint2*>(p.grid_il + e * 8 + p.il_net * 4) = e4;
+      }
     }
-    float g = graw / p.loss_scale;
-    local_sq += static_cast<double>(g) * g;
-    const bool skip = i >= p.n_mlp && g == 0.0f;
-    float w16;
-    if (!skip) {
-      const float wf = p.master[i];
-      if (i < p.n_mlp) g += p.l2_reg * wf;
-      const float m1 = p.m[i] = p.beta1 * p.m[i] + (1 - p.beta1) * g;
-      const float m2 = p.v[i] = p.beta2 * p.v[i] + (1 - p.beta2) * (g * g);
-      const uint32_t cs = ++p.step[i];
-      const float lr = p.lr * sqrtf(1 - powf(p.beta2, static_cast<float>(cs))) /
-                       (1 - powf(p.beta1, static_cast<float>(cs)));
-      const float eff = fminf(fmaxf(lr / (sqrtf(m2) + p.eps), 0.0f), 3.402823466e38f);
-      const float nw = wf - eff * m1;
-      p.master[i] = nw;
-      const __half h = __float2half_rn(nw);
-      p.w16[i] = h;
-      w16 = __half2float(h);
-    } else {
-      w16 = __half2float(p.w16[i]);
-    }
-    const __half e = __float2half_rn((__half2float(p.ema16[i]) * p.ema_decay * p.debias_old +
-                                      w16 * (1 - p.ema_decay)) * p.debias_new);
-    p.ema16[i] = e;
-    if (i >= p.n_mlp && p.grid_il != nullptr) {
-      const int64_t j = i - p.n_mlp, F = p.il_features;
-      p.grid_il[(j / F) * 2 * F + p.il_net * F + j % F] = e;
-    }
-    if (i < p.n_mlp) {
-      // re-layout for the tensor cores (canonical K-major per matrix)
-      int l = 0;
-      while (l + 1 < p.n_layers && i >= p.layer_off[l + 1]) ++l;
-      const uint32_t k = static_cast<uint32_t>(i - p.layer_off[l]);
-      const uint32_t cols = static_cast<uint32_t>(p.layer_cols[l]);
-      const uint32_t off = static_cast<uint32_t>(p.layer_off[l]) + canon_offset(k / cols, k % cols, cols);
-      p.blob_w16[off] = __float2half_rn(w16);
-      p.blob_ema[off] = e;
+  }
+  for (int64_t j = ng4 * 4 + tid; j < ng; j += nth) {  // remainder (none for tcnn grid sizes)
+    const int64_t i = p.n_mlp + j;
+    const float graw = p.grid_grad[j];
+    p.grid_grad[j] = 0.f;
+    float wf = p.master[i], m1 = p.m[i], m2 = p.v[i];
+    uint32_t step = p.step[i];
+    __half w16h = p.w16[i], emah = p.ema16[i];
+    adam_param(p, false, graw, wf, m1, m2, step, w16h, emah, local_sq);
+    p.master[i] = wf;
+    p.m[i] = m1;
+    p.v[i] = m2;
+    p.step[i] = step;
+    p.w16[i] = w16h;
+    p.ema16[i] = emah;
+    if (p.grid_il != nullptr) {
+      const int64_t F = p.il_features;
+      p.grid_il[(j / F) * 2 * F + p.il_net * F + j % F] = emah;
     }
   }
   // per-block sum of squared gradients (FP64), reduced by the host-side kernel
@@ -481,6 +553,12 @@ size_t df_train_bwd_smem_bytes(int levels, int features, bool phi, uint32_t blob
   const int lf = levels * features;
   const int k0 = phi ? pad16t(lf + 40) : pad16t(lf + 28);
   return ((blob_bytes + 127u) & ~127u) + 128u * k0 * 2u + static_cast<size_t>(hidden + 1) * 128u * 64u * 2u + 64u;
+}
+
+cudaError_t launch_adam_lr_table(float lr, float beta1, float beta2, float* table, int32_t n,
+                                 cudaStream_t st) {
+  adam_lr_table_kernel<<<(n + 255) / 256, 256, 0, st>>>(lr, beta1, beta2, table, n);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_adam_ema(const AdamParams& p, cudaStream_t st) {

@@ -52,12 +52,18 @@ struct AdamParams {
   // nullable; this network's half is at il_net * F
   __half* grid_il;
   int32_t il_net, il_features;
+  // lr sqrt(1 - beta2^k) / (1 - beta1^k) for step counters k < lr_table_n;
+  // the last entry equals lr (both powers below float resolution)
+  const float* lr_table;
+  int32_t lr_table_n;
 };
 
 cudaError_t launch_df_train_bwd(const DfShape& s, bool phi, const DfBwdParams& p, int ctas,
                                 cudaStream_t st);
 size_t df_train_bwd_smem_bytes(int levels, int features, bool phi, uint32_t blob_bytes, int hidden);
 cudaError_t launch_adam_ema(const AdamParams& p, cudaStream_t st);
+cudaError_t launch_adam_lr_table(float lr, float beta1, float beta2, float* table, int32_t n,
+                                 cudaStream_t st);
 cudaError_t launch_train_stats(const float* fwd, int64_t n, const double* sq, int n_sq, double* out,
                                cudaStream_t st);
 

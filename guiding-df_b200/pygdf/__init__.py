@@ -154,6 +154,8 @@ def lib() -> C.CDLL:
             "gdf_train_loss_static": [P, P, P, P, C.c_int64, P, P, P],
             "gdf_infer_ex": [P, C.POINTER(InferArgs), P],
             "gdf_infer_host": [P, P, P, P, C.c_uint64, C.c_uint64, P, P, C.c_int64, P],
+            "gdf_pdf_image": [P, P, C.c_int32, C.c_int32, P, P],
+            "gdf_sample_histogram": [P, P, C.c_int64, C.c_uint64, C.c_int32, C.c_int32, P, P, P],
             "gdf_prepare_queries": [C.POINTER(Shading), C.POINTER(Aabb), P, C.c_int64, P],
             "gdf_build_train_records": [P, C.POINTER(PathState), C.POINTER(Aabb), C.POINTER(TrainPixels),
                                         P, P, P, C.c_int64, C.POINTER(C.c_int64), P],
@@ -281,6 +283,17 @@ class Context:
         n = queries.shape[0] if n is None else n
         check(lib().gdf_infer_host(self.h, _ptr(queries), _ptr(guided), _ptr(uniforms), seed, offset,
                                    _ptr(wi_in), _ptr(wi_out), n, _stream(stream)))
+
+    def pdf_image(self, query, width, height, image, stream=None):
+        import numpy as np
+        q = np.ascontiguousarray(query, dtype=np.float32)
+        check(lib().gdf_pdf_image(self.h, q.ctypes.data, width, height, _ptr(image), _stream(stream)))
+
+    def sample_histogram(self, query, n_samples, seed, width, height, counts, dirs=None, stream=None):
+        import numpy as np
+        q = np.ascontiguousarray(query, dtype=np.float32)
+        check(lib().gdf_sample_histogram(self.h, q.ctypes.data, n_samples, seed, width, height,
+                                         _ptr(counts), _ptr(dirs), _stream(stream)))
 
     def eval_pdf(self, queries, u, pdf_out, n=None, stream=None):
         n = queries.shape[0] if n is None else n

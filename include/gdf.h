@@ -271,6 +271,26 @@ gdf_status gdf_post_inference(gdf_ctx* ctx, const float* logits_theta_dev,
                               const float* uniforms_dev, float* wi_dev, int64_t n,
                               void* stream);
 
+/* LearnedDistribution::mouseOverInference (learnedDistribution.cpp:486-583)
+ * for one query row query_h[9] (host): the solid-angle pdf
+ * pdf_theta * pdf_phi / (4 pi) of the learned distribution at the centre of
+ * every pixel of a width x height image over the square of directions
+ * (pixel (x, y) at u = (x + 1/2) / width, v = (y + 1/2) / height,
+ * integrator.cpp:721-731), row-major into image_dev. At most 2^26 pixels. */
+gdf_status gdf_pdf_image(gdf_ctx* ctx, const float* query_h, int32_t width, int32_t height,
+                         float* image_dev, void* stream);
+
+/* LearnedDistribution::mouseOverSampling (learnedDistribution.cpp:585-654)
+ * with the integrator's binning (integrator.cpp:782-827): n_samples
+ * directions drawn from the learned distribution of query_h[9] (every draw
+ * guided, Philox uniforms keyed by seed, counter = sample index), counted
+ * into counts_dev[height][width] by pixel ((int)(u width), (int)(v height));
+ * counts are zeroed first. dirs_dev [n_samples x 2] (nullable) receives the
+ * samples. */
+gdf_status gdf_sample_histogram(gdf_ctx* ctx, const float* query_h, int64_t n_samples, uint64_t seed,
+                                int32_t width, int32_t height, uint32_t* counts_dev, float* dirs_dev,
+                                void* stream);
+
 /* --------------------------------------------------------------- training */
 
 /* One iteration of LearnedDistribution::trainStep (learnedDistribution.cpp:
