@@ -358,9 +358,9 @@ def _report(args, rank, world, dist, dev, n, cfg, params, times, e2e_times, trai
         flops = FLOP_PER_QUERY[args.workload] * n
         achieved = flops / (ms * 1e-3) / 1e12  # average launch duration
         traffic = None
-        prof = os.path.join(ROOT, "profiles", f"df_fused_{args.workload}.json")
+        prof = os.path.join(ROOT, "profiles", f"infer_step_{args.workload}.json")
         if os.path.exists(prof):
-            traffic = json.load(open(prof)).get("dram_bytes_per_launch")
+            traffic = json.load(open(prof)).get("dram_bytes_per_step")
         if args.cpu_seconds > 0:
             cpu_v, cpu_n, cpu_s = cpu_reference(args.workload, cfg, params, args.cpu_seconds, threads)
         else:

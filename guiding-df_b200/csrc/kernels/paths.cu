@@ -104,6 +104,24 @@ __device__ __forceinline__ void nrc_target(const gdf_record_fields& r, uint32_t 
   for (int c = 0; c < 3; ++c) L[c] = L[c] * bv[c] / den;
 }
 
+// A direction stored as (theta, phi) turns into a NaN through
+// sphericalToCartesian exactly when an angle is NaN or infinite (sin and cos
+// of finite floats are finite, and the unit-sphere maps that follow keep
+// finite vectors finite), so the validity tests of the producers need no
+// trigonometry: they test the stored angles.
+__device__ __forceinline__ bool angles_ok(const float* a, uint32_t p) {
+  return isfinite(a[2ull * p]) && isfinite(a[2ull * p + 1]);
+}
+
+__device__ __forceinline__ bool position_ok(const gdf_record_fields& r, uint32_t p, const rec::SceneFrame& f) {
+  float v[3], o[3];
+  load3(r.pos, p, v);
+  rec::normalize_spatial(v, f, o);
+  return !rec::any_nan(o, 3);
+}
+
+// The depths of one pixel that emit a record (bits 0-4: list A, 8-12: list
+// B); the same decisions as df_record / nrc_input / nrc_target make.
 template <int KIND>
 __device__ __forceinline__ uint32_t pixel_mask(const ProduceParams& P, uint32_t p, int depth,
                                                const rec::SceneFrame& f) {
@@ -113,13 +131,16 @@ __device__ __forceinline__ uint32_t pixel_mask(const ProduceParams& P, uint32_t 
     const gdf_record_fields& r = P.st.depth[d];
     if (r.delta[p]) continue;
     if constexpr (KIND == kRecordsDf) {
-      float in[9], pt, out[9];
-      if (df_record(r, p, f, P.bins_theta, P.linear != 0, in, pt, out)) mask |= 1u << d;
+      // train.cu:77-81: pos, wi, wo direction, wiPdf, L / thp * misWeight
+      float L[3];
+      local_radiance(r, p, L);
+      const float wi_pdf = r.wi_pdf[p];
+      const bool ok = position_ok(r, p, f) && angles_ok(r.dir, p) && angles_ok(r.wo, p) &&
+                      !isnan(wi_pdf) && wi_pdf != 0.0f && !rec::any_nan(L, 3);
+      if (ok) mask |= 1u << d;
     } else {
       if (r.miss[p]) continue;
-      float in[15];
-      nrc_input(r, p, f, in);
-      bool ok = !(rec::any_nan(in, 3) || rec::any_nan(in + 3, 3));
+      bool ok = position_ok(r, p, f) && angles_ok(r.wo, p);
       if constexpr (KIND == kRecordsNrcTrain) {
         float L[3];
         nrc_target(r, p, L);
@@ -207,63 +228,160 @@ __global__ void __launch_bounds__(kScanThreads) scan_blocks_kernel(const int32_t
   }
 }
 
+// Words staged per record: DF [GuidedInput 9 | GuidedInputPhi 10 |
+// GuidedOutput 9]; NRC list A [GuidedInputNRC 15 | depth | pixel], list B
+// [GuidedInputNRC 15 | RGB 3].
+template <int KIND> struct Stage;
+template <> struct Stage<kRecordsDf> { static constexpr int A = 28, B = 0; };
+template <> struct Stage<kRecordsNrcTrain> { static constexpr int A = 17, B = 18; };
+template <> struct Stage<kRecordsNrcQuery> { static constexpr int A = 17, B = 0; };
+// Staged records per warp: 32 pixels average about 2.3 records each with a
+// 0.7 survival per bounce, so 96 slots hold a warp's records nearly always;
+// records past slot 96 are written straight to memory.
+constexpr int kWarpRecords = 96;
+
+template <int KIND>
+constexpr size_t emit_smem_bytes() {
+  return static_cast<size_t>(kProduceBlock / 32) * kWarpRecords * (Stage<KIND>::A + Stage<KIND>::B) * 4u;
+}
+
+// Warp-cooperative copy of `words` staged words per record (stride `stride`
+// words, starting at word `first`) of records [0, n) to out + (base + r) * words:
+// the destination range is contiguous, so lane l writes words l, l + 32, ...
+template <typename T>
+__device__ __forceinline__ void warp_copy(const uint32_t* stage, int stride, int first, int words, int n,
+                                          int64_t base, int64_t cap, T* out, int lane) {
+  if (out == nullptr) return;
+  for (int w = lane; w < n * words; w += 32) {
+    const int r = w / words, k = w - r * words;
+    if (base + r < cap) out[(base + r) * words + k] = __uint_as_float(stage[r * stride + first + k]);
+  }
+}
+__device__ __forceinline__ void warp_copy_i(const uint32_t* stage, int stride, int first, int n, int64_t base,
+                                            int64_t cap, int32_t* out, int lane) {
+  if (out == nullptr) return;
+  for (int r = lane; r < n; r += 32)
+    if (base + r < cap) out[base + r] = static_cast<int32_t>(stage[r * stride + first]);
+}
+
+// Writes each record of this block's pixels. A warp's records are
+// contiguous in every output (pixel, then depth order), so they are staged
+// in shared memory and copied out with consecutive lanes on consecutive
+// words instead of scattered per-thread 36- to 60-byte rows.
 template <int KIND>
 __global__ void __launch_bounds__(kProduceBlock) produce_emit_kernel(const __grid_constant__ ProduceParams P) {
+  constexpr int SA = Stage<KIND>::A, SB = Stage<KIND>::B;
+  extern __shared__ uint32_t stage[];
   __shared__ int2 warp_sums[kProduceBlock / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t i = static_cast<int64_t>(blockIdx.x) * kProduceBlock + threadIdx.x;
   const uint32_t mask = i < P.n_train ? P.mask[i] : 0u;
   const int2 ca = make_int2(__popc(mask & 0xffu), __popc(mask >> 8));
-  const int2 inc = block_inclusive(ca, warp_sums, nullptr);
-  if (i >= P.n_train) return;
-  int64_t ia = P.block_offsets[2 * blockIdx.x] + inc.x - ca.x;
-  int64_t ib = P.block_offsets[2 * blockIdx.x + 1] + inc.y - ca.y;
-  const uint32_t p = P.offset + static_cast<uint32_t>(i) * P.stride;
-  const rec::SceneFrame f = rec::scene_frame(P.aabb);
-  for (int d = 0; d < GDF_MAX_TRAIN_DEPTH; ++d) {
-    const bool in_a = (mask >> d) & 1u, in_b = (mask >> (8 + d)) & 1u;
-    if (!in_a && !in_b) continue;
-    const gdf_record_fields& r = P.st.depth[d];
-    if constexpr (KIND == kRecordsDf) {
-      float in[9], pt, out[9];
-      df_record(r, p, f, P.bins_theta, P.linear != 0, in, pt, out);
-      if (ia < P.cap_a) {
+  // warp-inclusive scan, then the warp's base within the block
+  int2 inc = ca;
 #pragma unroll
-        for (int k = 0; k < 9; ++k) {
-          P.out_a0[ia * 9 + k] = in[k];
-          P.out_a1[ia * 10 + k] = in[k];
-          P.out_a2[ia * 9 + k] = out[k];
+  for (int o = 1; o < 32; o <<= 1) {
+    const int ax = __shfl_up_sync(0xffffffffu, inc.x, o);
+    const int ay = __shfl_up_sync(0xffffffffu, inc.y, o);
+    if (lane >= o) { inc.x += ax; inc.y += ay; }
+  }
+  const int2 wtot = make_int2(__shfl_sync(0xffffffffu, inc.x, 31), __shfl_sync(0xffffffffu, inc.y, 31));
+  if (lane == 31) warp_sums[warp] = wtot;
+  __syncthreads();
+  int64_t base_a = P.block_offsets[2 * blockIdx.x], base_b = P.block_offsets[2 * blockIdx.x + 1];
+  for (int w = 0; w < warp; ++w) { base_a += warp_sums[w].x; base_b += warp_sums[w].y; }
+  uint32_t* sa = stage + static_cast<size_t>(warp) * kWarpRecords * (SA + SB);
+  uint32_t* sb = sa + kWarpRecords * SA;
+  int ra = inc.x - ca.x, rb = inc.y - ca.y;  // this thread's first slot in the warp
+  if (i < P.n_train) {
+    const uint32_t p = P.offset + static_cast<uint32_t>(i) * P.stride;
+    const rec::SceneFrame f = rec::scene_frame(P.aabb);
+    for (int d = 0; d < GDF_MAX_TRAIN_DEPTH; ++d) {
+      const bool in_a = (mask >> d) & 1u, in_b = (mask >> (8 + d)) & 1u;
+      if (!in_a && !in_b) continue;
+      const gdf_record_fields& r = P.st.depth[d];
+      if constexpr (KIND == kRecordsDf) {
+        float in[9], pt, out[9];
+        df_record(r, p, f, P.bins_theta, P.linear != 0, in, pt, out);
+        if (ra < kWarpRecords) {
+          uint32_t* o = sa + ra * SA;
+#pragma unroll
+          for (int k = 0; k < 9; ++k) {
+            o[k] = __float_as_uint(in[k]);
+            o[9 + k] = __float_as_uint(in[k]);
+            o[19 + k] = __float_as_uint(out[k]);
+          }
+          o[18] = __float_as_uint(pt);
+        } else if (base_a + ra < P.cap_a) {
+          const int64_t g = base_a + ra;
+#pragma unroll
+          for (int k = 0; k < 9; ++k) {
+            P.out_a0[g * 9 + k] = in[k];
+            P.out_a1[g * 10 + k] = in[k];
+            P.out_a2[g * 9 + k] = out[k];
+          }
+          P.out_a1[g * 10 + 9] = pt;
         }
-        P.out_a1[ia * 10 + 9] = pt;
-      }
-      ++ia;
-    } else {
-      float in[15];
-      nrc_input(r, p, f, in);
-      if (in_a) {
-        if (ia < P.cap_a) {
+        ++ra;
+      } else {
+        float in[15];
+        nrc_input(r, p, f, in);
+        if (in_a) {
+          if (ra < kWarpRecords) {
+            uint32_t* o = sa + ra * SA;
 #pragma unroll
-          for (int k = 0; k < 15; ++k) P.out_a0[ia * 15 + k] = in[k];
-          P.a_depth[ia] = d;
-          P.a_pixel[ia] = static_cast<int32_t>(p);
+            for (int k = 0; k < 15; ++k) o[k] = __float_as_uint(in[k]);
+            o[15] = static_cast<uint32_t>(d);
+            o[16] = p;
+          } else if (base_a + ra < P.cap_a) {
+            const int64_t g = base_a + ra;
+#pragma unroll
+            for (int k = 0; k < 15; ++k) P.out_a0[g * 15 + k] = in[k];
+            P.a_depth[g] = d;
+            P.a_pixel[g] = static_cast<int32_t>(p);
+          }
+          ++ra;
         }
-        ++ia;
-      }
-      if (KIND == kRecordsNrcTrain && in_b) {
-        float L[3];
-        nrc_target(r, p, L);
-        if (ib < P.cap_b) {
+        if (KIND == kRecordsNrcTrain && in_b) {
+          float L[3];
+          nrc_target(r, p, L);
+          if (rb < kWarpRecords) {
+            uint32_t* o = sb + rb * SB;
 #pragma unroll
-          for (int k = 0; k < 15; ++k) P.out_b0[ib * 15 + k] = in[k];
+            for (int k = 0; k < 15; ++k) o[k] = __float_as_uint(in[k]);
 #pragma unroll
-          for (int k = 0; k < 3; ++k) P.out_b1[ib * 3 + k] = L[k];
+            for (int k = 0; k < 3; ++k) o[15 + k] = __float_as_uint(L[k]);
+          } else if (base_b + rb < P.cap_b) {
+            const int64_t g = base_b + rb;
+#pragma unroll
+            for (int k = 0; k < 15; ++k) P.out_b0[g * 15 + k] = in[k];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) P.out_b1[g * 3 + k] = L[k];
+          }
+          ++rb;
         }
-        ++ib;
       }
     }
+    // generate_training_data_nrc_with_inference / generate_NRCinput_from_
+    // training_data end with curDepth-- (train.cu:213, 261), unsigned.
+    if constexpr (KIND != kRecordsDf) P.st.cur_depth[p] = P.st.cur_depth[p] - 1u;
   }
-  // generate_training_data_nrc_with_inference / generate_NRCinput_from_
-  // training_data end with curDepth-- (train.cu:213, 261), unsigned.
-  if constexpr (KIND != kRecordsDf) P.st.cur_depth[p] = P.st.cur_depth[p] - 1u;
+  __syncwarp();
+  const int na = wtot.x < kWarpRecords ? wtot.x : kWarpRecords;
+  const int nb = wtot.y < kWarpRecords ? wtot.y : kWarpRecords;
+  if constexpr (KIND == kRecordsDf) {
+    warp_copy(sa, SA, 0, 9, na, base_a, P.cap_a, P.out_a0, lane);
+    warp_copy(sa, SA, 9, 10, na, base_a, P.cap_a, P.out_a1, lane);
+    warp_copy(sa, SA, 19, 9, na, base_a, P.cap_a, P.out_a2, lane);
+  } else {
+    warp_copy(sa, SA, 0, 15, na, base_a, P.cap_a, P.out_a0, lane);
+    warp_copy_i(sa, SA, 15, na, base_a, P.cap_a, P.a_depth, lane);
+    warp_copy_i(sa, SA, 16, na, base_a, P.cap_a, P.a_pixel, lane);
+    if constexpr (KIND == kRecordsNrcTrain) {
+      warp_copy(sb, SB, 0, 15, nb, base_b, P.cap_b, P.out_b0, lane);
+      warp_copy(sb, SB, 15, 3, nb, base_b, P.cap_b, P.out_b1, lane);
+    }
+  }
 }
 
 __global__ void prepare_queries_kernel(const gdf_shading s, const gdf_aabb aabb,
@@ -329,7 +447,11 @@ cudaError_t produce(const ProduceParams& p, cudaStream_t st) {
   if (nb == 0) return cudaMemsetAsync(p.totals, 0, 2 * sizeof(int64_t), st);
   produce_mask_kernel<KIND><<<static_cast<unsigned>(nb), kProduceBlock, 0, st>>>(p);
   scan_blocks_kernel<<<1, kScanThreads, 0, st>>>(p.block_counts, p.block_offsets, p.totals, nb);
-  produce_emit_kernel<KIND><<<static_cast<unsigned>(nb), kProduceBlock, 0, st>>>(p);
+  constexpr size_t smem = emit_smem_bytes<KIND>();
+  cudaError_t e = cudaFuncSetAttribute(produce_emit_kernel<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  produce_emit_kernel<KIND><<<static_cast<unsigned>(nb), kProduceBlock, smem, st>>>(p);
   return cudaGetLastError();
 }
 

@@ -14,7 +14,7 @@ enum RecordKind : int {
   kRecordsNrcQuery = 2,    // generate_NRCinput_from_training_data (train.cu:216-262)
 };
 
-constexpr int kProduceBlock = 256;
+constexpr int kProduceBlock = 128;
 
 // One record-production pass over the training pixels of a frame. List A
 // holds DF records (in_a0/in_a1/in_a2 = GuidedInput, GuidedInputPhi,

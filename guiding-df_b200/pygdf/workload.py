@@ -222,6 +222,8 @@ def path_state(n_pixels: int, seed: int, aabb=((-2.0, -1.0, -3.0), (4.0, 2.0, 1.
         poke("pos", 0.004, np.nan)
         poke("dir", 0.003, np.nan)
         poke("wo", 0.002, np.nan)
+        poke("wo", 0.001, np.inf)
+        poke("dir", 0.001, -np.inf)
         poke("L", 0.004, np.nan)
         poke("thp", 0.02, 1e-6)
         poke("wi_pdf", 0.01, 0.0)

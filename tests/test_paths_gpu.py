@@ -288,3 +288,38 @@ def test_infer_ex_dir_pdf_is_the_autoregressive_view():
     np.testing.assert_array_equal(d[:, 3], pdf.astype(np.float32))
     np.testing.assert_allclose(np.linalg.norm(d[:, :3], axis=1), 1.0, atol=4e-6)
     ctx.close()
+
+
+@pytest.mark.parametrize("kind", ["df", "nrc"])
+def test_dense_paths_match_oracle(kind):
+    """Every pixel five vertices deep, no delta or miss vertices: each warp
+    emits 160 records, more than the producer stages in shared memory, so
+    the direct-write path is exercised too."""
+    fields, depth = W.path_state(4000, 17, defects=False)
+    fields["delta"][:] = 0
+    fields["miss"][:] = 0
+    depth[:] = 5
+    cfg, ctx = _ctx()
+    f, cd, st = _state_dev(fields, depth)
+    cap = 4000 * 5
+    if kind == "df":
+        a, b, t = (dev(np.zeros((cap, k), np.float32)) for k in (9, 10, 9))
+        k = ctx.build_train_records(st, pygdf.Aabb.of(*AABB), _px(4000), a, b, t)
+        ra, rb, rt = O.build_df_records(fields, depth.copy(), AABB, 4000, 0, 1, cfg.n_bins_theta, True)
+        assert k == ra.shape[0] == cap
+        np.testing.assert_allclose(_host(a), ra, rtol=0, atol=TOL)
+        np.testing.assert_allclose(_host(b), rb, rtol=0, atol=TOL)
+        np.testing.assert_allclose(_host(t), rt, rtol=0, atol=TOL)
+    else:
+        qi, ti = dev(np.zeros((cap, 15), np.float32)), dev(np.zeros((cap, 15), np.float32))
+        qd, qp = (dev(np.zeros(cap, np.int32)) for _ in range(2))
+        tt = dev(np.zeros((cap, 3), np.float32))
+        kq, kt = ctx.build_nrc_records(st, pygdf.Aabb.of(*AABB), _px(4000), True, qi, qd, qp, ti, tt)
+        r = O.build_nrc_records(fields, depth.copy(), AABB, 4000, 0, 1, True)
+        assert kq == cap and kt == 4000 * 4
+        np.testing.assert_array_equal(_host(qd), r["q_depth"])
+        np.testing.assert_array_equal(_host(qp), r["q_pixel"])
+        np.testing.assert_allclose(_host(qi), r["q_in"], rtol=0, atol=TOL)
+        np.testing.assert_allclose(_host(ti)[:kt], r["t_in"], rtol=0, atol=TOL)
+        np.testing.assert_array_equal(_host(tt)[:kt], r["t_target"])
+    ctx.close()
