@@ -112,18 +112,27 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sms)}
 
 
-def make_context(workload: str, seed: int):
+def mlp_params(cfg, net: int) -> int:
+    """MLP parameters of a DF network in tcnn order: first layer 64 x k0
+    (encoded width padded to 16), hidden 64 x 64, output padded to 16 rows."""
+    lf = cfg.grid_theta.n_levels * cfg.grid_theta.n_features_per_level
+    k0 = (lf + 28 + (12 if net == 1 else 0) + 15) // 16 * 16
+    h = cfg.mlp_theta.n_hidden_layers if net == 0 else cfg.mlp_phi.n_hidden_layers
+    bins = cfg.n_bins_theta if net == 0 else cfg.n_bins_phi
+    return 64 * k0 + (h - 1) * 64 * 64 + (bins + 15) // 16 * 16 * 64
+
+
+def make_context(workload: str, seed: int, precision: int = 0):
     import pygdf
     preset = pygdf.PRESET_FULL if workload == "full" else pygdf.PRESET_SMALL
     cfg = pygdf.default_config(preset)
+    cfg.precision = precision
     ctx = pygdf.Context(cfg)
     rng = np.random.default_rng(seed)
-    import oracle as O
-    d = O.df_cfg_from(cfg)
     params = []
     for net in (0, 1):
         p = ctx.get_params(net)
-        n_mlp = O.df_mlp_params(d, net)
+        n_mlp = mlp_params(cfg, net)
         p[:n_mlp] *= 2.5
         p[n_mlp:] = rng.uniform(-0.5, 0.5, p.size - n_mlp).astype(np.float32)
         ctx.set_params(net, p)
@@ -162,7 +171,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="CPU-baseline sample length; 0 skips it (profiling runs)")
     ap.add_argument("--skip-e2e", action="store_true", help="profiling runs: kernel timing only")
-    ap.add_argument("--stages", default="infer,train,records",
+    ap.add_argument("--stages", default="infer,train,records,bf16",
                     help="comma list of infer, train, records (profiling runs select one)")
     args = ap.parse_args()
     stages = set(args.stages.split(","))
@@ -278,10 +287,29 @@ def main():
         train_times, last = time_train(ctx, cfg, W, nb, rank, dev, stream, flush, args)
     if "records" in stages:
         rec_times, n_rec, rec_bytes = time_records(ctx, W, n, rank, dev, stream, flush, args)
+    bf16_times = []
+    if "bf16" in stages:
+        # the same bounce with the bf16 inference form (MLP operands in bf16)
+        import pygdf
+        cb, _, _ = make_context(args.workload, seed=1234 + rank, precision=pygdf.PREC_BF16)
+        for i in range(args.warmup):
+            wi.copy_(wi0)
+            cb.infer(q, wi, guided=guided, seed=7, offset=i, n=n, stream=stream)
+        for i in range(args.steps):
+            wi.copy_(wi0)
+            flush.zero_()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            cb.infer(q, wi, guided=guided, seed=7, offset=1000 + i, n=n, stream=stream)
+            e.record(stream)
+            e.synchronize()
+            bf16_times.append(s.elapsed_time(e))
+        cb.sync(stream)
+        cb.close()
     clk = clocks.stop()
     ctx.sync(stream)
     _report(args, rank, world, dist, dev, n, cfg, params, times, e2e_times, train_times, rec_times,
-            last, n_rec, rec_bytes, clk, nb, workload_name, threads, q_h, wi_h, guided_h)
+            last, n_rec, rec_bytes, clk, nb, workload_name, threads, q_h, wi_h, guided_h, bf16_times)
     ctx.close()
     if dist:
         dist.destroy_process_group()
@@ -340,7 +368,7 @@ def time_records(ctx, W, n, rank, dev, stream, flush, args):
 
 
 def _report(args, rank, world, dist, dev, n, cfg, params, times, e2e_times, train_times, rec_times,
-            last, n_rec, rec_bytes, clk, nb, workload_name, threads, q_h, wi_h, guided_h):
+            last, n_rec, rec_bytes, clk, nb, workload_name, threads, q_h, wi_h, guided_h, bf16_times):
     import torch
     ms = statistics.mean(times)
     ms_e2e = statistics.mean(e2e_times) if e2e_times else float("nan")
@@ -396,6 +424,11 @@ def _report(args, rank, world, dist, dev, n, cfg, params, times, e2e_times, trai
                 "achieved_gbs": rec_bytes / (ms_rec * 1e-3) / 1e9,
                 "frac_hbm": rec_bytes / (ms_rec * 1e-3) / 1e9 / peaks["hbm_gbs"],
                 "launches_per_step": 3}
+        if bf16_times:
+            mb = statistics.mean(bf16_times)
+            line["bf16"] = {"metric": "guided queries/s, bf16 MLP operands (fp32 accumulation)",
+                            "value": n * world / (mb * 1e-3), "unit": "queries/s", "ms_per_step": mb,
+                            "vs_fp16": ms / mb}
         line.update({
             "clocks": clk,
             "gpu_launches": 2 * args.steps,  # grid features + fused kernel per step

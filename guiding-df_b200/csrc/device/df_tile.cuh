@@ -11,6 +11,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
 #include "df_math.cuh"
@@ -32,15 +33,26 @@ __device__ __forceinline__ uint32_t elem_off(uint32_t row, uint32_t col, uint32_
   return chunk_off(row, col >> 3, K) + ((col & 7u) << 1);
 }
 
+// Two values rounded to the MLP operand format (fp16, or bf16 for the
+// bf16 inference form), packed low-first.
+__device__ __forceinline__ uint32_t pack2(float a, float b, bool bf16) {
+  if (bf16) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<const uint32_t*>(&h);
+  }
+  const __half2 h = __floats2half2_rn(a, b);
+  return *reinterpret_cast<const uint32_t*>(&h);
+}
+
 __device__ __forceinline__ void store_h2(uint8_t* t, uint32_t row, uint32_t col, uint32_t K, float a,
-                                         float b) {
-  *reinterpret_cast<__half2*>(t + elem_off(row, col, K)) = __floats2half2_rn(a, b);
+                                         float b, bool bf16 = false) {
+  *reinterpret_cast<uint32_t*>(t + elem_off(row, col, K)) = pack2(a, b, bf16);
 }
 
 // Stores n (even) consecutive values starting at column col (even).
 __device__ __forceinline__ void store_run(uint8_t* t, uint32_t row, uint32_t col, uint32_t K,
-                                          const float* v, int n) {
-  for (int i = 0; i < n; i += 2) store_h2(t, row, col + i, K, v[i], v[i + 1]);
+                                          const float* v, int n, bool bf16 = false) {
+  for (int i = 0; i < n; i += 2) store_h2(t, row, col + i, K, v[i], v[i + 1], bf16);
 }
 
 // ------------------------------------------------------------------ grid
@@ -250,18 +262,18 @@ __device__ __forceinline__ void grids_to_tiles(const GridLevels& gt, const __hal
 
 // SH(16) of q[3..5] and OneBlob(4 bins) of q[6..8] at columns [col, col+28).
 __device__ __forceinline__ void sh_ob_to_tile(const float* q, uint8_t* tile, uint32_t row,
-                                              uint32_t col, uint32_t K) {
+                                              uint32_t col, uint32_t K, bool bf16 = false) {
   float v[28];
   sh4_encode(q[3], q[4], q[5], v);
   oneblob_encode<4>(q[6], v + 16);
   oneblob_encode<4>(q[7], v + 20);
   oneblob_encode<4>(q[8], v + 24);
-  store_run(tile, row, col, K, v, 28);
+  store_run(tile, row, col, K, v, 28, bf16);
 }
 
 __device__ __forceinline__ void ones_to_tile(uint8_t* tile, uint32_t row, uint32_t col0,
-                                             uint32_t col1, uint32_t K) {
-  for (uint32_t c = col0; c < col1; c += 2) store_h2(tile, row, c, K, 1.f, 1.f);
+                                             uint32_t col1, uint32_t K, bool bf16 = false) {
+  for (uint32_t c = col0; c < col1; c += 2) store_h2(tile, row, c, K, 1.f, 1.f, bf16);
 }
 
 // ------------------------------------------------------------- warpgroup
@@ -278,6 +290,7 @@ struct Wg {
   uint32_t row;
   bool leader;
   uint32_t* err;
+  bool bf16;           // MLP operands in bf16 (inference form); fp16 otherwise
 };
 
 // One K segment of an MMA's A operand: `ksteps` K=16 steps read from a
@@ -301,7 +314,7 @@ __device__ __forceinline__ void issue(Wg& c, const ASeg* segs, int nseg, uint32_
                                       uint32_t N) {
   if (!c.leader) return;
   tc_fence_after();
-  const uint32_t idesc = idesc_f16(128, N, 0, 0, 0);
+  const uint32_t idesc = idesc_f16(128, N, c.bf16 ? 1u : 0u, 0, 0);  // A and B share one type
   const uint32_t bsbo = Kw * 16u;
   int s = 0;
   for (int g = 0; g < nseg; ++g) {
@@ -330,16 +343,28 @@ __device__ __forceinline__ void relu_to_tile(Wg& c) {
     tmem_ld_wait();
 #pragma unroll
     for (int kc = 0; kc < 4; ++kc) {
-      __half2 v[4];
+      uint32_t v[4];
       // ReLU after rounding: max(round(x), 0) = round(max(x, 0)), and
       // __hmax2 maps NaN to 0 like tcnn's relu (x > 0 ? x : 0)
+      if (c.bf16) {
 #pragma unroll
-      for (int j = 0; j < 4; ++j)
-        v[j] = __hmax2(__floats2half2_rn(__uint_as_float(r[kc * 8 + 2 * j]),
-                                         __uint_as_float(r[kc * 8 + 2 * j + 1])),
-                       __float2half2_rn(0.f));
+        for (int j = 0; j < 4; ++j) {
+          const __nv_bfloat162 b = __hmax2(__floats2bfloat162_rn(__uint_as_float(r[kc * 8 + 2 * j]),
+                                                                 __uint_as_float(r[kc * 8 + 2 * j + 1])),
+                                           __float2bfloat162_rn(0.f));
+          v[j] = *reinterpret_cast<const uint32_t*>(&b);
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const __half2 b = __hmax2(__floats2half2_rn(__uint_as_float(r[kc * 8 + 2 * j]),
+                                                      __uint_as_float(r[kc * 8 + 2 * j + 1])),
+                                    __float2half2_rn(0.f));
+          v[j] = *reinterpret_cast<const uint32_t*>(&b);
+        }
+      }
       *reinterpret_cast<uint4*>(c.tile_a + chunk_off(c.row, h * 4 + kc, 64)) =
-          *reinterpret_cast<uint4*>(v);
+          make_uint4(v[0], v[1], v[2], v[3]);
     }
   }
   tc_fence_before();

@@ -103,6 +103,8 @@ gdf_status validate(const gdf_config& c) {
       return fail(GDF_ERR_INVALID_ARG, "Adam betas must lie in [0, 1)");
   if (c.precision < GDF_PREC_FP16 || c.precision > GDF_PREC_FP8)
     return fail(GDF_ERR_INVALID_ARG, "precision");
+  if (c.precision == GDF_PREC_FP8)
+    return fail(GDF_ERR_UNSUPPORTED, "the FP8 inference form is not built; use FP16 or BF16");
   if (c.max_queries < 0 || c.max_train_batch < 0)
     return fail(GDF_ERR_INVALID_ARG, "negative capacity");
   const int64_t cap = c.max_train_batch > 0 ? c.max_train_batch : 65536;
@@ -201,7 +203,7 @@ gdf_status alloc_net(Net& n) {
 // Re-packs the tensor-core weight blobs from the fp16 copies.
 gdf_status repack(Net& n, cudaStream_t st) {
   cudaError_t e = gdf::launch_pack_mlp(n.ema16, n.blob_ema, n.rows.data(), n.cols.data(),
-                                       static_cast<int>(n.rows.size()), st);
+                                       static_cast<int>(n.rows.size()), st, n.infer_bf16);
   if (e != cudaSuccess) return cuda_fail(e, "pack ema");
   e = gdf::launch_pack_mlp(n.w16, n.blob_w16, n.rows.data(), n.cols.data(),
                            static_cast<int>(n.rows.size()), st);
@@ -512,6 +514,7 @@ static gdf_status grid_features(Context& c, const float* queries, const gdf_shad
   g.n_tiles = tiles;
   g.grid_il = c.grid_il;
   g.gl = c.net[0].gl;
+  g.bf16 = c.cfg.precision == GDF_PREC_BF16;
   g.feat_theta = c.feat + tile_base * 128 * feat_row_halves(c);
   g.feat_phi = c.feat + (c.feat_tiles + tile_base) * 128 * feat_row_halves(c);
   cudaError_t e = gdf::launch_grid_features(df_shape(c), g, st);
@@ -548,6 +551,7 @@ gdf_status gdf_create(const gdf_config* cfg, gdf_ctx** out) {
   };
   if ((s = layout_df_net(c.cfg, 0, c.net[0])) || (s = layout_df_net(c.cfg, 1, c.net[1])))
     return cleanup(s);
+  c.net[0].infer_bf16 = c.net[1].infer_bf16 = c.cfg.precision == GDF_PREC_BF16;
   if (c.cfg.nrc_enable && (s = layout_nrc_net(c.cfg, c.net[2]))) return cleanup(s);
   for (Net& n : c.net)
     if (n.present && (s = alloc_net(n))) return cleanup(s);
@@ -690,6 +694,7 @@ static gdf::DfKernelParams df_params(Context& c) {
   p.gl_theta = t.gl;
   p.gl_phi = f.gl;
   p.err = c.d_err;
+  p.bf16 = c.cfg.precision == GDF_PREC_BF16;
   return p;
 }
 
@@ -1005,6 +1010,7 @@ static gdf::AdamParams adam_params(Context& c, int id, const gdf_adam_config& a,
   }
   p.lr_table = c.lr_table[id < 2 ? 0 : 1];
   p.lr_table_n = c.lr_table_n[id < 2 ? 0 : 1];
+  p.blob_ema_bf16 = n.infer_bf16;
   return p;
 }
 

@@ -34,6 +34,7 @@ struct Net {
   __half* blob_ema = nullptr;  // n_mlp, canonical tensor-core layout of ema16
   __half* blob_w16 = nullptr;  // n_mlp, canonical layout of w16
   uint32_t blob_bytes = 0;
+  bool infer_bf16 = false;     // blob_ema holds bf16 (bf16 inference form, DF networks)
   uint32_t opt_step = 0;       // optimizer step counter (Adam m_current_step)
 };
 

@@ -18,6 +18,7 @@
 //     ReLU, rounds to fp16 and writes the next layer's A operand; after the
 //     last layer the row's logits stay in registers for the softmax / CDF /
 //     sampling epilogue.
+#include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
 #include "../device/df_math.cuh"
@@ -57,7 +58,7 @@ struct DfWidths {
 //   5. phi input rest (SH | OneBlob | TriangleWave(u_theta) | 1-pad) -> tile A;
 //      phi layer 0 reads K steps from tile P then tile A;
 //   6. phi layers, epilogue -> u_phi, pdf_phi -> guiding data.
-template <int L, int F, int NBT, int NBP, bool LINEAR, int MODE, int WGS>
+template <int L, int F, int NBT, int NBP, bool LINEAR, int MODE, int WGS, bool BF16>
 __global__ void __launch_bounds__(128 * WGS, 1) df_fused_kernel(const __grid_constant__ DfKernelParams p) {
   using Wd = DfWidths<L, F>;
   constexpr uint32_t LF = L * F;
@@ -123,6 +124,7 @@ __global__ void __launch_bounds__(128 * WGS, 1) df_fused_kernel(const __grid_con
   c.row = tid & 127u;
   c.leader = c.row == 0;
   c.err = p.err;
+  c.bf16 = kFeat && BF16;  // operand format of the inference forms
   const uint32_t w_theta = smem_addr(smem);
   const uint32_t w_phi = smem_addr(smem + off_phi);
   const uint32_t w_theta_hidden = w_theta + 64u * KT * 2u;
@@ -189,8 +191,8 @@ __global__ void __launch_bounds__(128 * WGS, 1) df_fused_kernel(const __grid_con
 
     // ---- 1. theta input (grid features | SH | OneBlob | 1-pad), layer 0
     if constexpr (kFeat) {
-      tile::sh_ob_to_tile(q, c.tile_a, c.row, 0, KTR);
-      tile::ones_to_tile(c.tile_a, c.row, 28, KTR, KTR);
+      tile::sh_ob_to_tile(q, c.tile_a, c.row, 0, KTR, c.bf16);
+      tile::ones_to_tile(c.tile_a, c.row, 28, KTR, KTR, c.bf16);
       mbar_wait(fbar, fphase, p.err, kErrMbarTimeout);
       fphase ^= 1u;
       tile::publish(c);
@@ -245,13 +247,13 @@ __global__ void __launch_bounds__(128 * WGS, 1) df_fused_kernel(const __grid_con
     }
 
     // ---- 5. phi input rest, layer 0 over tile P (grid) + tile A (rest)
-    tile::sh_ob_to_tile(qp, c.tile_a, c.row, 0, KR);
+    tile::sh_ob_to_tile(qp, c.tile_a, c.row, 0, KR, c.bf16);
     {
       float tw[12];
       triangle_wave_encode<12>(cond, tw);
-      tile::store_run(c.tile_a, c.row, 28, KR, tw, 12);
+      tile::store_run(c.tile_a, c.row, 28, KR, tw, 12, c.bf16);
     }
-    tile::ones_to_tile(c.tile_a, c.row, 40, KR, KR);
+    tile::ones_to_tile(c.tile_a, c.row, 40, KR, KR, c.bf16);
     tile::publish(c);
     {
       const tile::ASeg a[2] = {{c.tile_p_s, LF, static_cast<int>(LF / 16)},
@@ -331,11 +333,16 @@ __global__ void df_post_kernel(const float* __restrict__ lt_in, const float* __r
 }
 
 __global__ void pack_mlp_kernel(const __half* __restrict__ src, __half* __restrict__ dst, int32_t rows,
-                                int32_t cols, int64_t n) {
+                                int32_t cols, int64_t n, bool to_bf16) {
   const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const uint32_t r = static_cast<uint32_t>(i / cols), cc = static_cast<uint32_t>(i % cols);
-  dst[canon_offset(r, cc, static_cast<uint32_t>(cols))] = src[i];
+  __half v = src[i];
+  if (to_bf16) {  // bf16 inference form: the fp16 value rounded to bf16, stored bit for bit
+    const __nv_bfloat16 b = __float2bfloat16_rn(__half2float(v));
+    v = *reinterpret_cast<const __half*>(&b);
+  }
+  dst[canon_offset(r, cc, static_cast<uint32_t>(cols))] = v;
 }
 
 template <int L, int F, int NBT, int NBP, bool LIN>
@@ -344,9 +351,14 @@ cudaError_t launch_t(int mode, const DfKernelParams& p, size_t smem, int num_sms
   int64_t ctas = (n_tiles + kDfWarpgroups - 1) / kDfWarpgroups;
   if (ctas > num_sms) ctas = num_sms;
   if (ctas < 1) ctas = 1;
-  auto kern = mode == kModeInfer  ? df_fused_kernel<L, F, NBT, NBP, LIN, kModeInfer, kDfWarpgroups>
-              : mode == kModeEval ? df_fused_kernel<L, F, NBT, NBP, LIN, kModeEval, kDfWarpgroups>
-                                  : df_fused_kernel<L, F, NBT, NBP, LIN, kModeTrainFwd, kDfWarpgroups>;
+  const bool bf = p.bf16 != 0 && mode != kModeTrainFwd;
+  auto kern = mode == kModeInfer
+                  ? (bf ? df_fused_kernel<L, F, NBT, NBP, LIN, kModeInfer, kDfWarpgroups, true>
+                        : df_fused_kernel<L, F, NBT, NBP, LIN, kModeInfer, kDfWarpgroups, false>)
+              : mode == kModeEval
+                  ? (bf ? df_fused_kernel<L, F, NBT, NBP, LIN, kModeEval, kDfWarpgroups, true>
+                        : df_fused_kernel<L, F, NBT, NBP, LIN, kModeEval, kDfWarpgroups, false>)
+                  : df_fused_kernel<L, F, NBT, NBP, LIN, kModeTrainFwd, kDfWarpgroups, false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
   if (e != cudaSuccess) return e;
@@ -412,10 +424,11 @@ cudaError_t launch_df_post(int nbt, int nbp, bool linear, const float* lt, const
 }
 
 cudaError_t launch_pack_mlp(const __half* src, __half* dst, const int32_t* rows, const int32_t* cols,
-                            int n_layers, cudaStream_t st) {
+                            int n_layers, cudaStream_t st, bool to_bf16) {
   for (int l = 0; l < n_layers; ++l) {
     const int64_t n = static_cast<int64_t>(rows[l]) * cols[l];
-    pack_mlp_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, st>>>(src, dst, rows[l], cols[l], n);
+    pack_mlp_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, st>>>(src, dst, rows[l], cols[l], n,
+                                                                            to_bf16);
     src += n;
     dst += n;
   }

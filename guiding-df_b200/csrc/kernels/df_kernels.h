@@ -49,6 +49,7 @@ struct DfKernelParams {
   gdf_shading shading;               // raw shading points when shading.pos != nullptr
   gdf_aabb aabb;
   float* dir_pdf;                    // n x 4 world direction + solid-angle pdf, nullable
+  int32_t bf16;                      // inference form with bf16 MLP operands
 };
 
 struct GridFeatParams {
@@ -60,6 +61,7 @@ struct GridFeatParams {
   GridLevels gl;             // the grid configuration both networks share
   __half* feat_theta;        // [n_tiles][128 x L*F] canonical
   __half* feat_phi;
+  int32_t bf16;              // features rounded to bf16 (bit patterns in __half storage)
 };
 
 struct DfShape {
@@ -84,8 +86,10 @@ cudaError_t launch_df_post(int bins_theta, int bins_phi, bool linear, const floa
                            const float* logits_phi, const uint8_t* guided, const float* uniforms,
                            float* wi, int64_t n, cudaStream_t stream);
 
-// Packs fp16 row-major [rows x cols] matrices into the canonical layout.
+// Packs fp16 row-major [rows x cols] matrices into the canonical layout,
+// optionally rounded to bf16 (bf16 inference form).
 cudaError_t launch_pack_mlp(const __half* src, __half* dst, const int32_t* rows,
-                            const int32_t* cols, int n_layers, cudaStream_t stream);
+                            const int32_t* cols, int n_layers, cudaStream_t stream,
+                            bool to_bf16 = false);
 
 }  // namespace gdf

@@ -20,6 +20,7 @@
 // adam_ema_kernel: Adam (tcnn optimizers/adam.h:48-117) + EMA (ema.h:63-130)
 // over one network, fused with the gradient reduction, the re-zeroing of the
 // grid gradient and the re-layout of the MLP weights for the tensor cores.
+#include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
 #include "../device/df_math.cuh"
@@ -430,7 +431,12 @@ __global__ void adam_ema_kernel(const __grid_constant__ AdamParams p) {
     const uint32_t cols = static_cast<uint32_t>(p.layer_cols[l]);
     const uint32_t off = static_cast<uint32_t>(p.layer_off[l]) + canon_offset(k / cols, k % cols, cols);
     p.blob_w16[off] = w16h;
-    p.blob_ema[off] = emah;
+    if (p.blob_ema_bf16) {
+      const __nv_bfloat16 b = __float2bfloat16_rn(__half2float(emah));
+      p.blob_ema[off] = *reinterpret_cast<const __half*>(&b);
+    } else {
+      p.blob_ema[off] = emah;
+    }
   }
   // grid tables: 4 parameters per thread and step, 16-byte accesses (the
   // grid part starts at a multiple of 1024 parameters and has a multiple of

@@ -54,10 +54,8 @@ __global__ void __launch_bounds__(256, 4) grid_features_kernel(const __grid_cons
     tile::grid_level_pair<F>(gl, chunk * LPC + j, gl.interp, p.grid_il, pos[0], pos[1], pos[2], ft, fp);
 #pragma unroll
     for (int k = 0; k < F; k += 2) {
-      const __half2 a = __floats2half2_rn(ft[k], ft[k + 1]);
-      const __half2 b = __floats2half2_rn(fp[k], fp[k + 1]);
-      pt[(j * F + k) / 2] = *reinterpret_cast<const uint32_t*>(&a);
-      pp[(j * F + k) / 2] = *reinterpret_cast<const uint32_t*>(&b);
+      pt[(j * F + k) / 2] = tile::pack2(ft[k], ft[k + 1], p.bf16 != 0);
+      pp[(j * F + k) / 2] = tile::pack2(fp[k], fp[k + 1], p.bf16 != 0);
     }
   }
   const int64_t off = (row >> 7) * (128 * LF) +

@@ -56,6 +56,7 @@ struct AdamParams {
   // the last entry equals lr (both powers below float resolution)
   const float* lr_table;
   int32_t lr_table_n;
+  bool blob_ema_bf16;       // the inference blob holds bf16 (bf16 inference form)
 };
 
 cudaError_t launch_df_train_bwd(const DfShape& s, bool phi, const DfBwdParams& p, int ctas,

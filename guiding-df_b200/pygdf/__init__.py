@@ -21,6 +21,7 @@ STATUS = {0: "OK", 1: "INVALID_ARG", 2: "OOM_BUDGET", 3: "CUDA", 4: "TIMEOUT", 5
 PRESET_SMALL, PRESET_FULL, PRESET_REFERENCE = 0, 1, 2
 NET_THETA, NET_PHI, NET_NRC = 0, 1, 2
 PDF_LINEAR, PDF_NEAREST = 0, 1
+PREC_FP16, PREC_BF16, PREC_FP8 = 0, 1, 2
 
 
 class GridConfig(C.Structure):

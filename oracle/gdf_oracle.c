@@ -339,7 +339,7 @@ void go_df_encode(const go_df_config* c, const go_grid* g, int net, const float*
     o += c->tw_frequencies;
   }
   for (; o < k0; ++o) tmp[o] = 1.0;
-  for (int i = 0; i < k0; ++i) out[i] = go_round_f16(tmp[i]);
+  for (int i = 0; i < k0; ++i) out[i] = go_store(tmp[i]);
 }
 
 /* NRC composite (common/configs/nn/base_hashgrid_nrc_df.json):
@@ -359,6 +359,30 @@ void go_nrc_encode(const go_nrc_config* c, const float* q15, float* out) {
 
 /* kernel_mlp_fused (tcnn/src/fully_fused_mlp.cu:500-556): ReLU hidden layers,
  * linear output, no biases; hidden activations stored as fp16. */
+/* Number format of the DF networks' stored MLP inputs and activations:
+ * 0 = fp16 (the reference's precision_t), 1 = bf16 (round to nearest
+ * even), 2 = unrounded (kept in fp32 beside the FP64 accumulation: the
+ * reference point of the precision comparison). */
+static int g_storage = 0;
+void go_set_storage(int fmt) { g_storage = fmt; }
+
+float go_round_bf16(float x) {
+  uint32_t u;
+  memcpy(&u, &x, 4);
+  if ((u & 0x7f800000u) == 0x7f800000u) return x; /* inf / nan */
+  u += 0x7fffu + ((u >> 16) & 1u);
+  u &= 0xffff0000u;
+  float r;
+  memcpy(&r, &u, 4);
+  return r;
+}
+
+float go_store(double x) {
+  if (g_storage == 1) return go_round_bf16((float)x);
+  if (g_storage == 2) return (float)x;
+  return go_round_f16(x);
+}
+
 /* Accumulation model of go_mlp_forward: 0 = FP64 (checker), 1 = sequential
  * FP32 (an emulation of a tensor-core kernel's accumulation, used only to
  * calibrate test tolerances). */
@@ -385,7 +409,7 @@ void go_mlp_forward(const float* w16, int k0, int width, int n_hidden, int n_out
   for (int l = 0; l < n_hidden; ++l) {
     for (int o = 0; o < width; ++o) {
       const double acc = dot_acc(w + (size_t)o * k, h, k);
-      hn[o] = go_round_f16(acc > 0.0 ? acc : 0.0);
+      hn[o] = go_store(acc > 0.0 ? acc : 0.0);
     }
     w += (size_t)width * k;
     k = width;

@@ -133,6 +133,12 @@ void go_nrc_query(const go_nrc_config* c, const float* params16, const float* in
                   int64_t m, int n_threads);
 
 
+/* Storage format of the DF networks' MLP inputs/activations: 0 fp16,
+ * 1 bf16, 2 unrounded. */
+void go_set_storage(int fmt);
+float go_round_bf16(float x);
+float go_store(double x);
+
 /* ---- path records (gdf_oracle_paths.c) ---------------------------------- */
 /* Host copy of GuidedPixelStateBuffer: each field is [5][n][k] (depth-major). */
 typedef struct go_paths {

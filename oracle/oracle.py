@@ -91,6 +91,7 @@ def lib():
             ("go_round_f16", [C.c_double], C.c_float),
             ("go_df_pdf_tables", [C.POINTER(DfCfg), P, P, P, P, P, P, C.c_int64], None),
             ("go_set_accumulation", [C.c_int], None),
+            ("go_set_storage", [C.c_int], None),
             ("go_df_train_grads", [C.POINTER(DfCfg), P, P, P, P, P, C.c_int64, C.c_float, P, P, P, P, P, P],
              C.c_int64),
             ("go_dlogits", [P, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float, P], None),
@@ -162,17 +163,53 @@ def df_mlp_params(d: DfCfg, net: int) -> int:
     return int(lib().go_df_mlp_params(C.byref(d), net))
 
 
+STORAGE = {"fp16": 0, "bf16": 1, "none": 2}
+
+
+def round_bf16(a) -> np.ndarray:
+    """Round to nearest even bf16, as cvt.rn.bf16.f32."""
+    x = np.ascontiguousarray(a, dtype=np.float32).copy()
+    u = x.view(np.uint32)
+    fin = (u & 0x7F800000) != 0x7F800000
+    r = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+    u[fin] = r[fin].astype(np.uint32)
+    return x
+
+
+def df_weights(d: DfCfg, net: int, params, storage: str = "fp16") -> np.ndarray:
+    """Inference weights of one DF network: the fp16 EMA copy; in bf16 the
+    MLP matrices are that copy rounded to bf16 (the grid tables stay fp16)."""
+    w = round_f16(params)
+    if storage == "bf16":
+        m = df_mlp_params(d, net)
+        w[:m] = round_bf16(w[:m])
+    return w
+
+
+class _storage:
+    def __init__(self, fmt: str):
+        self.fmt = STORAGE[fmt]
+
+    def __enter__(self):
+        lib().go_set_storage(self.fmt)
+
+    def __exit__(self, *exc):
+        lib().go_set_storage(0)
+
+
 def infer(d: DfCfg, p_theta, p_phi, queries, wi, guided=None, uniforms=None, n_threads=0,
-          edge_gap=False):
-    """gdf_infer restated; params are fp32 and rounded to fp16 here (EMA copy)."""
-    pt, pp = round_f16(p_theta), round_f16(p_phi)
+          edge_gap=False, storage: str = "fp16"):
+    """gdf_infer restated; params are fp32 and rounded to the inference
+    format here (fp16 EMA copy, bf16 MLP matrices in the bf16 form)."""
+    pt, pp = df_weights(d, 0, p_theta, storage), df_weights(d, 1, p_phi, storage)
     q = f32(queries)
     w = f32(wi).copy()
     g = None if guided is None else np.ascontiguousarray(guided, dtype=np.uint8)
     u = f32(uniforms)
     n = q.shape[0]
     gap = np.empty((n, 2), dtype=np.float32) if edge_gap else None
-    lib().go_infer(C.byref(d), _p(pt), _p(pp), _p(q), _p(g), _p(u), _p(w), _p(gap), n, n_threads)
+    with _storage(storage):
+        lib().go_infer(C.byref(d), _p(pt), _p(pp), _p(q), _p(g), _p(u), _p(w), _p(gap), n, n_threads)
     return (w, gap) if edge_gap else w
 
 
@@ -184,11 +221,16 @@ def infer_fp32(d: DfCfg, p_theta16, p_phi16, queries, wi, guided, uniforms, n_th
     return w
 
 
-def eval_pdf(d: DfCfg, p_theta, p_phi, queries, u, n_threads=0):
-    pt, pp = round_f16(p_theta), round_f16(p_phi)
+def eval_pdf(d: DfCfg, p_theta, p_phi, queries, u, n_threads=0, storage: str = "fp16",
+             weights: str | None = None):
+    """pdfs at given directions; `storage` rounds the activations, `weights`
+    (default: storage) selects the weight format."""
+    wf = storage if weights is None else weights
+    pt, pp = df_weights(d, 0, p_theta, wf), df_weights(d, 1, p_phi, wf)
     q, uu = f32(queries), f32(u)
     out = np.empty((q.shape[0], 2), dtype=np.float32)
-    lib().go_eval_pdf(C.byref(d), _p(pt), _p(pp), _p(q), _p(uu), _p(out), q.shape[0], n_threads)
+    with _storage(storage):
+        lib().go_eval_pdf(C.byref(d), _p(pt), _p(pp), _p(q), _p(uu), _p(out), q.shape[0], n_threads)
     return out
 
 
@@ -272,13 +314,14 @@ def grid_encode(g: Grid, table, pos) -> np.ndarray:
     return out
 
 
-def pdf_tables(d: DfCfg, p_theta, p_phi, queries, u_theta):
-    pt, pp = round_f16(p_theta), round_f16(p_phi)
+def pdf_tables(d: DfCfg, p_theta, p_phi, queries, u_theta, storage: str = "fp16"):
+    pt, pp = df_weights(d, 0, p_theta, storage), df_weights(d, 1, p_phi, storage)
     q, ut = f32(queries), f32(u_theta)
     n = q.shape[0]
     a = np.empty((n, d.n_bins_theta), dtype=np.float32)
     b = np.empty((n, d.n_bins_phi), dtype=np.float32)
-    lib().go_df_pdf_tables(C.byref(d), _p(pt), _p(pp), _p(q), _p(ut), _p(a), _p(b), n)
+    with _storage(storage):
+        lib().go_df_pdf_tables(C.byref(d), _p(pt), _p(pp), _p(q), _p(ut), _p(a), _p(b), n)
     return a, b
 
 

@@ -138,7 +138,7 @@ def check_pdfs(got_pdf, ref_pdf, rtol=PDF_RTOL):
     return worst
 
 
-def run_infer_pair(ctx, pt, pp, n, seed, guided_frac=0.8, one_sided=0.2, philox=None):
+def run_infer_pair(ctx, pt, pp, n, seed, guided_frac=0.8, one_sided=0.2, philox=None, storage="fp16"):
     """Runs gdf_infer and the oracle on identical inputs.
 
     theta is compared with the oracle directly. phi is compared *chained*: the
@@ -162,16 +162,16 @@ def run_infer_pair(ctx, pt, pp, n, seed, guided_frac=0.8, one_sided=0.2, philox=
     ctx.sync()
     got = wi_dev.cpu().numpy()
     d = O.df_cfg_from(cfg)
-    ref, gap = O.infer(d, pt, pp, q, wi, guided, u, edge_gap=True)
+    ref, gap = O.infer(d, pt, pp, q, wi, guided, u, edge_gap=True, storage=storage)
     # chained phi: oracle phi tables conditioned on the kernel's u_theta
-    tt, tp = O.pdf_tables(d, pt, pp, q, got[:, 0])
+    tt, tp = O.pdf_tables(d, pt, pp, q, got[:, 0], storage=storage)
     lin = cfg.pdf_interp == 0
     gsel = guided.astype(bool)
     for i in np.nonzero(gsel)[0]:
         _, ref[i, 1], gap[i, 1] = O.sample_dir(tp[i], lin, float(u[i, 2]), float(u[i, 3]))
     exact = exact_directions(cfg, tt, tp, u)
     # oracle pdfs at the kernel's directions (phi conditioned on the kernel's theta)
-    ref_pdf_at_got = O.eval_pdf(d, pt, pp, q, got[:, :2]) * wi[:, 2:4]
+    ref_pdf_at_got = O.eval_pdf(d, pt, pp, q, got[:, :2], storage=storage) * wi[:, 2:4]
     dump("infer", q=q, wi=wi, guided=guided, u=u, got=got, ref=ref, gap=gap, ref_pdf=ref_pdf_at_got,
          exact=exact)
     return got, ref, gap, guided, ref_pdf_at_got, q, exact
