@@ -33,7 +33,9 @@ SOURCES = [
     ("kernels/nrc.cu", ["-fmad=false"]),
     ("kernels/paths.cu", ["-fmad=false"]),
     ("kernels/tools.cu", ["-fmad=false"]),
+    ("kernels/grouped.cu", ["-fmad=false"]),
     ("host/api.cpp", []),
+    ("host/group.cpp", []),
 ]
 
 

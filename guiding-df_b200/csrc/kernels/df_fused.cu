@@ -370,7 +370,8 @@ cudaError_t launch_t(int mode, const DfKernelParams& p, size_t smem, int num_sms
 
 bool df_shape_supported(const DfShape& s) {
   const bool a = s.levels == 8 && s.features == 2 && s.bins_theta == 32 && s.bins_phi == 32;
-  const bool b = s.levels == 16 && s.features == 2 && s.bins_theta == 64 && s.bins_phi == 64;
+  const bool b = s.levels == 16 && s.features == 2 && (s.bins_theta == 64 || s.bins_theta == 32) &&
+                 s.bins_phi == s.bins_theta;
   const bool c = s.levels == 8 && s.features == 4 && s.bins_theta == 16 && s.bins_phi == 32;
   return a || b || c;
 }
@@ -400,6 +401,7 @@ cudaError_t launch_df_fused(const DfShape& s, int mode, const DfKernelParams& p,
   }
   GDF_DISPATCH(8, 2, 32, 32)
   GDF_DISPATCH(16, 2, 64, 64)
+  GDF_DISPATCH(16, 2, 32, 32)
   GDF_DISPATCH(8, 4, 16, 32)
 #undef GDF_DISPATCH
   return cudaErrorNotSupported;

@@ -550,6 +550,7 @@ cudaError_t launch_df_train_bwd(const DfShape& s, bool phi, const DfBwdParams& p
   }
   GDF_BWD(8, 2, 32, 32)
   GDF_BWD(16, 2, 64, 64)
+  GDF_BWD(16, 2, 32, 32)
   GDF_BWD(8, 4, 16, 32)
 #undef GDF_BWD
   return cudaErrorNotSupported;

@@ -111,6 +111,12 @@ def path_state(fields: dict, cur_depth) -> PathState:
     return st
 
 
+class Job(C.Structure):
+    _fields_ = [("ctx", C.c_void_p), ("queries_dev", C.c_void_p), ("guided_dev", C.c_void_p),
+                ("uniforms_dev", C.c_void_p), ("philox_seed", C.c_uint64), ("philox_offset", C.c_uint64),
+                ("wi_dev", C.c_void_p), ("n", C.c_int64)]
+
+
 class TrainStats(C.Structure):
     _fields_ = [("loss", C.c_double), ("grad_norm", C.c_double), ("n_records", C.c_int64),
                 ("n_dropped", C.c_int64)]
@@ -156,6 +162,11 @@ def lib() -> C.CDLL:
             "gdf_infer_ex": [P, C.POINTER(InferArgs), P],
             "gdf_infer_host": [P, P, P, P, C.c_uint64, C.c_uint64, P, P, C.c_int64, P],
             "gdf_pdf_image": [P, P, C.c_int32, C.c_int32, P, P],
+            "gdf_group_create": [C.c_int32, C.POINTER(C.c_void_p)],
+            "gdf_group_destroy": [P],
+            "gdf_group_infer": [P, P, C.c_int32, P],
+            "gdf_group_tuning": [P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), P],
+            "gdf_group_sync_status": [P, P],
             "gdf_sample_histogram": [P, P, C.c_int64, C.c_uint64, C.c_int32, C.c_int32, P, P, P],
             "gdf_prepare_queries": [C.POINTER(Shading), C.POINTER(Aabb), P, C.c_int64, P],
             "gdf_build_train_records": [P, C.POINTER(PathState), C.POINTER(Aabb), C.POINTER(TrainPixels),
@@ -406,3 +417,48 @@ class Context:
 
     def sync(self, stream=None):
         check(lib().gdf_sync_status(self.h, _stream(stream)))
+
+
+class Group:
+    """A grouped inference engine (gdf_group): one launch pair for many jobs."""
+
+    def __init__(self, max_jobs: int = 64):
+        h = C.c_void_p()
+        check(lib().gdf_group_create(max_jobs, C.byref(h)))
+        self.h = h
+
+    def infer(self, jobs, stream=None):
+        """jobs: list of dicts with ctx, queries, wi and optional guided,
+        uniforms, seed, offset, n."""
+        arr = (Job * len(jobs))()
+        for a, j in zip(arr, jobs):
+            a.ctx = j["ctx"].h
+            a.queries_dev = _ptr(j["queries"])
+            a.guided_dev = _ptr(j.get("guided"))
+            a.uniforms_dev = _ptr(j.get("uniforms"))
+            a.philox_seed = j.get("seed", 0)
+            a.philox_offset = j.get("offset", 0)
+            a.wi_dev = _ptr(j["wi"])
+            a.n = j.get("n", j["queries"].shape[0])
+        check(lib().gdf_group_infer(self.h, arr, len(jobs), _stream(stream)))
+
+    def tuning(self):
+        import numpy as np
+        w, b = C.c_int32(), C.c_int32()
+        ms = np.zeros(4, np.float32)
+        check(lib().gdf_group_tuning(self.h, C.byref(w), C.byref(b), ms.ctypes.data))
+        return w.value, b.value, ms
+
+    def sync(self, stream=None):
+        check(lib().gdf_group_sync_status(self.h, _stream(stream)))
+
+    def close(self):
+        if self.h:
+            lib().gdf_group_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -336,6 +336,50 @@ gdf_status gdf_train_loss_static(gdf_ctx* ctx, const float* in_theta_dev, const 
                                  const float* target_dev, int64_t n, double* loss_out_dev,
                                  int64_t* dropped_out_dev, void* stream);
 
+/* ------------------------------------------------------------ grouped */
+
+/* One job of a grouped inference: a context (its own networks) and one
+ * wavefront of queries, with the arguments of gdf_infer. */
+typedef struct gdf_job {
+  gdf_ctx* ctx;
+  const float* queries_dev;   /* [n x 9]                                  */
+  const uint8_t* guided_dev;  /* [n] or NULL                              */
+  const float* uniforms_dev;  /* [n x 4] or NULL (Philox: seed, offset)    */
+  uint64_t philox_seed;
+  uint64_t philox_offset;
+  float* wi_dev;              /* [n x 4] in/out                           */
+  int64_t n;
+} gdf_job;
+
+typedef struct gdf_group gdf_group;
+
+/* A grouped inference engine for up to max_jobs jobs per call, on the
+ * current device. No counterpart in the reference, which guides one render
+ * job (LearnedDistribution::inferenceStep, learnedDistribution.cpp:167-206);
+ * a grouped call gives every job exactly what gdf_infer gives it. */
+gdf_status gdf_group_create(int32_t max_jobs, gdf_group** out);
+gdf_status gdf_group_destroy(gdf_group* g);
+
+/* Inference of all jobs in one grid-feature launch and one persistent fused
+ * launch, replayed from a CUDA graph built on first use of a configuration
+ * (the job table is read from device memory, so later calls with other jobs
+ * reuse it). Jobs must share the grid configuration, pdf interpolation and
+ * precision; bin counts may differ. The first call for a new job-set
+ * signature (grid shape, job count, log2 of the tile count) times the
+ * candidate launch shapes (2 or 4 warpgroups per CTA x 128- or 256-thread
+ * feature blocks) on scratch copies of the guiding data and keeps the
+ * fastest; that call synchronises `stream`. Jobs must not share wi
+ * buffers. */
+gdf_status gdf_group_infer(gdf_group* g, const gdf_job* jobs, int32_t n_jobs, void* stream);
+
+/* The launch shape chosen for the last call and the candidates' times (ms)
+ * of the last tuning, in the order (4,256), (4,128), (2,256), (2,128). */
+gdf_status gdf_group_tuning(const gdf_group* g, int32_t* warpgroups, int32_t* feature_block,
+                            float* tuned_ms);
+
+/* gdf_sync_status for the group's kernels. */
+gdf_status gdf_group_sync_status(gdf_group* g, void* stream);
+
 /* -------------------------------------------------------------------- NRC */
 
 /* NRC::inferenceStep (nrc.cpp:172-181): in [m x 15] fp32 (GuidedInputNRC,
