@@ -171,7 +171,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="CPU-baseline sample length; 0 skips it (profiling runs)")
     ap.add_argument("--skip-e2e", action="store_true", help="profiling runs: kernel timing only")
-    ap.add_argument("--stages", default="infer,train,records,bf16",
+    ap.add_argument("--stages", default="infer,train,records,bf16,grouped,serve",
                     help="comma list of infer, train, records (profiling runs select one)")
     args = ap.parse_args()
     stages = set(args.stages.split(","))
@@ -306,13 +306,166 @@ def main():
             bf16_times.append(s.elapsed_time(e))
         cb.sync(stream)
         cb.close()
+    grouped = None
+    if "grouped" in stages and args.workload == "full":
+        grouped = time_grouped(W, rank, dev, stream, flush, args)
+    serving = None
+    if "serve" in stages and args.workload == "full":
+        serving = time_serving(W, rank, dev, args)
     clk = clocks.stop()
     ctx.sync(stream)
     _report(args, rank, world, dist, dev, n, cfg, params, times, e2e_times, train_times, rec_times,
-            last, n_rec, rec_bytes, clk, nb, workload_name, threads, q_h, wi_h, guided_h, bf16_times)
+            last, n_rec, rec_bytes, clk, nb, workload_name, threads, q_h, wi_h, guided_h, bf16_times,
+            grouped, serving)
     ctx.close()
     if dist:
         dist.destroy_process_group()
+
+
+def time_grouped(W, rank, dev, stream, flush, args):
+    """8 render jobs with their own networks (4 with 64 bins, 4 with 32), 6
+    bounces with wavefronts round(2,073,600 * 0.7^b): one grouped launch per
+    bounce for all jobs, against the same work as separate gdf_infer calls."""
+    import torch
+    import pygdf
+    n0, jobs_n, bounces = 2073600, 8, 6
+    sizes = [int(round(n0 * 0.7 ** b)) for b in range(bounces)]
+    ctxs, qs, wis, wi0s, gs = [], [], [], [], []
+    for k in range(jobs_n):
+        cfg = pygdf.default_config(pygdf.PRESET_FULL)
+        cfg.n_bins_theta = cfg.n_bins_phi = 64 if k < 4 else 32
+        ctxs.append(pygdf.Context(cfg))
+        qs.append(torch.from_numpy(W.queries(n0, 500 + 7 * rank + k)).to(dev))
+        wi_h, g_h = W.wi_init(n0, 500 + k, guided_frac=0.7, one_sided_frac=0.1)
+        wi0s.append(torch.from_numpy(wi_h).to(dev))
+        gs.append(torch.from_numpy(g_h).to(dev))
+        wis.append([torch.empty((nb, 4), dtype=torch.float32, device=dev) for nb in sizes])
+    group = pygdf.Group(max_jobs=jobs_n)
+
+    def reset():
+        for k in range(jobs_n):
+            for b, nb in enumerate(sizes):
+                wis[k][b].copy_(wi0s[k][:nb])
+
+    def frame(grouped, f):
+        for b, nb in enumerate(sizes):
+            if grouped:
+                group.infer([{"ctx": ctxs[k], "queries": qs[k], "wi": wis[k][b], "guided": gs[k], "n": nb,
+                              "seed": 9, "offset": 100 * f + b} for k in range(jobs_n)], stream=stream)
+            else:
+                for k in range(jobs_n):
+                    ctxs[k].infer(qs[k], wis[k][b], guided=gs[k], seed=9, offset=100 * f + b, n=nb,
+                                  stream=stream)
+
+    out = {}
+    for name, grouped in (("grouped", True), ("separate", False)):
+        for f in range(max(args.warmup, 1)):
+            reset()
+            frame(grouped, f)
+        times = []
+        for f in range(args.steps):
+            reset()
+            flush.zero_()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            frame(grouped, 1000 + f)
+            e.record(stream)
+            e.synchronize()
+            times.append(s.elapsed_time(e))
+        out[name] = statistics.mean(times)
+    group.sync(stream)
+    wgs, fb, tune_ms = group.tuning()
+    total = jobs_n * sum(sizes)
+    res = {"metric": "guided queries/s, 8 jobs x 6 bounces in grouped launches",
+           "value": total / (out["grouped"] * 1e-3), "unit": "queries/s", "ms_per_frame": out["grouped"],
+           "separate_calls_ms_per_frame": out["separate"], "speedup_vs_separate": out["separate"] / out["grouped"],
+           "queries_per_frame": total, "wavefronts": sizes, "bins": "4 jobs x 64, 4 jobs x 32",
+           "launches_per_frame": 2 * bounces, "tuned": {"warpgroups": wgs, "feature_block": fb}}
+    group.close()
+    for c in ctxs:
+        c.close()
+    return res
+
+
+def time_serving(W, rank, dev, args):
+    """64 resident instances (config-1 networks, 32 or 64 bins), requests of
+    log-uniform size in [2^10, 2^21] queries, 1 training to 3 inference, under
+    a 120 GB budget: a saturating burst gives the batched peak; Poisson
+    arrivals at 80 % of it give the latency percentiles."""
+    import time
+    import torch
+    import pygdf
+    n_inst, n_max, train_max = 64, 1 << 21, 1 << 20
+    insts = []
+    for k in range(n_inst):
+        cfg = pygdf.default_config(pygdf.PRESET_FULL)
+        cfg.n_bins_theta = cfg.n_bins_phi = 64 if k % 2 == 0 else 32
+        cfg.max_queries = n_max
+        insts.append(pygdf.Context(cfg))
+    budget = 120 * (1 << 30)
+    srv = pygdf.Server(budget, slots=8, max_batch=32)
+    for c in insts:
+        srv.add_instance(c)
+    q = torch.from_numpy(W.queries(n_max, 800 + rank)).to(dev)
+    g = torch.from_numpy(W.wi_init(n_max, 800, guided_frac=0.7)[1]).to(dev)
+    wi0 = torch.from_numpy(W.wi_init(n_max, 800, guided_frac=0.7)[0]).to(dev)
+    wis = [wi0.clone() for _ in range(n_inst)]
+    tb = {}
+    for bins in (32, 64):
+        tb[bins] = tuple(torch.from_numpy(x).to(dev) for x in W.training_batch(train_max, 801, bins))
+    rng = np.random.default_rng(900 + rank)
+
+    def draw(m):
+        out = []
+        for _ in range(m):
+            n = int(np.exp(rng.uniform(np.log(1 << 10), np.log(n_max))))
+            out.append((int(rng.integers(n_inst)), n, rng.random() < 0.25))
+        return out
+
+    def submit(k, n, train, i):
+        c = insts[k]
+        if train:
+            bins = c.cfg.n_bins_theta
+            n = min(n, train_max)
+            return srv.submit_train(c, tb[bins][0], tb[bins][1], tb[bins][2], n=n)
+        return srv.submit_infer(c, q, wis[k], guided=g, seed=k, offset=i, n=n)
+
+    # warm-up: every graph shape and every instance's first requests
+    for t in [submit(*r, i) for i, r in enumerate(draw(3 * n_inst))]:
+        srv.wait(t)
+    srv.stats(reset=True)
+    # batched peak: a burst of requests submitted at once
+    burst = draw(400)
+    for t in [submit(*r, i) for i, r in enumerate(burst)]:
+        srv.wait(t)
+    peak = srv.stats(reset=True)
+    mean_n = float(np.mean([min(n, train_max) if tr else n for _, n, tr in burst]))
+    rate = 0.8 * peak.queries_per_s / mean_n  # requests per second
+    reqs = draw(1000)
+    tickets = []
+    t0 = time.perf_counter()
+    next_t = t0
+    for i, r in enumerate(reqs):
+        next_t += rng.exponential(1.0 / rate)
+        while time.perf_counter() < next_t:
+            pass
+        tickets.append(submit(*r, 10000 + i))
+    for t in tickets:
+        srv.wait(t)
+    st = srv.stats(reset=True)
+    res = {"metric": "serving: 64 instances, Poisson arrivals, continuous batching",
+           "p50_ms": st.p50_ms, "p99_ms": st.p99_ms, "max_ms": st.max_ms,
+           "p99_over_p50": st.p99_ms / st.p50_ms if st.p50_ms > 0 else None,
+           "throughput": st.queries_per_s, "unit": "queries/s",
+           "batched_peak": peak.queries_per_s, "frac_of_peak": st.queries_per_s / peak.queries_per_s,
+           "offered_load": "80 % of the batched peak", "requests": st.requests,
+           "resident_gb": peak.resident_bytes / 2 ** 30, "budget_gb": budget / 2 ** 30,
+           "sizes": "log-uniform 2^10..2^21 queries (training batches capped at 2^20)",
+           "mix": "1 training : 3 inference"}
+    srv.close()
+    for c in insts:
+        c.close()
+    return res
 
 
 def time_train(ctx, cfg, W, nb, rank, dev, stream, flush, args):
@@ -368,7 +521,8 @@ def time_records(ctx, W, n, rank, dev, stream, flush, args):
 
 
 def _report(args, rank, world, dist, dev, n, cfg, params, times, e2e_times, train_times, rec_times,
-            last, n_rec, rec_bytes, clk, nb, workload_name, threads, q_h, wi_h, guided_h, bf16_times):
+            last, n_rec, rec_bytes, clk, nb, workload_name, threads, q_h, wi_h, guided_h, bf16_times,
+            grouped, serving):
     import torch
     ms = statistics.mean(times)
     ms_e2e = statistics.mean(e2e_times) if e2e_times else float("nan")
@@ -429,6 +583,10 @@ def _report(args, rank, world, dist, dev, n, cfg, params, times, e2e_times, trai
             line["bf16"] = {"metric": "guided queries/s, bf16 MLP operands (fp32 accumulation)",
                             "value": n * world / (mb * 1e-3), "unit": "queries/s", "ms_per_step": mb,
                             "vs_fp16": ms / mb}
+        if grouped:
+            line["grouped"] = grouped
+        if serving:
+            line["serving"] = serving
         line.update({
             "clocks": clk,
             "gpu_launches": 2 * args.steps,  # grid features + fused kernel per step

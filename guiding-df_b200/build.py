@@ -36,6 +36,7 @@ SOURCES = [
     ("kernels/grouped.cu", ["-fmad=false"]),
     ("host/api.cpp", []),
     ("host/group.cpp", []),
+    ("host/serve.cpp", []),
 ]
 
 

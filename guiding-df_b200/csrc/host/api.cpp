@@ -607,6 +607,27 @@ gdf_status gdf_reset_training(gdf_ctx* ctx, uint32_t seed) {
   return refresh_grid_il(ctx->c);
 }
 
+gdf_status gdf_ctx_bytes(const gdf_ctx* ctx, int64_t* bytes) {
+  if (!ctx || !bytes) return fail(GDF_ERR_INVALID_ARG, "null argument");
+  const Context& c = ctx->c;
+  int64_t b = 0;
+  for (const Net& n : c.net) {
+    if (!n.present) continue;
+    // master, m, v, step, grad (4 B) + w16, ema16 (2 B) + two MLP blobs
+    b += n.n_params * (4 * 5 + 2 * 2) + n.n_mlp * 2 * 2;
+  }
+  const int64_t lf = static_cast<int64_t>(c.cfg.grid_theta.n_levels) * c.cfg.grid_theta.n_features_per_level;
+  b += c.net[0].n_grid * 2 * 2;                               // interleaved inference grid
+  b += c.feat_tiles * 128 * lf * 2 * 2;                       // inference feature tiles
+  b += c.ws.capacity * 16 + 3 * static_cast<int64_t>(c.num_sms) * (c.net[0].n_mlp + c.net[1].n_mlp) +
+       3 * gdf::kAdamBlocks * 8 + 64;                         // training workspace
+  b += (c.lr_table_n[0] + c.lr_table_n[1]) * 4;
+  b += c.host_cap * (9 * 4 + 1 + 4 * 4 + 4 * 4) + c.tool_cap * (9 + 2 + 4) * 4;
+  b += c.pw.pixels * 2 + c.pw.df_cap * 28 * 4 + c.pw.nrc_cap * (15 + 1 + 1 + 3 + 15 + 3) * 4;
+  *bytes = b;
+  return GDF_OK;
+}
+
 gdf_status gdf_n_params(const gdf_ctx* ctx, int32_t net, int64_t* n_params) {
   Net* n = net_of(const_cast<Context*>(ctx ? &ctx->c : nullptr), net);
   if (!n || !n_params) return fail(GDF_ERR_INVALID_ARG, "bad ctx / net id / output pointer");

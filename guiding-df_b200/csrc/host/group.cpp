@@ -37,7 +37,11 @@ struct Plan {
   int wgs = 0, fblock = 0;
   uint32_t bt = 0, bp = 0;
   gdf::GridLevels gl{};
+  cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  // the feature launch, whose grid follows the call's row count
+  cudaGraphNode_t feat_node = nullptr;
+  cudaKernelNodeParams feat_params{};
 };
 
 }  // namespace
@@ -64,6 +68,7 @@ struct gdf_group {
   int64_t tune_cap = 0;
   int last_wgs = 0, last_fblock = 0;
   float last_tune_ms[4] = {0.f, 0.f, 0.f, 0.f};
+  int pinned_wgs = 0, pinned_fblock = 0;  // set: skip tuning
 };
 
 namespace {
@@ -73,8 +78,10 @@ size_t stage_bytes(int32_t max_jobs) {
 }
 
 void drop_plans(gdf_group* g) {
-  for (Plan& p : g->plans)
+  for (Plan& p : g->plans) {
     if (p.exec) cudaGraphExecDestroy(p.exec);
+    if (p.graph) cudaGraphDestroy(p.graph);
+  }
   g->plans.clear();
 }
 
@@ -184,14 +191,20 @@ gdf_status upload_table(gdf_group* g, const gdf_job* jobs, int32_t n, int wgs, f
   return GDF_OK;
 }
 
-gdf_status get_plan(gdf_group* g, const JobSet& js, int wgs, int fblock, cudaGraphExec_t* out) {
-  for (const Plan& p : g->plans)
+int64_t feature_blocks(const JobSet& js, int fblock) {
+  return js.total_tiles * 128 * (js.levels * js.features / 8) / fblock;
+}
+
+gdf_status get_plan(gdf_group* g, const JobSet& js, int wgs, int fblock, size_t* out) {
+  for (size_t i = 0; i < g->plans.size(); ++i) {
+    const Plan& p = g->plans[i];
     if (p.levels == js.levels && p.features == js.features && p.linear == js.linear && p.bf16 == js.bf16 &&
         p.wgs == wgs && p.fblock == fblock && p.bt == js.bt && p.bp == js.bp &&
         std::memcmp(&p.gl, &js.gl, sizeof(gdf::GridLevels)) == 0) {
-      *out = p.exec;
+      *out = i;
       return GDF_OK;
     }
+  }
   const gdf::GroupShape shape{js.levels, js.features, js.linear, js.bf16};
   gdf::GroupParams prm;
   std::memset(&prm, 0, sizeof(prm));
@@ -207,17 +220,24 @@ gdf_status get_plan(gdf_group* g, const JobSet& js, int wgs, int fblock, cudaGra
   if (smem > 227u * 1024u) return gfail(GDF_ERR_UNSUPPORTED, "grouped kernel shared memory exceeds 227 KB");
   cudaGraph_t graph = nullptr;
   GDF_GCUDA(cudaStreamBeginCapture(g->cap_stream, cudaStreamCaptureModeRelaxed));
-  cudaError_t e1 = gdf::launch_group_features(shape, prm, g->num_sms * (1024 / fblock), fblock, g->cap_stream);
+  cudaError_t e1 = gdf::launch_group_features(shape, prm, static_cast<int>(feature_blocks(js, fblock)), fblock,
+                                              g->cap_stream);
   cudaError_t e2 = gdf::launch_group_fused(shape, wgs, prm, g->num_sms, g->cap_stream);
   cudaError_t e3 = cudaStreamEndCapture(g->cap_stream, &graph);
   if (e1 != cudaSuccess) return gcuda(e1, "grouped features (capture)");
   if (e2 != cudaSuccess) return gcuda(e2, "grouped fused (capture)");
   if (e3 != cudaSuccess) return gcuda(e3, "end capture");
-  cudaGraphExec_t exec = nullptr;
-  cudaError_t e4 = cudaGraphInstantiate(&exec, graph, 0);
-  cudaGraphDestroy(graph);
-  if (e4 != cudaSuccess) return gcuda(e4, "graph instantiate");
   Plan p;
+  p.graph = graph;
+  size_t n_roots = 1;
+  cudaError_t e4 = cudaGraphGetRootNodes(graph, &p.feat_node, &n_roots);
+  if (e4 == cudaSuccess && n_roots != 1) e4 = cudaErrorInvalidValue;
+  if (e4 == cudaSuccess) e4 = cudaGraphKernelNodeGetParams(p.feat_node, &p.feat_params);
+  if (e4 == cudaSuccess) e4 = cudaGraphInstantiate(&p.exec, graph, 0);
+  if (e4 != cudaSuccess) {
+    cudaGraphDestroy(graph);
+    return gcuda(e4, "graph instantiate");
+  }
   p.levels = js.levels;
   p.features = js.features;
   p.linear = js.linear;
@@ -227,9 +247,18 @@ gdf_status get_plan(gdf_group* g, const JobSet& js, int wgs, int fblock, cudaGra
   p.bt = js.bt;
   p.bp = js.bp;
   p.gl = js.gl;
-  p.exec = exec;
   g->plans.push_back(p);
-  *out = exec;
+  *out = g->plans.size() - 1;
+  return GDF_OK;
+}
+
+// Sizes the feature launch to the job set and replays the plan's graph
+// (parameter updates apply to launches queued after them).
+gdf_status launch_plan(gdf_group* g, size_t plan, const JobSet& js, cudaStream_t st) {
+  Plan& p = g->plans[plan];
+  p.feat_params.gridDim = dim3(static_cast<unsigned>(feature_blocks(js, p.fblock)));
+  GDF_GCUDA(cudaGraphExecKernelNodeSetParams(p.exec, p.feat_node, &p.feat_params));
+  GDF_GCUDA(cudaGraphLaunch(p.exec, st));
   return GDF_OK;
 }
 
@@ -264,12 +293,12 @@ gdf_status autotune(gdf_group* g, const gdf_job* jobs, int32_t n, const JobSet& 
                                   cudaMemcpyDeviceToDevice, st));
       off += (jobs[i].n + 3) / 4 * 4;
     }
-    cudaGraphExec_t exec = nullptr;
+    size_t plan = 0;
     if ((s = upload_table(g, jobs, n, cand[k].first, g->tune_wi, st))) break;
-    if ((s = get_plan(g, js, cand[k].first, cand[k].second, &exec))) break;
-    GDF_GCUDA(cudaGraphLaunch(exec, st));  // warm-up
+    if ((s = get_plan(g, js, cand[k].first, cand[k].second, &plan))) break;
+    if ((s = launch_plan(g, plan, js, st))) break;  // warm-up
     GDF_GCUDA(cudaEventRecord(a, st));
-    GDF_GCUDA(cudaGraphLaunch(exec, st));
+    if ((s = launch_plan(g, plan, js, st))) break;
     GDF_GCUDA(cudaEventRecord(b, st));
     GDF_GCUDA(cudaEventSynchronize(b));
     float ms = 0.f;
@@ -352,7 +381,9 @@ gdf_status gdf_group_infer(gdf_group* g, const gdf_job* jobs, int32_t n_jobs, vo
                                    static_cast<int>(std::ceil(std::log2(static_cast<double>(js.total_tiles)))));
   auto it = g->tuned.find(key);
   std::pair<int, int> cfg;
-  if (it == g->tuned.end()) {
+  if (g->pinned_wgs) {
+    cfg = {g->pinned_wgs, g->pinned_fblock};
+  } else if (it == g->tuned.end()) {
     if ((s = autotune(g, jobs, n_jobs, js, st, &cfg))) return s;
     g->tuned[key] = cfg;
   } else {
@@ -360,10 +391,22 @@ gdf_status gdf_group_infer(gdf_group* g, const gdf_job* jobs, int32_t n_jobs, vo
   }
   g->last_wgs = cfg.first;
   g->last_fblock = cfg.second;
-  cudaGraphExec_t exec = nullptr;
+  size_t plan = 0;
   if ((s = upload_table(g, jobs, n_jobs, cfg.first, nullptr, st))) return s;
-  if ((s = get_plan(g, js, cfg.first, cfg.second, &exec))) return s;
-  GDF_GCUDA(cudaGraphLaunch(exec, st));
+  if ((s = get_plan(g, js, cfg.first, cfg.second, &plan))) return s;
+  return launch_plan(g, plan, js, st);
+}
+
+gdf_status gdf_group_set_shape(gdf_group* g, int32_t warpgroups, int32_t feature_block) {
+  if (!g) return gfail(GDF_ERR_INVALID_ARG, "null group");
+  if (warpgroups == 0) {
+    g->pinned_wgs = g->pinned_fblock = 0;
+    return GDF_OK;
+  }
+  if ((warpgroups != 2 && warpgroups != 4) || (feature_block != 128 && feature_block != 256))
+    return gfail(GDF_ERR_INVALID_ARG, "launch shape must be 2 or 4 warpgroups x 128 or 256 threads");
+  g->pinned_wgs = warpgroups;
+  g->pinned_fblock = feature_block;
   return GDF_OK;
 }
 

@@ -55,7 +55,9 @@ struct GroupShape {
 };
 
 bool group_shape_supported(const GroupShape& s);
-// Grid features of every job's rows (grid-stride over the header's tiles).
+// Grid features of every job's rows: one thread per 16-byte chunk (8 / F
+// levels) of a row, so blocks * block_threads must equal the header's
+// total_tiles * 128 * (levels * features / 8).
 cudaError_t launch_group_features(const GroupShape& s, const GroupParams& p, int blocks, int block_threads,
                                   cudaStream_t st);
 // The grouped fused kernel: wgs warpgroups per CTA (2 or 4), one CTA per SM.

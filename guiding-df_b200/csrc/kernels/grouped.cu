@@ -61,42 +61,46 @@ __device__ __forceinline__ float condition_bins(int nb, float u) {
   return theta_condition<64, LINEAR>(u);
 }
 
+// One 16-byte chunk of one row per thread, as grid_features_kernel; the
+// host sizes the grid to the call's rows (the graph's launch node is
+// updated per call), so every thread has exactly one item.
 template <int L, int F, bool BF16>
 __global__ void __launch_bounds__(256, 4) group_features_kernel(const __grid_constant__ GroupParams g) {
   constexpr int LPC = 8 / F;
   constexpr int NCH = L / LPC;
   constexpr uint32_t LF = L * F;
-  const int n_jobs = g.hdr->n_jobs;
   const int64_t rows = g.hdr->total_tiles * 128;
-  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
-  for (int64_t gid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; gid < rows * NCH;
-       gid += stride) {
-    const int64_t row = gid % rows;
-    const int chunk = static_cast<int>(gid / rows);
-    const int64_t t = row >> 7;
-    const GroupJobDev& J = g.jobs[find_job(g.jobs, n_jobs, t, false)];
-    const int64_t lr = row - J.tile_begin * 128;
-    float pos[3] = {0.5f, 0.5f, 0.5f};
-    if (lr < J.n) {
+  const int64_t gid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (gid >= rows * NCH) return;  // whole warps: rows * NCH is a multiple of 256
+  const int64_t row = gid % rows;
+  const int chunk = static_cast<int>(gid / rows);
+  const int64_t t = row >> 7;
+  // a warp's 32 rows lie in one 128-row tile, hence in one job
+  int jb = 0;
+  if ((threadIdx.x & 31) == 0) jb = find_job(g.jobs, g.hdr->n_jobs, t, false);
+  jb = __shfl_sync(0xffffffffu, jb, 0);
+  const GroupJobDev& J = g.jobs[jb];
+  const int64_t lr = row - J.tile_begin * 128;
+  float pos[3] = {0.5f, 0.5f, 0.5f};
+  if (lr < J.n) {
 #pragma unroll
-      for (int k = 0; k < 3; ++k) pos[k] = __ldg(J.queries + lr * 9 + k);
-    }
-    uint32_t pt[4], pp[4];
-#pragma unroll
-    for (int j = 0; j < LPC; ++j) {
-      float ft[F], fp[F];
-      tile::grid_level_pair<F>(g.gl, chunk * LPC + j, g.gl.interp, J.grid_il, pos[0], pos[1], pos[2], ft, fp);
-#pragma unroll
-      for (int k = 0; k < F; k += 2) {
-        pt[(j * F + k) / 2] = tile::pack2(ft[k], ft[k + 1], BF16);
-        pp[(j * F + k) / 2] = tile::pack2(fp[k], fp[k + 1], BF16);
-      }
-    }
-    const int64_t off = t * (128 * LF) +
-                        canon_offset(static_cast<uint32_t>(row & 127), static_cast<uint32_t>(chunk * 8), LF);
-    *reinterpret_cast<uint4*>(g.feat_theta + off) = make_uint4(pt[0], pt[1], pt[2], pt[3]);
-    *reinterpret_cast<uint4*>(g.feat_phi + off) = make_uint4(pp[0], pp[1], pp[2], pp[3]);
+    for (int k = 0; k < 3; ++k) pos[k] = __ldg(J.queries + lr * 9 + k);
   }
+  uint32_t pt[4], pp[4];
+#pragma unroll
+  for (int j = 0; j < LPC; ++j) {
+    float ft[F], fp[F];
+    tile::grid_level_pair<F>(g.gl, chunk * LPC + j, g.gl.interp, J.grid_il, pos[0], pos[1], pos[2], ft, fp);
+#pragma unroll
+    for (int k = 0; k < F; k += 2) {
+      pt[(j * F + k) / 2] = tile::pack2(ft[k], ft[k + 1], BF16);
+      pp[(j * F + k) / 2] = tile::pack2(fp[k], fp[k + 1], BF16);
+    }
+  }
+  const int64_t off = t * (128 * LF) +
+                      canon_offset(static_cast<uint32_t>(row & 127), static_cast<uint32_t>(chunk * 8), LF);
+  *reinterpret_cast<uint4*>(g.feat_theta + off) = make_uint4(pt[0], pt[1], pt[2], pt[3]);
+  *reinterpret_cast<uint4*>(g.feat_phi + off) = make_uint4(pp[0], pp[1], pp[2], pp[3]);
 }
 
 template <int L, int F, bool LINEAR, int WGS, bool BF16>

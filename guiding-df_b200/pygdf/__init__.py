@@ -117,6 +117,24 @@ class Job(C.Structure):
                 ("wi_dev", C.c_void_p), ("n", C.c_int64)]
 
 
+class Request(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("instance", C.c_void_p), ("n", C.c_int64),
+                ("queries_dev", C.c_void_p), ("guided_dev", C.c_void_p), ("uniforms_dev", C.c_void_p),
+                ("philox_seed", C.c_uint64), ("philox_offset", C.c_uint64), ("wi_dev", C.c_void_p),
+                ("in_theta_dev", C.c_void_p), ("in_phi_dev", C.c_void_p), ("target_dev", C.c_void_p)]
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [("device", C.c_int32), ("slots", C.c_int32), ("max_batch", C.c_int32),
+                ("hbm_budget_bytes", C.c_int64)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("requests", C.c_int64), ("queries", C.c_int64), ("pending", C.c_int64),
+                ("resident_bytes", C.c_int64), ("p50_ms", C.c_double), ("p99_ms", C.c_double),
+                ("max_ms", C.c_double), ("queries_per_s", C.c_double)]
+
+
 class TrainStats(C.Structure):
     _fields_ = [("loss", C.c_double), ("grad_norm", C.c_double), ("n_records", C.c_int64),
                 ("n_dropped", C.c_int64)]
@@ -167,6 +185,14 @@ def lib() -> C.CDLL:
             "gdf_group_infer": [P, P, C.c_int32, P],
             "gdf_group_tuning": [P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), P],
             "gdf_group_sync_status": [P, P],
+            "gdf_group_set_shape": [P, C.c_int32, C.c_int32],
+            "gdf_ctx_bytes": [P, C.POINTER(C.c_int64)],
+            "gdf_server_create": [C.POINTER(ServerConfig), C.POINTER(C.c_void_p)],
+            "gdf_server_destroy": [P],
+            "gdf_server_add_instance": [P, P],
+            "gdf_server_submit": [P, C.POINTER(Request), C.POINTER(C.c_uint64)],
+            "gdf_server_wait": [P, C.c_uint64, C.POINTER(TrainStats), C.POINTER(C.c_double)],
+            "gdf_server_get_stats": [P, C.POINTER(ServerStats), C.c_int32],
             "gdf_sample_histogram": [P, P, C.c_int64, C.c_uint64, C.c_int32, C.c_int32, P, P, P],
             "gdf_prepare_queries": [C.POINTER(Shading), C.POINTER(Aabb), P, C.c_int64, P],
             "gdf_build_train_records": [P, C.POINTER(PathState), C.POINTER(Aabb), C.POINTER(TrainPixels),
@@ -455,6 +481,70 @@ class Group:
     def close(self):
         if self.h:
             lib().gdf_group_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+REQ_INFER, REQ_TRAIN = 0, 1
+
+
+def ctx_bytes(ctx) -> int:
+    b = C.c_int64()
+    check(lib().gdf_ctx_bytes(ctx.h, C.byref(b)))
+    return b.value
+
+
+class Server:
+    """gdf_server: resident instances, continuous admission and batching."""
+
+    def __init__(self, budget_bytes: int, slots: int = 4, max_batch: int = 16, device: int = 0):
+        cfg = ServerConfig(device, slots, max_batch, budget_bytes)
+        h = C.c_void_p()
+        check(lib().gdf_server_create(C.byref(cfg), C.byref(h)))
+        self.h = h
+        self._keep = {}
+
+    def add_instance(self, ctx):
+        check(lib().gdf_server_add_instance(self.h, ctx.h))
+
+    def submit_infer(self, ctx, queries, wi, guided=None, uniforms=None, seed=0, offset=0, n=None) -> int:
+        r = Request(REQ_INFER, ctx.h, queries.shape[0] if n is None else n, _ptr(queries), _ptr(guided),
+                    _ptr(uniforms), seed, offset, _ptr(wi), None, None, None)
+        return self._submit(r, (queries, wi, guided, uniforms))
+
+    def submit_train(self, ctx, in_theta, in_phi, target, n=None) -> int:
+        r = Request(REQ_TRAIN, ctx.h, in_theta.shape[0] if n is None else n, None, None, None, 0, 0, None,
+                    _ptr(in_theta), _ptr(in_phi), _ptr(target))
+        return self._submit(r, (in_theta, in_phi, target))
+
+    def _submit(self, r, keep) -> int:
+        t = C.c_uint64()
+        check(lib().gdf_server_submit(self.h, C.byref(r), C.byref(t)))
+        self._keep[t.value] = keep
+        return t.value
+
+    def wait(self, ticket: int):
+        st = TrainStats()
+        lat = C.c_double()
+        try:
+            check(lib().gdf_server_wait(self.h, ticket, C.byref(st), C.byref(lat)))
+        finally:
+            self._keep.pop(ticket, None)
+        return st, lat.value
+
+    def stats(self, reset: bool = False) -> ServerStats:
+        st = ServerStats()
+        check(lib().gdf_server_get_stats(self.h, C.byref(st), int(reset)))
+        return st
+
+    def close(self):
+        if self.h:
+            lib().gdf_server_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -377,8 +377,73 @@ gdf_status gdf_group_infer(gdf_group* g, const gdf_job* jobs, int32_t n_jobs, vo
 gdf_status gdf_group_tuning(const gdf_group* g, int32_t* warpgroups, int32_t* feature_block,
                             float* tuned_ms);
 
+/* Fixes the launch shape (warpgroups 2 or 4, feature block 128 or 256)
+ * and skips tuning; warpgroups = 0 returns to tuning. */
+gdf_status gdf_group_set_shape(gdf_group* g, int32_t warpgroups, int32_t feature_block);
+
 /* gdf_sync_status for the group's kernels. */
 gdf_status gdf_group_sync_status(gdf_group* g, void* stream);
+
+/* ------------------------------------------------------------- serving */
+
+/* Device memory held by a context: networks, optimizer state, workspaces. */
+gdf_status gdf_ctx_bytes(const gdf_ctx* ctx, int64_t* bytes);
+
+typedef enum gdf_request_kind { GDF_REQ_INFER = 0, GDF_REQ_TRAIN = 1 } gdf_request_kind;
+
+/* One request to a server: gdf_infer (queries_dev, guided_dev,
+ * uniforms_dev, philox_*, wi_dev) or gdf_train_step (in_theta_dev,
+ * in_phi_dev, target_dev) on one registered instance. The buffers stay
+ * owned by the caller and must stay valid until gdf_server_wait returns. */
+typedef struct gdf_request {
+  int32_t kind;               /* gdf_request_kind */
+  gdf_ctx* instance;
+  int64_t n;
+  const float* queries_dev;
+  const uint8_t* guided_dev;
+  const float* uniforms_dev;
+  uint64_t philox_seed;
+  uint64_t philox_offset;
+  float* wi_dev;
+  const float* in_theta_dev;
+  const float* in_phi_dev;
+  const float* target_dev;
+} gdf_request;
+
+typedef struct gdf_server_config {
+  int32_t device;
+  int32_t slots;              /* concurrent device streams (1..64)            */
+  int32_t max_batch;          /* inference requests per grouped launch        */
+  int64_t hbm_budget_bytes;   /* resident instances + in-flight requests      */
+} gdf_server_config;
+
+typedef struct gdf_server_stats {
+  int64_t requests, queries, pending, resident_bytes;
+  double p50_ms, p99_ms, max_ms;   /* submit -> completion latency            */
+  double queries_per_s;            /* completed queries / first submit..last completion */
+} gdf_server_stats;
+
+typedef struct gdf_server gdf_server;
+
+/* A request server over resident instances (no counterpart in the
+ * reference, which guides one job per process). A scheduler thread admits
+ * requests in arrival order as stream slots and budget allow -- requests
+ * of one instance run in submission order, one at a time -- batches all
+ * inference requests admitted together into one grouped launch
+ * (gdf_group_infer) and runs training requests on streams of their own, so
+ * their work overlaps on the device. Instances must share the grid
+ * configuration, pdf interpolation and precision, and must not be used
+ * directly while registered. */
+gdf_status gdf_server_create(const gdf_server_config* cfg, gdf_server** out);
+gdf_status gdf_server_destroy(gdf_server* s);
+/* Registers a context; its gdf_ctx_bytes count against the budget. */
+gdf_status gdf_server_add_instance(gdf_server* s, gdf_ctx* ctx);
+gdf_status gdf_server_submit(gdf_server* s, const gdf_request* r, uint64_t* ticket);
+/* Blocks until the request completed; training requests fill stats. */
+gdf_status gdf_server_wait(gdf_server* s, uint64_t ticket, gdf_train_stats* stats, double* latency_ms);
+/* Latency percentiles and throughput of the requests completed since the
+ * last reset. */
+gdf_status gdf_server_get_stats(gdf_server* s, gdf_server_stats* out, int32_t reset);
 
 /* -------------------------------------------------------------------- NRC */
 

@@ -1,0 +1,124 @@
+"""The request server (gdf_server_*): each result is the same alone and in
+the mix. Two instances serve inference requests and two train, all
+submitted interleaved so that grouped inference launches and training
+steps overlap on the device; then the same per-instance sequences run
+directly on fresh copies of the instances. Inference results must be
+identical bit for bit; a first training step's loss is identical, later ones
+within 2e-5 relative (they see weights updated by the earlier steps). Grid
+gradients are summed with float atomics in no fixed order, and Adam
+normalises each step, so a near-zero gradient whose sum changes sign moves
+its weight by up to the learning rate: at least 99.9 % of the final weights
+must agree within 1e-5 relative and every weight within 2 x lr per step
+(the same holds between two runs alone)."""
+import numpy as np
+import pytest
+import torch
+
+import pygdf
+from gdf_testutil import dev, make_ctx
+from pygdf import workload as W
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [3000, 17000, 512, 9000, 25000, 1000]
+
+
+def _instances():
+    return [make_ctx(pygdf.PRESET_SMALL, seed=200 + k)[0] for k in range(4)]
+
+
+def _infer_requests():
+    reqs = []
+    for k in range(2):
+        for i, n in enumerate(SIZES):
+            q = W.queries(n, 10 * k + i)
+            wi, guided = W.wi_init(n, 10 * k + i, guided_frac=0.8, one_sided_frac=0.2)
+            reqs.append(dict(inst=k, q=q, wi=wi, guided=guided, seed=k + 1, offset=i))
+    return reqs
+
+
+def _train_batches(cfg):
+    return [[W.training_batch(16384, 50 + 7 * k + s, cfg.n_bins_theta) for s in range(3)] for k in range(2)]
+
+
+def test_results_same_alone_and_in_the_mix():
+    insts = _instances()
+    cfg = insts[0].cfg
+    budget = sum(pygdf.ctx_bytes(c) for c in insts) + (1 << 30)
+    srv = pygdf.Server(budget, slots=4, max_batch=8)
+    for c in insts:
+        srv.add_instance(c)
+    ireqs = _infer_requests()
+    tb = _train_batches(cfg)
+    # interleave: inference of instances 0/1 and training of instances 2/3
+    order = []
+    for i in range(len(SIZES)):
+        order += [("i", i), ("i", len(SIZES) + i)]
+        if i < 3:
+            order += [("t", (0, i)), ("t", (1, i))]
+    tickets, outs, keep = [], {}, []
+    for kind, key in order:
+        if kind == "i":
+            r = ireqs[key]
+            wi_d = dev(r["wi"])
+            q_d, g_d = dev(r["q"]), dev(r["guided"])
+            keep += [q_d, g_d]
+            outs[("i", key)] = wi_d
+            tickets.append((("i", key), srv.submit_infer(insts[r["inst"]], q_d, wi_d, guided=g_d,
+                                                         seed=r["seed"], offset=r["offset"])))
+        else:
+            k, s = key
+            a, b, t = (dev(x) for x in tb[k][s])
+            keep += [a, b, t]
+            tickets.append((("t", key), srv.submit_train(insts[2 + k], a, b, t)))
+    losses = {}
+    for key, t in tickets:
+        st, lat = srv.wait(t)
+        assert lat > 0
+        if key[0] == "t":
+            losses[key[1]] = st.loss
+    stats = srv.stats()
+    assert stats.requests == len(tickets) and stats.p50_ms <= stats.p99_ms
+    srv.close()
+    mix_params = [insts[2 + k].get_params(n) for k in range(2) for n in (0, 1)]
+
+    # alone: fresh instances with the same initial weights, direct calls
+    alone = _instances()
+    for key, _ in tickets:
+        if key[0] == "i":
+            r = ireqs[key[1]]
+            wi_d = dev(r["wi"])
+            alone[r["inst"]].infer(dev(r["q"]), wi_d, guided=dev(r["guided"]), seed=r["seed"], offset=r["offset"])
+            torch.cuda.synchronize()
+            np.testing.assert_array_equal(outs[key].cpu().numpy(), wi_d.cpu().numpy())
+        else:
+            k, s = key[1]
+            a, b, t = (dev(x) for x in tb[k][s])
+            st = alone[2 + k].train_step(a, b, t)
+            assert abs(st.loss - losses[(k, s)]) <= 2e-5 * abs(st.loss), (st.loss, losses[(k, s)])
+    alone_params = [alone[2 + k].get_params(n) for k in range(2) for n in (0, 1)]
+    lr = cfg.adam_df.learning_rate
+    for x, y in zip(mix_params, alone_params):
+        close = np.isclose(x, y, rtol=1e-5, atol=1e-7)
+        assert close.mean() >= 0.999, close.mean()
+        # the rest: near-zero gradients whose float-atomic sum changed sign,
+        # each Adam step moving the weight by at most about lr
+        assert np.abs(x - y).max() <= 2 * 3 * lr, np.abs(x - y).max()
+    for c in insts + alone:
+        c.close()
+
+
+def test_budget_is_enforced():
+    insts = _instances()[:2]
+    one = pygdf.ctx_bytes(insts[0])
+    srv = pygdf.Server(one + (1 << 20), slots=2, max_batch=4)
+    srv.add_instance(insts[0])
+    with pytest.raises(pygdf.GdfError):
+        srv.add_instance(insts[1])
+    q = dev(W.queries(1 << 16, 3))
+    wi = dev(W.wi_init(1 << 16, 3)[0])
+    with pytest.raises(pygdf.GdfError):          # 64K queries need 8 MiB of feature tiles
+        srv.submit_infer(insts[0], q, wi)
+    srv.close()
+    for c in insts:
+        c.close()
