@@ -387,6 +387,9 @@ def time_grouped(W, rank, dev, stream, flush, args):
     return res
 
 
+SERVE_SLOTS, SERVE_TRAIN_SLOTS = 8, 2
+
+
 def time_serving(W, rank, dev, args):
     """64 resident instances (config-1 networks, 32 or 64 bins), requests of
     log-uniform size in [2^10, 2^21] queries, 1 training to 3 inference, under
@@ -403,7 +406,7 @@ def time_serving(W, rank, dev, args):
         cfg.max_queries = n_max
         insts.append(pygdf.Context(cfg))
     budget = 120 * (1 << 30)
-    srv = pygdf.Server(budget, slots=8, max_batch=32)
+    srv = pygdf.Server(budget, slots=SERVE_SLOTS, max_batch=32, max_train_slots=SERVE_TRAIN_SLOTS)
     for c in insts:
         srv.add_instance(c)
     q = torch.from_numpy(W.queries(n_max, 800 + rank)).to(dev)
@@ -441,6 +444,20 @@ def time_serving(W, rank, dev, args):
     peak = srv.stats(reset=True)
     mean_n = float(np.mean([min(n, train_max) if tr else n for _, n, tr in burst]))
     rate = 0.8 * peak.queries_per_s / mean_n  # requests per second
+    # isolated service time by kind, bin count and size (one request at a time)
+    inf_sizes = [1 << e for e in range(10, 22)]
+    trn_sizes = [1 << e for e in range(10, 21)]
+    iso = {}
+    for train, sizes in ((False, inf_sizes), (True, trn_sizes)):
+        for k in (0, 1):  # even instances have 64 bins, odd ones 32
+            iso[(train, k)] = [min(srv.wait(submit(k, n, train, 50000 + r))[1] for r in range(3)) for n in sizes]
+
+    def iso_ms(k, n, train):
+        sizes = trn_sizes if train else inf_sizes
+        n = min(n, train_max) if train else n
+        return float(np.exp(np.interp(np.log(n), np.log(sizes), np.log(iso[(train, k % 2)]))))
+
+    srv.stats(reset=True)
     reqs = draw(1000)
     tickets = []
     t0 = time.perf_counter()
@@ -450,12 +467,20 @@ def time_serving(W, rank, dev, args):
         while time.perf_counter() < next_t:
             pass
         tickets.append(submit(*r, 10000 + i))
-    for t in tickets:
-        srv.wait(t)
+    lat = np.array([srv.wait(t)[1] for t in tickets])
     st = srv.stats(reset=True)
+    slow = lat / np.array([iso_ms(k, n, tr) for k, n, tr in reqs])
+    is_tr = np.array([tr for _, _, tr in reqs])
+
+    def pct(x):
+        return {"p50": float(np.percentile(x, 50)), "p99": float(np.percentile(x, 99))}
+
     res = {"metric": "serving: 64 instances, Poisson arrivals, continuous batching",
            "p50_ms": st.p50_ms, "p99_ms": st.p99_ms, "max_ms": st.max_ms,
            "p99_over_p50": st.p99_ms / st.p50_ms if st.p50_ms > 0 else None,
+           "slowdown": {**pct(slow), "p99_over_p50": float(np.percentile(slow, 99) / np.percentile(slow, 50)),
+                        "definition": "latency / the same request's isolated latency (same kind, bins, size)"},
+           "inference_ms": pct(lat[~is_tr]), "training_ms": pct(lat[is_tr]),
            "throughput": st.queries_per_s, "unit": "queries/s",
            "batched_peak": peak.queries_per_s, "frac_of_peak": st.queries_per_s / peak.queries_per_s,
            "offered_load": "80 % of the batched peak", "requests": st.requests,

@@ -76,6 +76,7 @@ struct gdf_server {
   std::vector<gdf_ctx*> instances;
   std::unordered_map<gdf_ctx*, int> busy;  // requests of the instance on the device
   int64_t resident = 0, transient = 0;
+  int max_train = 1, train_busy = 0;  // slots training may hold / holds
   std::deque<Request*> pending;
   std::unordered_map<uint64_t, Request*> all;
   std::vector<Slot> slots;
@@ -113,7 +114,8 @@ void admit(gdf_server* s) {
     bool ok = !inst_busy && mem_ok;
     if (ok && q->r.kind == GDF_REQ_INFER)
       ok = static_cast<int>(infer.size()) < s->cfg.max_batch && (!infer.empty() || slots_needed < free_slots.size());
-    if (ok && q->r.kind == GDF_REQ_TRAIN) ok = slots_needed < free_slots.size();
+    if (ok && q->r.kind == GDF_REQ_TRAIN)
+      ok = slots_needed < free_slots.size() && s->train_busy + static_cast<int>(train.size()) < s->max_train;
     taken.push_back(inst);  // keeps arrival order per instance
     if (!ok) {
       ++it;
@@ -144,6 +146,7 @@ void admit(gdf_server* s) {
                     sl.stream);
     sl.reqs.assign(1, q);
     sl.busy = true;
+    s->train_busy += 1;
     cudaEventRecord(sl.done, sl.stream);
   }
   if (!infer.empty()) {
@@ -173,6 +176,7 @@ bool complete(gdf_server* s) {
     for (Request* q : sl.reqs) {
       if (e != cudaSuccess && q->status == GDF_OK) q->status = GDF_ERR_CUDA;
       if (q->r.kind == GDF_REQ_TRAIN) {
+        s->train_busy -= 1;
         q->stats.loss = sl.out->stats[0] / static_cast<double>(q->r.n);
         q->stats.grad_norm = std::sqrt(sl.out->stats[1]);
         q->stats.n_records = q->r.n;
@@ -214,12 +218,16 @@ extern "C" {
 
 gdf_status gdf_server_create(const gdf_server_config* cfg, gdf_server** out) {
   if (!cfg || !out) return sfail(GDF_ERR_INVALID_ARG, "null config / output");
-  if (cfg->slots < 1 || cfg->slots > 64 || cfg->max_batch < 1 || cfg->max_batch > 4096 || cfg->hbm_budget_bytes <= 0)
-    return sfail(GDF_ERR_INVALID_ARG, "slots in [1, 64], max_batch in [1, 4096], positive budget");
+  if (cfg->slots < 1 || cfg->slots > 64 || cfg->max_batch < 1 || cfg->max_batch > 4096 ||
+      cfg->max_train_slots < 0 || cfg->hbm_budget_bytes <= 0)
+    return sfail(GDF_ERR_INVALID_ARG,
+                 "slots in [1, 64], max_batch in [1, 4096], max_train_slots >= 0, positive budget");
   *out = nullptr;
   gdf_server* s = new (std::nothrow) gdf_server();
   if (!s) return sfail(GDF_ERR_OOM_BUDGET, "host allocation failed");
   s->cfg = *cfg;
+  s->max_train = cfg->max_train_slots > 0 ? std::min(cfg->max_train_slots, cfg->slots)
+                                          : std::max(1, cfg->slots - 1);
   if (cudaSetDevice(cfg->device) != cudaSuccess) {
     delete s;
     return sfail(GDF_ERR_CUDA, "cudaSetDevice");

@@ -126,7 +126,7 @@ class Request(C.Structure):
 
 class ServerConfig(C.Structure):
     _fields_ = [("device", C.c_int32), ("slots", C.c_int32), ("max_batch", C.c_int32),
-                ("hbm_budget_bytes", C.c_int64)]
+                ("max_train_slots", C.c_int32), ("hbm_budget_bytes", C.c_int64)]
 
 
 class ServerStats(C.Structure):
@@ -502,8 +502,9 @@ def ctx_bytes(ctx) -> int:
 class Server:
     """gdf_server: resident instances, continuous admission and batching."""
 
-    def __init__(self, budget_bytes: int, slots: int = 4, max_batch: int = 16, device: int = 0):
-        cfg = ServerConfig(device, slots, max_batch, budget_bytes)
+    def __init__(self, budget_bytes: int, slots: int = 4, max_batch: int = 16, device: int = 0,
+                 max_train_slots: int = 0):
+        cfg = ServerConfig(device, slots, max_batch, max_train_slots, budget_bytes)
         h = C.c_void_p()
         check(lib().gdf_server_create(C.byref(cfg), C.byref(h)))
         self.h = h

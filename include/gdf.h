@@ -414,6 +414,7 @@ typedef struct gdf_server_config {
   int32_t device;
   int32_t slots;              /* concurrent device streams (1..64)            */
   int32_t max_batch;          /* inference requests per grouped launch        */
+  int32_t max_train_slots;    /* slots training may hold at once (0: slots-1) */
   int64_t hbm_budget_bytes;   /* resident instances + in-flight requests      */
 } gdf_server_config;
 
