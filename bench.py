@@ -171,7 +171,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="CPU-baseline sample length; 0 skips it (profiling runs)")
     ap.add_argument("--skip-e2e", action="store_true", help="profiling runs: kernel timing only")
-    ap.add_argument("--stages", default="infer,train,records,bf16,grouped,serve",
+    ap.add_argument("--stages", default="infer,train,records,forms,grouped,serve",
                     help="comma list of infer, train, records (profiling runs select one)")
     args = ap.parse_args()
     stages = set(args.stages.split(","))
@@ -287,25 +287,28 @@ def main():
         train_times, last = time_train(ctx, cfg, W, nb, rank, dev, stream, flush, args)
     if "records" in stages:
         rec_times, n_rec, rec_bytes = time_records(ctx, W, n, rank, dev, stream, flush, args)
-    bf16_times = []
-    if "bf16" in stages:
-        # the same bounce with the bf16 inference form (MLP operands in bf16)
+    form_times = {}
+    if "forms" in stages:
+        # the same bounce with the bf16 and FP8 inference forms
         import pygdf
-        cb, _, _ = make_context(args.workload, seed=1234 + rank, precision=pygdf.PREC_BF16)
-        for i in range(args.warmup):
-            wi.copy_(wi0)
-            cb.infer(q, wi, guided=guided, seed=7, offset=i, n=n, stream=stream)
-        for i in range(args.steps):
-            wi.copy_(wi0)
-            flush.zero_()
-            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            s.record(stream)
-            cb.infer(q, wi, guided=guided, seed=7, offset=1000 + i, n=n, stream=stream)
-            e.record(stream)
-            e.synchronize()
-            bf16_times.append(s.elapsed_time(e))
-        cb.sync(stream)
-        cb.close()
+        for name, prec in (("bf16", pygdf.PREC_BF16), ("fp8", pygdf.PREC_FP8)):
+            cb, _, _ = make_context(args.workload, seed=1234 + rank, precision=prec)
+            for i in range(args.warmup):
+                wi.copy_(wi0)
+                cb.infer(q, wi, guided=guided, seed=7, offset=i, n=n, stream=stream)
+            ts = []
+            for i in range(args.steps):
+                wi.copy_(wi0)
+                flush.zero_()
+                s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                s.record(stream)
+                cb.infer(q, wi, guided=guided, seed=7, offset=1000 + i, n=n, stream=stream)
+                e.record(stream)
+                e.synchronize()
+                ts.append(s.elapsed_time(e))
+            form_times[name] = ts
+            cb.sync(stream)
+            cb.close()
     grouped = None
     if "grouped" in stages and args.workload == "full":
         grouped = time_grouped(W, rank, dev, stream, flush, args)
@@ -315,7 +318,7 @@ def main():
     clk = clocks.stop()
     ctx.sync(stream)
     _report(args, rank, world, dist, dev, n, cfg, params, times, e2e_times, train_times, rec_times,
-            last, n_rec, rec_bytes, clk, nb, workload_name, threads, q_h, wi_h, guided_h, bf16_times,
+            last, n_rec, rec_bytes, clk, nb, workload_name, threads, q_h, wi_h, guided_h, form_times,
             grouped, serving)
     ctx.close()
     if dist:
@@ -546,7 +549,7 @@ def time_records(ctx, W, n, rank, dev, stream, flush, args):
 
 
 def _report(args, rank, world, dist, dev, n, cfg, params, times, e2e_times, train_times, rec_times,
-            last, n_rec, rec_bytes, clk, nb, workload_name, threads, q_h, wi_h, guided_h, bf16_times,
+            last, n_rec, rec_bytes, clk, nb, workload_name, threads, q_h, wi_h, guided_h, form_times,
             grouped, serving):
     import torch
     ms = statistics.mean(times)
@@ -603,11 +606,13 @@ def _report(args, rank, world, dist, dev, n, cfg, params, times, e2e_times, trai
                 "achieved_gbs": rec_bytes / (ms_rec * 1e-3) / 1e9,
                 "frac_hbm": rec_bytes / (ms_rec * 1e-3) / 1e9 / peaks["hbm_gbs"],
                 "launches_per_step": 3}
-        if bf16_times:
-            mb = statistics.mean(bf16_times)
-            line["bf16"] = {"metric": "guided queries/s, bf16 MLP operands (fp32 accumulation)",
-                            "value": n * world / (mb * 1e-3), "unit": "queries/s", "ms_per_step": mb,
-                            "vs_fp16": ms / mb}
+        what = {"bf16": "bf16 MLP operands (fp32 accumulation)",
+                "fp8": "e4m3 hidden matrices, per-matrix and per-row power-of-two scales (fp32 accumulation)"}
+        for name, ts in form_times.items():
+            mb = statistics.mean(ts)
+            line[name] = {"metric": "guided queries/s, " + what[name],
+                          "value": n * world / (mb * 1e-3), "unit": "queries/s", "ms_per_step": mb,
+                          "vs_fp16": ms / mb}
         if grouped:
             line["grouped"] = grouped
         if serving:

@@ -13,6 +13,7 @@
 #include <cstdint>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
+#include <cuda_fp8.h>
 
 #include "df_math.cuh"
 #include "sm100.cuh"
@@ -334,13 +335,20 @@ __device__ __forceinline__ void wait_mma(Wg& c) {
   tc_fence_after();
 }
 
-// ReLU of the 64 accumulator columns -> fp16 -> tile_a (K = 64).
-__device__ __forceinline__ void relu_to_tile(Wg& c) {
+// ReLU of the 64 accumulator columns -> fp16 -> tile_a (K = 64). SCALED:
+// the accumulators are first multiplied by d (a power of two: the FP8
+// form's descale of its last e4m3 layer).
+template <bool SCALED = false>
+__device__ __forceinline__ void relu_to_tile(Wg& c, float d = 1.f) {
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
     uint32_t r[32];
     tmem_ld32(c.tmem + c.lane_base + h * 32, r);
     tmem_ld_wait();
+    if constexpr (SCALED) {
+#pragma unroll
+      for (int j = 0; j < 32; ++j) r[j] = __float_as_uint(__uint_as_float(r[j]) * d);
+    }
 #pragma unroll
     for (int kc = 0; kc < 4; ++kc) {
       uint32_t v[4];
@@ -382,6 +390,104 @@ __device__ __forceinline__ void mlp_tail(Wg& c, uint32_t w_s, int n_hidden, uint
     const bool last = l == n_hidden;
     issue(c, &a, 1, w_s, 64, last ? n_out : 64u);
     w_s += (last ? n_out : 64u) * 64u * 2u;
+  }
+  wait_mma(c);
+}
+
+// ------------------------------------------------------------ FP8 form
+// The 64x64 hidden matrices run as e4m3 x e4m3 MMAs with fp32 accumulation;
+// the first matrix (encoded inputs) and the output matrix stay fp16. A
+// hidden matrix W is stored as e4m3(W * 2^kw) with one exponent per matrix,
+// an activation row h as e4m3(h * 2^kr) with one exponent per row (query),
+// both chosen from the absolute maximum, so the accumulator of row r is
+// descaled exactly by 2^-(kw + kr).
+
+// Exponent k of the largest power of two with amax * 2^k <= 448 (e4m3's
+// largest finite value), clamped to [-100, 100]; 0 for a zero or
+// non-finite amax.
+__device__ __forceinline__ int e4m3_scale_exp(float amax) {
+  const uint32_t b = __float_as_uint(amax);
+  const uint32_t ef = (b >> 23) & 0xffu;
+  if (amax == 0.f || ef == 0xffu) return 0;
+  // amax = m * 2^e with m in [1, 2): m * 2^(e+k) <= 1.75 * 2^8
+  const int k = ((b & 0x7fffffu) <= 0x600000u ? 8 : 7) - (static_cast<int>(ef) - 127);
+  return k < -100 ? -100 : (k > 100 ? 100 : k);
+}
+
+__device__ __forceinline__ float exp2i(int k) { return __uint_as_float(static_cast<uint32_t>(k + 127) << 23); }
+
+// Two values -> e4m3 (round to nearest even, saturating), low byte first.
+__device__ __forceinline__ uint32_t pack_e4m3x2(float a, float b) {
+  return static_cast<uint32_t>(__nv_cvt_float2_to_fp8x2(make_float2(a, b), __NV_SATFINITE, __NV_E4M3));
+}
+
+// ReLU(acc * d) of the 64 accumulator columns -> e4m3 with the row's
+// exponent -> tile_a as a 64-byte row (canonical layout of 32 two-byte
+// columns). Returns the row's descale 2^-k.
+__device__ __forceinline__ float relu_to_tile_f8(Wg& c, float d) {
+  uint32_t r0[32], r1[32];
+  tmem_ld32(c.tmem + c.lane_base, r0);
+  tmem_ld32(c.tmem + c.lane_base + 32, r1);
+  tmem_ld_wait();
+  float amax = 0.f;
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    // fmaxf(NaN, 0) = 0, tcnn relu's NaN behaviour
+    const float a = fmaxf(__uint_as_float(r0[j]) * d, 0.f), b = fmaxf(__uint_as_float(r1[j]) * d, 0.f);
+    r0[j] = __float_as_uint(a);
+    r1[j] = __float_as_uint(b);
+    amax = fmaxf(amax, fmaxf(a, b));
+  }
+  const int k = e4m3_scale_exp(amax);
+  const float s = exp2i(k);
+#pragma unroll
+  for (int kc = 0; kc < 4; ++kc) {
+    const uint32_t* r = kc < 2 ? r0 + kc * 16 : r1 + (kc - 2) * 16;
+    uint32_t v[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      v[j] = pack_e4m3x2(__uint_as_float(r[4 * j]) * s, __uint_as_float(r[4 * j + 1]) * s) |
+             (pack_e4m3x2(__uint_as_float(r[4 * j + 2]) * s, __uint_as_float(r[4 * j + 3]) * s) << 16);
+    *reinterpret_cast<uint4*>(c.tile_a + chunk_off(c.row, kc, 32)) = make_uint4(v[0], v[1], v[2], v[3]);
+  }
+  tc_fence_before();
+  return exp2i(-k);
+}
+
+// D[tmem] = A8 * W8^T for a 64-byte-row e4m3 A tile at a_s and the e4m3
+// [N x 64] matrix at w_s: two K = 32 steps.
+__device__ __forceinline__ void issue_f8(Wg& c, uint32_t a_s, uint32_t w_s, uint32_t N) {
+  if (!c.leader) return;
+  tc_fence_after();
+  const uint32_t idesc = idesc_f16(128, N, 0, 0, 0);  // format fields 0: E4M3 x E4M3
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    const uint64_t ad = smem_desc(a_s + j * 256, 128, 32u * 16u);
+    const uint64_t bd = smem_desc(w_s + j * 256, 128, 32u * 16u);
+    mma_f8_ss(c.tmem, ad, bd, idesc, j > 0 ? 1u : 0u);
+  }
+  mma_commit(c.bar);
+}
+
+// mlp_tail of the FP8 form: matrices 1..n_hidden-1 e4m3 (4096 bytes each
+// from w_s), then the fp16 output matrix; descale[l-1] = 2^-kw of matrix l.
+__device__ __forceinline__ void mlp_tail_f8(Wg& c, uint32_t w_s, int n_hidden, uint32_t n_out,
+                                            const float* descale) {
+  const ASeg a{c.tile_a_s, 64, 4};
+  float d = 1.f;
+  for (int l = 1; l <= n_hidden; ++l) {
+    wait_mma(c);
+    if (l < n_hidden) {
+      const float inv_s = relu_to_tile_f8(c, d);
+      publish(c);
+      issue_f8(c, c.tile_a_s, w_s, 64);
+      w_s += 64u * 64u;
+      d = descale[l - 1] * inv_s;
+    } else {
+      relu_to_tile<true>(c, d);
+      publish(c);
+      issue(c, &a, 1, w_s, 64, n_out);
+    }
   }
   wait_mma(c);
 }

@@ -162,6 +162,20 @@ __device__ __forceinline__ void mma_f16_ss(uint32_t d_tmem, uint64_t a_desc, uin
       : "memory");
 }
 
+// D[tmem] (+)= A[smem] * B[smem]^T with e4m3 operands (kind::f8f6f4; the
+// instruction descriptor's format fields 0 = E4M3), one instruction covers
+// K = 32 (32 bytes per row: the same two core matrices as a K = 16 fp16
+// step, so descriptors advance as for fp16).
+__device__ __forceinline__ void mma_f8_ss(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc,
+                                          uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
 // Arrive on `bar` once all tcgen05 operations issued so far by this thread
 // have completed.
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {

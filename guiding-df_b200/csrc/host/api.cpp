@@ -104,7 +104,9 @@ gdf_status validate(const gdf_config& c) {
   if (c.precision < GDF_PREC_FP16 || c.precision > GDF_PREC_FP8)
     return fail(GDF_ERR_INVALID_ARG, "precision");
   if (c.precision == GDF_PREC_FP8)
-    return fail(GDF_ERR_UNSUPPORTED, "the FP8 inference form is not built; use FP16 or BF16");
+    for (const gdf_mlp_config* m : {&c.mlp_theta, &c.mlp_phi})
+      if (m->n_hidden_layers + 1 > gdf::kMaxMlpLayers)
+        return fail(GDF_ERR_UNSUPPORTED, "FP8 form: at most 9 hidden layers");
   if (c.max_queries < 0 || c.max_train_batch < 0)
     return fail(GDF_ERR_INVALID_ARG, "negative capacity");
   const int64_t cap = c.max_train_batch > 0 ? c.max_train_batch : 65536;
@@ -135,7 +137,7 @@ gdf_status dalloc(T** p, size_t n) {
 void free_net(Net& n) {
   cudaFree(n.master); cudaFree(n.w16); cudaFree(n.ema16); cudaFree(n.adam_m);
   cudaFree(n.adam_v); cudaFree(n.adam_step); cudaFree(n.grad); cudaFree(n.blob_ema);
-  cudaFree(n.blob_w16);
+  cudaFree(n.blob_w16); cudaFree(n.blob_f8);
   n = Net{};
 }
 
@@ -197,6 +199,12 @@ gdf_status alloc_net(Net& n) {
       (s = dalloc(&n.blob_ema, static_cast<size_t>(n.n_mlp))) ||
       (s = dalloc(&n.blob_w16, static_cast<size_t>(n.n_mlp))))
     return s;
+  if (n.infer_f8) {
+    n.f8_bytes = gdf::fp8_blob_bytes(n.rows.data(), n.cols.data(), static_cast<int>(n.rows.size()), &n.f8_pack);
+    if ((s = dalloc(&n.blob_f8, n.f8_bytes))) return s;
+    n.f8_pack.src = n.ema16;
+    n.f8_pack.dst = n.blob_f8;
+  }
   return GDF_OK;
 }
 
@@ -208,6 +216,7 @@ gdf_status repack(Net& n, cudaStream_t st) {
   e = gdf::launch_pack_mlp(n.w16, n.blob_w16, n.rows.data(), n.cols.data(),
                            static_cast<int>(n.rows.size()), st);
   if (e != cudaSuccess) return cuda_fail(e, "pack w16");
+  if (n.infer_f8 && (e = gdf::launch_pack_fp8(n.f8_pack, st)) != cudaSuccess) return cuda_fail(e, "pack fp8");
   return GDF_OK;
 }
 
@@ -552,6 +561,7 @@ gdf_status gdf_create(const gdf_config* cfg, gdf_ctx** out) {
   if ((s = layout_df_net(c.cfg, 0, c.net[0])) || (s = layout_df_net(c.cfg, 1, c.net[1])))
     return cleanup(s);
   c.net[0].infer_bf16 = c.net[1].infer_bf16 = c.cfg.precision == GDF_PREC_BF16;
+  c.net[0].infer_f8 = c.net[1].infer_f8 = c.cfg.precision == GDF_PREC_FP8;
   if (c.cfg.nrc_enable && (s = layout_nrc_net(c.cfg, c.net[2]))) return cleanup(s);
   for (Net& n : c.net)
     if (n.present && (s = alloc_net(n))) return cleanup(s);
@@ -614,7 +624,7 @@ gdf_status gdf_ctx_bytes(const gdf_ctx* ctx, int64_t* bytes) {
   for (const Net& n : c.net) {
     if (!n.present) continue;
     // master, m, v, step, grad (4 B) + w16, ema16 (2 B) + two MLP blobs
-    b += n.n_params * (4 * 5 + 2 * 2) + n.n_mlp * 2 * 2;
+    b += n.n_params * (4 * 5 + 2 * 2) + n.n_mlp * 2 * 2 + n.f8_bytes;
   }
   const int64_t lf = static_cast<int64_t>(c.cfg.grid_theta.n_levels) * c.cfg.grid_theta.n_features_per_level;
   b += c.net[0].n_grid * 2 * 2;                               // interleaved inference grid
@@ -706,16 +716,18 @@ static gdf::DfKernelParams df_params(Context& c) {
   const Net& f = c.net[1];
   p.grid_theta = t.ema16 + t.n_mlp;
   p.grid_phi = f.ema16 + f.n_mlp;
-  p.blob_theta = t.blob_ema;
-  p.blob_phi = f.blob_ema;
-  p.blob_theta_bytes = t.blob_bytes;
-  p.blob_phi_bytes = f.blob_bytes;
+  const bool f8 = c.cfg.precision == GDF_PREC_FP8;
+  p.blob_theta = f8 ? reinterpret_cast<const __half*>(t.blob_f8) : t.blob_ema;
+  p.blob_phi = f8 ? reinterpret_cast<const __half*>(f.blob_f8) : f.blob_ema;
+  p.blob_theta_bytes = f8 ? t.f8_bytes : t.blob_bytes;
+  p.blob_phi_bytes = f8 ? f.f8_bytes : f.blob_bytes;
   p.hidden_theta = t.hidden;
   p.hidden_phi = f.hidden;
   p.gl_theta = t.gl;
   p.gl_phi = f.gl;
   p.err = c.d_err;
   p.bf16 = c.cfg.precision == GDF_PREC_BF16;
+  p.fp8 = f8;
   return p;
 }
 
@@ -1055,6 +1067,9 @@ gdf_status gdf_train_step(gdf_ctx* ctx, const float* in_theta, const float* in_p
   p.grid_phi = c.net[1].w16 + c.net[1].n_mlp;
   p.blob_theta = c.net[0].blob_w16;
   p.blob_phi = c.net[1].blob_w16;
+  p.blob_theta_bytes = c.net[0].blob_bytes;
+  p.blob_phi_bytes = c.net[1].blob_bytes;
+  p.bf16 = p.fp8 = 0;
   p.queries = in_theta;
   p.in_phi = in_phi;
   p.target = target;
@@ -1094,6 +1109,8 @@ gdf_status gdf_train_step(gdf_ctx* ctx, const float* in_theta, const float* in_p
     a.grid_grad = c.net[id].grad + c.net[id].n_mlp;
     e = gdf::launch_adam_ema(a, st);
     if (e != cudaSuccess) return cuda_fail(e, "adam_ema");
+    if (c.net[id].infer_f8 && (e = gdf::launch_pack_fp8(c.net[id].f8_pack, st)) != cudaSuccess)
+      return cuda_fail(e, "pack fp8");
   }
   // 4. FP64 loss and gradient-norm reductions
   e = gdf::launch_train_stats(c.ws.fwd, n, c.ws.sq, 2 * gdf::kAdamBlocks, c.ws.stats, st);

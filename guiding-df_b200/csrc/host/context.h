@@ -10,6 +10,7 @@
 
 #include "../../../include/gdf.h"
 #include "../device/grid_levels.h"
+#include "../kernels/df_kernels.h"
 
 namespace gdf {
 
@@ -35,6 +36,12 @@ struct Net {
   __half* blob_w16 = nullptr;  // n_mlp, canonical layout of w16
   uint32_t blob_bytes = 0;
   bool infer_bf16 = false;     // blob_ema holds bf16 (bf16 inference form, DF networks)
+  // FP8 inference form (DF networks): e4m3 hidden matrices, rebuilt from
+  // ema16 after every optimizer step (launch_pack_fp8)
+  bool infer_f8 = false;
+  uint8_t* blob_f8 = nullptr;
+  uint32_t f8_bytes = 0;
+  Fp8PackParams f8_pack{};
   uint32_t opt_step = 0;       // optimizer step counter (Adam m_current_step)
 };
 

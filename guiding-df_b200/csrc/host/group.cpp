@@ -122,6 +122,8 @@ gdf_status check_jobs(const gdf_job* jobs, int32_t n, JobSet* js) {
     const gdf::Context& c = j.ctx->c;
     const int levels = c.cfg.grid_theta.n_levels, features = c.cfg.grid_theta.n_features_per_level;
     const bool linear = c.cfg.pdf_interp == GDF_PDF_LINEAR, bf16 = c.cfg.precision == GDF_PREC_BF16;
+    if (c.cfg.precision == GDF_PREC_FP8)
+      return gfail(GDF_ERR_UNSUPPORTED, "grouped launches take the FP16 and BF16 forms");
     if (i == 0) {
       js->levels = levels;
       js->features = features;

@@ -20,6 +20,7 @@
 //     sampling epilogue.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
+#include <cuda_fp8.h>
 
 #include "../device/df_math.cuh"
 #include "../device/df_tile.cuh"
@@ -58,7 +59,9 @@ struct DfWidths {
 //   5. phi input rest (SH | OneBlob | TriangleWave(u_theta) | 1-pad) -> tile A;
 //      phi layer 0 reads K steps from tile P then tile A;
 //   6. phi layers, epilogue -> u_phi, pdf_phi -> guiding data.
-template <int L, int F, int NBT, int NBP, bool LINEAR, int MODE, int WGS, bool BF16>
+// FMT: MLP operand format of the inference forms, 0 fp16, 1 bf16, 2 FP8
+// (e4m3 hidden matrices, mlp_tail_f8).
+template <int L, int F, int NBT, int NBP, bool LINEAR, int MODE, int WGS, int FMT>
 __global__ void __launch_bounds__(128 * WGS, 1) df_fused_kernel(const __grid_constant__ DfKernelParams p) {
   using Wd = DfWidths<L, F>;
   constexpr uint32_t LF = L * F;
@@ -124,11 +127,17 @@ __global__ void __launch_bounds__(128 * WGS, 1) df_fused_kernel(const __grid_con
   c.row = tid & 127u;
   c.leader = c.row == 0;
   c.err = p.err;
-  c.bf16 = kFeat && BF16;  // operand format of the inference forms
+  c.bf16 = kFeat && FMT == 1;  // operand format of the inference forms
+  constexpr bool kF8 = kFeat && FMT == 2;
   const uint32_t w_theta = smem_addr(smem);
   const uint32_t w_phi = smem_addr(smem + off_phi);
   const uint32_t w_theta_hidden = w_theta + 64u * KT * 2u;
   const uint32_t w_phi_hidden = w_phi + 64u * (LF + KR) * 2u;
+  // FP8 form: descale factors after each blob's output matrix
+  const float* ds_theta = reinterpret_cast<const float*>(
+      smem + 64u * KT * 2u + static_cast<uint32_t>(p.hidden_theta - 1) * 4096u + NBT * 128u);
+  const float* ds_phi = reinterpret_cast<const float*>(
+      smem + off_phi + 64u * (LF + KR) * 2u + static_cast<uint32_t>(p.hidden_phi - 1) * 4096u + NBP * 128u);
 
   const int64_t n_tiles = (p.n + 127) / 128;
   // Both feature tiles of tile t, one bulk copy each, completing on fbar.
@@ -209,7 +218,8 @@ __global__ void __launch_bounds__(128 * WGS, 1) df_fused_kernel(const __grid_con
       tile::issue(c, &a, 1, w_theta, KT, 64);
     }
     // ---- 2./3. theta layers
-    tile::mlp_tail(c, w_theta_hidden, p.hidden_theta, NBT);
+    if constexpr (kF8) tile::mlp_tail_f8(c, w_theta_hidden, p.hidden_theta, NBT, ds_theta);
+    else tile::mlp_tail(c, w_theta_hidden, p.hidden_theta, NBT);
     // ---- 4. theta epilogue
     float4 wi = make_float4(0.f, 0.f, 1.f, 1.f);
     float u[4] = {0.f, 0.f, 0.f, 0.f};
@@ -261,7 +271,8 @@ __global__ void __launch_bounds__(128 * WGS, 1) df_fused_kernel(const __grid_con
       tile::issue(c, a, 2, w_phi, LF + KR, 64);
     }
     // ---- 6. phi layers and epilogue
-    tile::mlp_tail(c, w_phi_hidden, p.hidden_phi, NBP);
+    if constexpr (kF8) tile::mlp_tail_f8(c, w_phi_hidden, p.hidden_phi, NBP, ds_phi);
+    else tile::mlp_tail(c, w_phi_hidden, p.hidden_phi, NBP);
     if constexpr (kFeat) {
       // every MMA that read this tile's feature tiles has completed
       const int64_t next = t + static_cast<int64_t>(gridDim.x) * WGS;
@@ -345,20 +356,59 @@ __global__ void pack_mlp_kernel(const __half* __restrict__ src, __half* __restri
   dst[canon_offset(r, cc, static_cast<uint32_t>(cols))] = v;
 }
 
+// One block per matrix (Fp8PackParams): fp16 copies for the first and last
+// matrices, e4m3(W * 2^k) for the hidden ones with k from the matrix's
+// absolute maximum (tile::e4m3_scale_exp) and descale 2^-k.
+__global__ void __launch_bounds__(256) pack_fp8_kernel(const __grid_constant__ Fp8PackParams p) {
+  const int l = blockIdx.x;
+  const int rows = p.rows[l], cols = p.cols[l];
+  const int n = rows * cols;
+  const __half* src = p.src + p.src_off[l];
+  if (l == 0 || l == p.n_layers - 1) {
+    __half* dst = reinterpret_cast<__half*>(p.dst + p.dst_off[l]);
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+      dst[canon_offset(static_cast<uint32_t>(i / cols), static_cast<uint32_t>(i % cols),
+                       static_cast<uint32_t>(cols))] = src[i];
+    return;
+  }
+  __shared__ float red[8];
+  float amax = 0.f;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) amax = fmaxf(amax, fabsf(__half2float(src[i])));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = amax;
+  __syncthreads();
+  amax = red[0];
+  for (int w = 1; w < static_cast<int>(blockDim.x >> 5); ++w) amax = fmaxf(amax, red[w]);
+  const int k = tile::e4m3_scale_exp(amax);
+  const float s = tile::exp2i(k);
+  if (threadIdx.x == 0) reinterpret_cast<float*>(p.dst + p.descale_off)[l - 1] = tile::exp2i(-k);
+  uint8_t* dst = p.dst + p.dst_off[l];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const uint32_t r = static_cast<uint32_t>(i / cols), cc = static_cast<uint32_t>(i % cols);
+    // byte cc of a 64-byte row: two-byte column cc / 2 of the canonical layout
+    const uint32_t off = 2u * canon_offset(r, cc >> 1, static_cast<uint32_t>(cols) >> 1) + (cc & 1u);
+    dst[off] = static_cast<uint8_t>(__nv_cvt_float_to_fp8(__half2float(src[i]) * s, __NV_SATFINITE, __NV_E4M3));
+  }
+}
+
 template <int L, int F, int NBT, int NBP, bool LIN>
 cudaError_t launch_t(int mode, const DfKernelParams& p, size_t smem, int num_sms, cudaStream_t st) {
   const int64_t n_tiles = (p.n + 127) / 128;
   int64_t ctas = (n_tiles + kDfWarpgroups - 1) / kDfWarpgroups;
   if (ctas > num_sms) ctas = num_sms;
   if (ctas < 1) ctas = 1;
-  const bool bf = p.bf16 != 0 && mode != kModeTrainFwd;
+  const int fmt = mode == kModeTrainFwd ? 0 : (p.fp8 ? 2 : (p.bf16 ? 1 : 0));
+  auto pick = [&](auto k16, auto kb16, auto k8) { return fmt == 2 ? k8 : (fmt == 1 ? kb16 : k16); };
   auto kern = mode == kModeInfer
-                  ? (bf ? df_fused_kernel<L, F, NBT, NBP, LIN, kModeInfer, kDfWarpgroups, true>
-                        : df_fused_kernel<L, F, NBT, NBP, LIN, kModeInfer, kDfWarpgroups, false>)
+                  ? pick(df_fused_kernel<L, F, NBT, NBP, LIN, kModeInfer, kDfWarpgroups, 0>,
+                         df_fused_kernel<L, F, NBT, NBP, LIN, kModeInfer, kDfWarpgroups, 1>,
+                         df_fused_kernel<L, F, NBT, NBP, LIN, kModeInfer, kDfWarpgroups, 2>)
               : mode == kModeEval
-                  ? (bf ? df_fused_kernel<L, F, NBT, NBP, LIN, kModeEval, kDfWarpgroups, true>
-                        : df_fused_kernel<L, F, NBT, NBP, LIN, kModeEval, kDfWarpgroups, false>)
-                  : df_fused_kernel<L, F, NBT, NBP, LIN, kModeTrainFwd, kDfWarpgroups, false>;
+                  ? pick(df_fused_kernel<L, F, NBT, NBP, LIN, kModeEval, kDfWarpgroups, 0>,
+                         df_fused_kernel<L, F, NBT, NBP, LIN, kModeEval, kDfWarpgroups, 1>,
+                         df_fused_kernel<L, F, NBT, NBP, LIN, kModeEval, kDfWarpgroups, 2>)
+                  : df_fused_kernel<L, F, NBT, NBP, LIN, kModeTrainFwd, kDfWarpgroups, 0>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
   if (e != cudaSuccess) return e;
@@ -423,6 +473,36 @@ cudaError_t launch_df_post(int nbt, int nbp, bool linear, const float* lt, const
   GDF_POST(16, 32)
 #undef GDF_POST
   return cudaErrorNotSupported;
+}
+
+uint32_t fp8_blob_bytes(const int32_t* rows, const int32_t* cols, int n_layers, Fp8PackParams* lay) {
+  uint32_t off = 0;
+  int64_t src = 0;
+  for (int l = 0; l < n_layers; ++l) {
+    const bool f16 = l == 0 || l == n_layers - 1;
+    if (lay) {
+      lay->rows[l] = rows[l];
+      lay->cols[l] = cols[l];
+      lay->src_off[l] = src;
+      lay->dst_off[l] = off;
+    }
+    off += static_cast<uint32_t>(rows[l] * cols[l] * (f16 ? 2 : 1));
+    src += static_cast<int64_t>(rows[l]) * cols[l];
+  }
+  if (lay) {
+    lay->n_layers = n_layers;
+    lay->descale_off = off;
+  }
+  off += static_cast<uint32_t>(n_layers > 2 ? n_layers - 2 : 0) * 4u;
+  return (off + 15u) & ~15u;
+}
+
+cudaError_t launch_pack_fp8(const Fp8PackParams& p, cudaStream_t st) {
+  if (p.n_layers < 2 || p.n_layers > kMaxMlpLayers) return cudaErrorInvalidValue;
+  for (int l = 1; l + 1 < p.n_layers; ++l)
+    if (p.rows[l] != 64 || p.cols[l] != 64) return cudaErrorInvalidValue;
+  pack_fp8_kernel<<<p.n_layers, 256, 0, st>>>(p);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_pack_mlp(const __half* src, __half* dst, const int32_t* rows, const int32_t* cols,

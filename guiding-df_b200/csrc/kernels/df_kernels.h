@@ -50,6 +50,7 @@ struct DfKernelParams {
   gdf_aabb aabb;
   float* dir_pdf;                    // n x 4 world direction + solid-angle pdf, nullable
   int32_t bf16;                      // inference form with bf16 MLP operands
+  int32_t fp8;                       // FP8 inference form: blobs from launch_pack_fp8
 };
 
 struct GridFeatParams {
@@ -91,5 +92,23 @@ cudaError_t launch_df_post(int bins_theta, int bins_phi, bool linear, const floa
 cudaError_t launch_pack_mlp(const __half* src, __half* dst, const int32_t* rows,
                             const int32_t* cols, int n_layers, cudaStream_t stream,
                             bool to_bf16 = false);
+
+// FP8 inference blob of one DF network from its fp16 EMA matrices (row-major,
+// back to back): matrix 0 and the last matrix fp16 in the canonical layout,
+// the 64x64 hidden matrices e4m3 scaled by a power of two per matrix
+// (canonical layout of 64-byte rows, 4096 bytes each), then one float
+// descale per hidden matrix. fp8_blob_bytes gives the size.
+constexpr int kMaxMlpLayers = 10;
+struct Fp8PackParams {
+  const __half* src;
+  uint8_t* dst;
+  int32_t n_layers;
+  int32_t rows[kMaxMlpLayers], cols[kMaxMlpLayers];
+  int64_t src_off[kMaxMlpLayers];
+  uint32_t dst_off[kMaxMlpLayers];
+  uint32_t descale_off;
+};
+uint32_t fp8_blob_bytes(const int32_t* rows, const int32_t* cols, int n_layers, Fp8PackParams* layout);
+cudaError_t launch_pack_fp8(const Fp8PackParams& p, cudaStream_t stream);
 
 }  // namespace gdf

@@ -362,7 +362,8 @@ void go_nrc_encode(const go_nrc_config* c, const float* q15, float* out) {
 /* Number format of the DF networks' stored MLP inputs and activations:
  * 0 = fp16 (the reference's precision_t), 1 = bf16 (round to nearest
  * even), 2 = unrounded (kept in fp32 beside the FP64 accumulation: the
- * reference point of the precision comparison). */
+ * reference point of the precision comparison), 3 = the FP8 form (fp16
+ * first and output matrices, e4m3 hidden matrices: mlp_forward_fp8). */
 static int g_storage = 0;
 void go_set_storage(int fmt) { g_storage = fmt; }
 
@@ -400,8 +401,77 @@ static double dot_acc(const float* a, const float* b, int k) {
   return acc;
 }
 
+/* OCP E4M3 (4 exponent bits, bias 7, 3 mantissa bits, no infinities,
+ * largest finite 448) rounded to nearest even from a double, saturating
+ * to +-448 (cvt.rn.satfinite.e4m3x2.f32 semantics for finite inputs). */
+double go_round_e4m3(double x) {
+  if (isnan(x) || x == 0.0) return x;
+  const double a = fabs(x);
+  int e;
+  frexp(a, &e);             /* a = m * 2^e, m in [0.5, 1): leading exponent e-1 */
+  int lead = e - 1;
+  if (lead < -6) lead = -6; /* subnormals: quantum 2^-9 */
+  const double q = ldexp(1.0, lead - 3);
+  double r = nearbyint(a / q) * q;
+  if (r > 448.0) r = 448.0;
+  return copysign(r, x);
+}
+
+/* Exponent k of the largest power of two with amax * 2^k <= 448, clamped
+ * to [-100, 100]; 0 for a zero or non-finite amax. */
+int go_e4m3_scale_exp(double amax) {
+  if (amax == 0.0 || !isfinite(amax)) return 0;
+  int e;
+  const double m = frexp(amax, &e); /* amax = (2m) * 2^(e-1), 2m in [1, 2) */
+  const int k = (m <= 0.875 ? 8 : 7) - (e - 1);
+  return k < -100 ? -100 : (k > 100 ? 100 : k);
+}
+
+/* The FP8 inference form: matrix 0 over the fp16 inputs with fp16 weights;
+ * each 64x64 hidden matrix W as e4m3(W * 2^kw), kw from max|W|, over the
+ * row's activations e4m3(h * 2^kr), kr from the row's max, the product
+ * descaled by 2^-(kw+kr); ReLU before each quantisation; the last hidden
+ * activations rounded to fp16 for the fp16 output matrix. */
+static void mlp_forward_fp8(const float* w16, int k0, int width, int n_hidden, int n_out_pad,
+                            const float* x16, float* out) {
+  double acc[256], v[256];
+  float qa[256], h16[256];
+  static __thread float qw[256 * 256];
+  const float* w = w16;
+  for (int o = 0; o < width; ++o) acc[o] = dot_acc(w + (size_t)o * k0, x16, k0);
+  w += (size_t)width * k0;
+  double d = 1.0;
+  for (int l = 1; l <= n_hidden; ++l) {
+    double amax = 0.0;
+    for (int o = 0; o < width; ++o) {
+      const double y = acc[o] * d;
+      v[o] = y > 0.0 ? y : 0.0; /* NaN -> 0 */
+      if (v[o] > amax) amax = v[o];
+    }
+    if (l < n_hidden) {
+      const int kr = go_e4m3_scale_exp(amax);
+      for (int o = 0; o < width; ++o) qa[o] = (float)go_round_e4m3(ldexp(v[o], kr));
+      double wmax = 0.0;
+      for (int i = 0; i < width * width; ++i)
+        if (fabs((double)w[i]) > wmax) wmax = fabs((double)w[i]);
+      const int kw = go_e4m3_scale_exp(wmax);
+      for (int i = 0; i < width * width; ++i) qw[i] = (float)go_round_e4m3(ldexp((double)w[i], kw));
+      for (int o = 0; o < width; ++o) acc[o] = dot_acc(qw + (size_t)o * width, qa, width);
+      d = ldexp(1.0, -(kw + kr));
+      w += (size_t)width * width;
+    } else {
+      for (int o = 0; o < width; ++o) h16[o] = go_round_f16(v[o]);
+      for (int o = 0; o < n_out_pad; ++o) out[o] = (float)dot_acc(w + (size_t)o * width, h16, width);
+    }
+  }
+}
+
 void go_mlp_forward(const float* w16, int k0, int width, int n_hidden, int n_out_pad,
                     const float* x16, float* out, float* hidden_out) {
+  if (g_storage == 3 && !hidden_out) {
+    mlp_forward_fp8(w16, k0, width, n_hidden, n_out_pad, x16, out);
+    return;
+  }
   float h[256], hn[256];
   memcpy(h, x16, sizeof(float) * (size_t)k0);
   int k = k0;

@@ -137,6 +137,8 @@ void go_nrc_query(const go_nrc_config* c, const float* params16, const float* in
  * 1 bf16, 2 unrounded. */
 void go_set_storage(int fmt);
 float go_round_bf16(float x);
+double go_round_e4m3(double x);
+int go_e4m3_scale_exp(double amax);
 float go_store(double x);
 
 /* ---- path records (gdf_oracle_paths.c) ---------------------------------- */

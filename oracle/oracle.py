@@ -89,6 +89,8 @@ def lib():
             ("go_sample_pdf", [P, C.c_float, C.c_int, C.c_int], C.c_float),
             ("go_softmax2_times_n", [P, C.c_int], None),
             ("go_round_f16", [C.c_double], C.c_float),
+            ("go_round_e4m3", [C.c_double], C.c_double),
+            ("go_e4m3_scale_exp", [C.c_double], C.c_int),
             ("go_df_pdf_tables", [C.POINTER(DfCfg), P, P, P, P, P, P, C.c_int64], None),
             ("go_set_accumulation", [C.c_int], None),
             ("go_set_storage", [C.c_int], None),
@@ -163,7 +165,7 @@ def df_mlp_params(d: DfCfg, net: int) -> int:
     return int(lib().go_df_mlp_params(C.byref(d), net))
 
 
-STORAGE = {"fp16": 0, "bf16": 1, "none": 2}
+STORAGE = {"fp16": 0, "bf16": 1, "none": 2, "fp8": 3}
 
 
 def round_bf16(a) -> np.ndarray:
