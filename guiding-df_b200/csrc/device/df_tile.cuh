@@ -667,6 +667,53 @@ __device__ __noinline__ RowResult row_epilogue(uint32_t taddr, bool guided, floa
   return r;
 }
 
+// The CDF normalisation check in FP64: recomputes the row's pdfs exactly as
+// row_epilogue does (same operations, same order) from the logits still in
+// TMEM, sums them in double and max-merges |1 - sum p_i / N| per warp into
+// *norm_err as the bits of a non-negative double (NaN sorts above all).
+// Called by every lane of the warp, right after row_epilogue.
+template <int NB>
+__device__ __noinline__ void row_norm_check(uint32_t taddr, unsigned long long* norm_err) {
+  float v[NB];
+  if constexpr (NB == 16) {
+    uint32_t r[16];
+    tmem_ld16(taddr, r);
+    tmem_ld_wait();
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+  } else {
+    uint32_t r[NB];
+#pragma unroll
+    for (int c = 0; c < NB / 32; ++c) tmem_ld32(taddr + c * 32, *reinterpret_cast<uint32_t(*)[32]>(r + c * 32));
+    tmem_ld_wait();
+#pragma unroll
+    for (int i = 0; i < NB; ++i) v[i] = __uint_as_float(r[i]);
+  }
+  tc_fence_before();
+  float m = 0.0f;
+#pragma unroll
+  for (int i = 0; i < NB; ++i) m = fmaxf(m, v[i]);
+  constexpr float kLog2e = 1.4426950408889634074f;
+  const float ml = m * kLog2e;
+  float s = 0.0f;
+#pragma unroll
+  for (int i = 0; i < NB; ++i) {
+    v[i] = ex2_approx(fmaf(v[i], kLog2e, -ml));
+    s += v[i];
+  }
+  const float k = static_cast<float>(NB) / s;
+  double sum = 0.0;
+#pragma unroll
+  for (int i = 0; i < NB; ++i) sum += static_cast<double>(v[i] * k);
+  unsigned long long b = static_cast<unsigned long long>(__double_as_longlong(fabs(1.0 - sum / NB)));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long x = __shfl_xor_sync(0xffffffffu, b, o);
+    b = x > b ? x : b;
+  }
+  if ((threadIdx.x & 31u) == 0) atomicMax(norm_err, b);
+}
+
 // Training flavour of the epilogue (forward of LearnedDistribution::trainStep,
 // learnedDistribution.cpp:252-262): the logits are the network's fp16
 // outputs, softmax2 is stored as fp16 and multiplied by N in fp16

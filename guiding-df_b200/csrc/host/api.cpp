@@ -782,6 +782,8 @@ gdf_status gdf_infer_ex(gdf_ctx* ctx, const gdf_infer_args* a, void* stream) {
       (a->uniforms_dev && (reinterpret_cast<uintptr_t>(a->uniforms_dev) & 15u)) ||
       (a->dir_pdf_dev && (reinterpret_cast<uintptr_t>(a->dir_pdf_dev) & 15u)))
     return fail(GDF_ERR_INVALID_ARG, "wi, uniforms and dir_pdf must be 16-byte aligned");
+  if (reinterpret_cast<uintptr_t>(a->cdf_norm_err_dev) & 7u)
+    return fail(GDF_ERR_INVALID_ARG, "cdf_norm_err must be 8-byte aligned");
   gdf::DfKernelParams p = df_params(ctx->c);
   p.queries = a->queries_dev;
   if (a->shading) p.shading = *a->shading;
@@ -790,6 +792,7 @@ gdf_status gdf_infer_ex(gdf_ctx* ctx, const gdf_infer_args* a, void* stream) {
   p.uniforms = a->uniforms_dev;
   p.wi = a->wi_dev;
   p.dir_pdf = a->dir_pdf_dev;
+  p.norm_err = reinterpret_cast<unsigned long long*>(a->cdf_norm_err_dev);
   p.n = n;
   p.philox_seed = a->philox_seed;
   p.philox_offset = a->philox_offset;

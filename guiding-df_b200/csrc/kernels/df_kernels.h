@@ -51,6 +51,7 @@ struct DfKernelParams {
   float* dir_pdf;                    // n x 4 world direction + solid-angle pdf, nullable
   int32_t bf16;                      // inference form with bf16 MLP operands
   int32_t fp8;                       // FP8 inference form: blobs from launch_pack_fp8
+  unsigned long long* norm_err;      // FP64 CDF normalisation check (double bits, max-merged), nullable
 };
 
 struct GridFeatParams {

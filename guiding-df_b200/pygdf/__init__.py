@@ -94,7 +94,8 @@ class InferArgs(C.Structure):
     _fields_ = [("queries_dev", C.c_void_p), ("shading", C.POINTER(Shading)), ("aabb", Aabb),
                 ("guided_dev", C.c_void_p), ("uniforms_dev", C.c_void_p),
                 ("philox_seed", C.c_uint64), ("philox_offset", C.c_uint64),
-                ("wi_dev", C.c_void_p), ("dir_pdf_dev", C.c_void_p), ("n", C.c_int64)]
+                ("wi_dev", C.c_void_p), ("dir_pdf_dev", C.c_void_p), ("n", C.c_int64),
+                ("cdf_norm_err_dev", C.c_void_p)]
 
 
 def path_state(fields: dict, cur_depth) -> PathState:
@@ -361,7 +362,7 @@ class Context:
         return st
 
     def infer_ex(self, wi, n=None, queries=None, shading: "Shading | None" = None, aabb=None,
-                 guided=None, uniforms=None, seed=0, offset=0, dir_pdf=None, stream=None):
+                 guided=None, uniforms=None, seed=0, offset=0, dir_pdf=None, norm_err=None, stream=None):
         n = wi.shape[0] if n is None else n
         a = InferArgs()
         a.queries_dev = _ptr(queries)
@@ -376,6 +377,7 @@ class Context:
         a.wi_dev = _ptr(wi)
         a.dir_pdf_dev = _ptr(dir_pdf)
         a.n = n
+        a.cdf_norm_err_dev = _ptr(norm_err)
         check(lib().gdf_infer_ex(self.h, C.byref(a), _stream(stream)))
 
     def build_train_records(self, st: PathState, aabb: Aabb, px: TrainPixels, in_theta, in_phi,

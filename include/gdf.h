@@ -227,7 +227,11 @@ typedef struct gdf_shading {
  *   - dir_pdf_dev != NULL: also writes, per query, the consumer view of
  *     the result (AutoRegressive, AR.h:25-48): the unit direction
  *     squareToUniformSphere(u_theta, u_phi) (math_utils.h:226-231) and the
- *     solid-angle pdf |wi[2]| * |wi[3]| / (4 pi), as [x, y, z, pdf]. */
+ *     solid-angle pdf |wi[2]| * |wi[3]| / (4 pi), as [x, y, z, pdf];
+ *   - cdf_norm_err_dev != NULL: the CDF normalisation check, in FP64: for
+ *     every row and both distributions, |1 - sum_i p_i / N| over the N bin
+ *     pdfs the sampling uses (summed in double), max-merged into
+ *     *cdf_norm_err_dev (8-byte aligned; the caller sets it to 0 first). */
 typedef struct gdf_infer_args {
   const float* queries_dev;
   const gdf_shading* shading;
@@ -239,6 +243,7 @@ typedef struct gdf_infer_args {
   float* wi_dev;
   float* dir_pdf_dev;
   int64_t n;
+  double* cdf_norm_err_dev;
 } gdf_infer_args;
 gdf_status gdf_infer_ex(gdf_ctx* ctx, const gdf_infer_args* args, void* stream);
 

@@ -100,6 +100,37 @@ def test_infer_is_deterministic_and_writes_every_row():
     ctx.close()
 
 
+@pytest.mark.parametrize("preset", [pygdf.PRESET_SMALL, pygdf.PRESET_FULL])
+def test_cdf_normalisation_check(preset):
+    """gdf_infer_args.cdf_norm_err_dev: the FP64 normalisation check of every
+    row's theta and phi pdfs. The fp32 pdfs p_i = e_i * (N / sum e) sum to N
+    up to a few fp32 roundings of the 64-term sum (<= ~N * 2^-24 relative),
+    as do the oracle's tables (softmax x N) of the same rows. The check must
+    not change the guiding data."""
+    import torch
+    from pygdf import workload as W
+    ctx, pt, pp = make_ctx(preset, seed=4)
+    n = 6000
+    q = dev(W.queries(n, 2))
+    wi0, guided = W.wi_init(n, 2, 0.8, 0.2)
+    g = dev(guided)
+    wi_a, wi_b = dev(wi0), dev(wi0)
+    err = torch.zeros(1, dtype=torch.float64, device="cuda")
+    ctx.infer_ex(wi_a, queries=q, guided=g, seed=3, offset=9, norm_err=err)
+    ctx.infer_ex(wi_b, queries=q, guided=g, seed=3, offset=9)
+    ctx.sync()
+    e = float(err.cpu().item())
+    nb = max(ctx.cfg.n_bins_theta, ctx.cfg.n_bins_phi)
+    print("max |1 - sum p / N| over rows (theta and phi):", e)
+    assert 0.0 <= e <= 4 * nb * 2.0 ** -24
+    assert np.array_equal(wi_a.cpu().numpy(), wi_b.cpu().numpy())
+    # the oracle's tables at the kernel's thetas sum to N as well
+    d = O.df_cfg_from(ctx.cfg)
+    tt, tp = O.pdf_tables(d, pt, pp, W.queries(200, 2), wi_a.cpu().numpy()[:200, 0])
+    assert np.abs(tt.sum(1) / tt.shape[1] - 1).max() < 1e-5 and np.abs(tp.sum(1) / tp.shape[1] - 1).max() < 1e-5
+    ctx.close()
+
+
 def test_eval_pdf_matches_oracle():
     from pygdf import workload as W
     ctx, pt, pp = make_ctx(pygdf.PRESET_FULL, seed=12)
