@@ -57,8 +57,10 @@ struct gdf_group {
   uint8_t* h_stage[2] = {nullptr, nullptr};
   cudaEvent_t copied[2] = {nullptr, nullptr};
   int slot = 0;
-  __half* feat = nullptr;
+  __half* feat = nullptr;  // stream-ordered allocation (cudaMallocAsync)
   int64_t feat_tiles = 0;
+  cudaEvent_t last_launch = nullptr;  // after the group's last replay
+  bool launched = false;
   uint32_t* d_err = nullptr;
   cudaStream_t cap_stream = nullptr;
   std::vector<Plan> plans;
@@ -85,15 +87,20 @@ void drop_plans(gdf_group* g) {
   g->plans.clear();
 }
 
-gdf_status ensure_feat(gdf_group* g, int64_t tiles, int lf) {
+// Grows the feature buffer. Its only reader is the group's own last replay
+// (calls on one group are ordered), so the growth waits for that replay
+// alone and frees and allocates stream-ordered: work on other streams (a
+// server's training steps) is not waited for.
+gdf_status ensure_feat(gdf_group* g, int64_t tiles, int lf, cudaStream_t st) {
   if (tiles <= g->feat_tiles) return GDF_OK;
-  GDF_GCUDA(cudaDeviceSynchronize());  // a replaced buffer may still be read by a queued graph
+  if (g->launched) GDF_GCUDA(cudaEventSynchronize(g->last_launch));
   drop_plans(g);
-  cudaFree(g->feat);
+  if (g->feat) cudaFreeAsync(g->feat, st);
   g->feat = nullptr;
   g->feat_tiles = 0;
   const int64_t cap = tiles + tiles / 4 + 64;
-  cudaError_t e = cudaMalloc(&g->feat, static_cast<size_t>(2 * cap * 128 * lf) * sizeof(__half));
+  cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&g->feat),
+                                  static_cast<size_t>(2 * cap * 128 * lf) * sizeof(__half), st);
   if (e != cudaSuccess) {
     cudaGetLastError();
     return gfail(GDF_ERR_OOM_BUDGET, "grouped feature buffer");
@@ -261,6 +268,8 @@ gdf_status launch_plan(gdf_group* g, size_t plan, const JobSet& js, cudaStream_t
   p.feat_params.gridDim = dim3(static_cast<unsigned>(feature_blocks(js, p.fblock)));
   GDF_GCUDA(cudaGraphExecKernelNodeSetParams(p.exec, p.feat_node, &p.feat_params));
   GDF_GCUDA(cudaGraphLaunch(p.exec, st));
+  GDF_GCUDA(cudaEventRecord(g->last_launch, st));
+  g->launched = true;
   return GDF_OK;
 }
 
@@ -346,6 +355,7 @@ gdf_status gdf_group_create(int32_t max_jobs, gdf_group** out) {
     }
   }
   if (cudaStreamCreateWithFlags(&g->cap_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&g->last_launch, cudaEventDisableTiming) != cudaSuccess ||
       cudaMemset(g->d_err, 0, 4) != cudaSuccess)
     return bail(gcuda(cudaGetLastError(), "grouped set-up"));
   *out = g;
@@ -359,8 +369,9 @@ gdf_status gdf_group_destroy(gdf_group* g) {
   cudaFree(g->d_hdr);
   cudaFree(g->d_jobs);
   cudaFree(g->d_err);
-  cudaFree(g->feat);
+  if (g->feat) cudaFreeAsync(g->feat, nullptr);
   cudaFree(g->tune_wi);
+  if (g->last_launch) cudaEventDestroy(g->last_launch);
   for (int k = 0; k < 2; ++k) {
     if (g->h_stage[k]) cudaFreeHost(g->h_stage[k]);
     if (g->copied[k]) cudaEventDestroy(g->copied[k]);
@@ -378,7 +389,7 @@ gdf_status gdf_group_infer(gdf_group* g, const gdf_job* jobs, int32_t n_jobs, vo
   if (s) return s;
   if (js.total_tiles == 0) return GDF_OK;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if ((s = ensure_feat(g, js.total_tiles, js.levels * js.features))) return s;
+  if ((s = ensure_feat(g, js.total_tiles, js.levels * js.features, st))) return s;
   const auto key = std::make_tuple(js.levels, js.features, static_cast<int>(n_jobs),
                                    static_cast<int>(std::ceil(std::log2(static_cast<double>(js.total_tiles)))));
   auto it = g->tuned.find(key);

@@ -373,8 +373,10 @@ gdf_status gdf_group_destroy(gdf_group* g);
  * signature (grid shape, job count, log2 of the tile count) times the
  * candidate launch shapes (2 or 4 warpgroups per CTA x 128- or 256-thread
  * feature blocks) on scratch copies of the guiding data and keeps the
- * fastest; that call synchronises `stream`. Jobs must not share wi
- * buffers. */
+ * fastest; that call synchronises `stream`. Calls on one group are ordered
+ * (one feature buffer); a call that needs a larger buffer waits for the
+ * group's previous call to finish (only that; other streams run on). Jobs
+ * must not share wi buffers. */
 gdf_status gdf_group_infer(gdf_group* g, const gdf_job* jobs, int32_t n_jobs, void* stream);
 
 /* The launch shape chosen for the last call and the candidates' times (ms)
