@@ -262,6 +262,8 @@ void free_ws(gdf::TrainWorkspace& w) {
   cudaFree(w.sq);
   cudaFree(w.stats);
   cudaFree(w.dropped);
+  cudaFree(w.feat[0]);
+  cudaFree(w.feat[1]);
   w = gdf::TrainWorkspace{};
 }
 
@@ -325,6 +327,9 @@ gdf_status alloc_ws(Context& c) {
   if ((s = dalloc(&w.sq, 3 * static_cast<size_t>(gdf::kAdamBlocks))) || (s = dalloc(&w.stats, 2)) ||
       (s = dalloc(&w.dropped, 1)))
     return s;
+  const size_t feat = static_cast<size_t>((cap + 127) / 128 * 128) * static_cast<size_t>(c.net[0].levels) *
+                      static_cast<size_t>(c.net[0].features);
+  if ((s = dalloc(&w.feat[0], feat)) || (s = dalloc(&w.feat[1], feat))) return s;
   return GDF_OK;
 }
 
@@ -630,7 +635,7 @@ gdf_status gdf_ctx_bytes(const gdf_ctx* ctx, int64_t* bytes) {
   b += c.net[0].n_grid * 2 * 2;                               // interleaved inference grid
   b += c.feat_tiles * 128 * lf * 2 * 2;                       // inference feature tiles
   b += c.ws.capacity * 16 + 3 * static_cast<int64_t>(c.num_sms) * (c.net[0].n_mlp + c.net[1].n_mlp) +
-       3 * gdf::kAdamBlocks * 8 + 64;                         // training workspace
+       3 * gdf::kAdamBlocks * 8 + 64 + (c.ws.capacity + 127) / 128 * 128 * lf * 2 * 2;  // training workspace
   b += (c.lr_table_n[0] + c.lr_table_n[1]) * 4;
   b += c.host_cap * (9 * 4 + 1 + 4 * 4 + 4 * 4) + c.tool_cap * (9 + 2 + 4) * 4;
   b += c.pw.pixels * 2 + c.pw.df_cap * 28 * 4 + c.pw.nrc_cap * (15 + 1 + 1 + 3 + 15 + 3) * 4;
@@ -1073,6 +1078,8 @@ gdf_status gdf_train_step(gdf_ctx* ctx, const float* in_theta, const float* in_p
   p.blob_theta_bytes = c.net[0].blob_bytes;
   p.blob_phi_bytes = c.net[1].blob_bytes;
   p.bf16 = p.fp8 = 0;
+  p.feat_out_theta = c.ws.feat[0];
+  p.feat_out_phi = c.ws.feat[1];
   p.queries = in_theta;
   p.in_phi = in_phi;
   p.target = target;
@@ -1096,6 +1103,7 @@ gdf_status gdf_train_step(gdf_ctx* ctx, const float* in_theta, const float* in_p
     b.blob = nt.blob_w16;
     b.blob_bytes = nt.blob_bytes;
     b.grid = nt.w16 + nt.n_mlp;
+    b.feat = c.ws.feat[id];
     b.grid_grad = nt.grad + nt.n_mlp;
     b.wgrad_partial = c.ws.partial[id];
     b.n_mlp = nt.n_mlp;

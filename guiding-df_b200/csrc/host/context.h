@@ -53,6 +53,7 @@ struct TrainWorkspace {
   double* sq = nullptr;                   // [3 x kAdamBlocks] optimizer partials
   double* stats = nullptr;                // [2]: loss sum, squared gradient norm
   unsigned long long* dropped = nullptr;  // [1]
+  __half* feat[2] = {nullptr, nullptr};   // [capacity rounded to 128 x L*F] per DF network
 };
 
 constexpr int kAdamBlocks = 1184;  // 8 x 148 SMs

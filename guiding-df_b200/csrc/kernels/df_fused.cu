@@ -211,6 +211,17 @@ __global__ void __launch_bounds__(128 * WGS, 1) df_fused_kernel(const __grid_con
     } else {
       tile::grids_to_tiles<L, F>(p.gl_theta, p.grid_theta, p.gl_phi, p.grid_phi, q, qp, c.tile_a, KT,
                                  c.tile_p, c.row);
+      if (p.feat_out_theta != nullptr) {
+        // the row's feature chunks, as written above, for the backward
+        uint8_t* const ot = reinterpret_cast<uint8_t*>(p.feat_out_theta + t * (128 * LF));
+        uint8_t* const op = reinterpret_cast<uint8_t*>(p.feat_out_phi + t * (128 * LF));
+#pragma unroll
+        for (uint32_t kc = 0; kc < LF / 8; ++kc) {
+          const uint32_t o = tile::chunk_off(c.row, kc, LF);
+          *reinterpret_cast<uint4*>(ot + o) = *reinterpret_cast<const uint4*>(c.tile_a + tile::chunk_off(c.row, kc, KT));
+          *reinterpret_cast<uint4*>(op + o) = *reinterpret_cast<const uint4*>(c.tile_p + o);
+        }
+      }
       tile::sh_ob_to_tile(q, c.tile_a, c.row, LF, KT);
       tile::ones_to_tile(c.tile_a, c.row, LF + 28, KT, KT);
       tile::publish(c);

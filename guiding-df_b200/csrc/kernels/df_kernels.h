@@ -52,6 +52,10 @@ struct DfKernelParams {
   int32_t bf16;                      // inference form with bf16 MLP operands
   int32_t fp8;                       // FP8 inference form: blobs from launch_pack_fp8
   unsigned long long* norm_err;      // FP64 CDF normalisation check (double bits, max-merged), nullable
+  // training forward: both networks' grid features, [tiles][128 x L*F]
+  // canonical, for the backward (nullable)
+  __half* feat_out_theta;
+  __half* feat_out_phi;
 };
 
 struct GridFeatParams {

@@ -4,6 +4,8 @@
 // records per tile, persistent over tiles):
 //   1. recomputes the forward of its network with every activation kept in
 //      shared memory (tcgen05, fp32 accumulators in TMEM, fp16 activations);
+//      the grid features are the training forward's, bulk-copied per tile
+//      (the next tile's while this one finishes), not gathered again;
 //   2. builds the fp16 pdf table and dL/dlogits of combine_AR_pdf_and_dl_doutput
 //      (src/render/guided/train.h:932-965, AR.h:51-104) from the per-record
 //      pdf of the other network and the loss prefix computed by the forward
@@ -158,14 +160,23 @@ __global__ void __launch_bounds__(128, 1) df_train_bwd_kernel(const __grid_const
   const uint32_t warp = tid >> 5;
   const int H = p.hidden;
 
-  // shared memory: weights | X tile | H_1..H_H tiles | D tile | barriers
-  const uint32_t off_x = (p.blob_bytes + 127u) & ~127u;
-  constexpr uint32_t kX = 128u * K0 * 2u, kT = 128u * 64u * 2u;
-  const uint32_t off_h = off_x + kX;
+  // shared memory: weights | XF (grid features) | XR (rest of the input) |
+  // H_1..H_H tiles | D tile | barriers
+  constexpr int KR0 = K0 - LF;
+  const uint32_t off_xf = (p.blob_bytes + 127u) & ~127u;
+  constexpr uint32_t kXF = 128u * LF * 2u, kXR = 128u * KR0 * 2u, kT = 128u * 64u * 2u;
+  const uint32_t off_x = off_xf + kXF;
+  const uint32_t off_h = off_x + kXR;
   const uint32_t off_d = off_h + static_cast<uint32_t>(H) * kT;
   const uint32_t off_bar = off_d + kT;
+  // [0] weights, [1] MMA completion, [2] feature tile
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + off_bar);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + off_bar + 16);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + off_bar + 32);
+  const int64_t n_tiles = (p.n + 127) / 128;
+  auto fetch_features = [&](int64_t t) {
+    mbar_arrive_expect_tx(&bars[2], kXF);
+    bulk_g2s(smem + off_xf, p.feat + t * (128 * LF), kXF, &bars[2]);
+  };
 
   if (warp == 0) {
     tmem_alloc(tmem_slot, 512);
@@ -174,11 +185,14 @@ __global__ void __launch_bounds__(128, 1) df_train_bwd_kernel(const __grid_const
   if (tid == 0) {
     mbar_init(&bars[0], 1);
     mbar_init(&bars[1], 1);
+    mbar_init(&bars[2], 1);
     fence_mbar_init();
     mbar_arrive_expect_tx(&bars[0], p.blob_bytes);
     for (uint32_t o = 0; o < p.blob_bytes; o += 32768u)
       bulk_g2s(smem + o, reinterpret_cast<const uint8_t*>(p.blob) + o, min(32768u, p.blob_bytes - o), &bars[0]);
+    if (blockIdx.x < n_tiles) fetch_features(blockIdx.x);
   }
+  uint32_t fphase = 0;
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -198,8 +212,9 @@ __global__ void __launch_bounds__(128, 1) df_train_bwd_kernel(const __grid_const
   c.row = tid;
   c.leader = tid == 0;
   c.err = p.err;
-  uint8_t* const x_tile = smem + off_x;
+  uint8_t* const x_tile = smem + off_x;  // XR: columns LF..K0 of the input
   uint8_t* const d_tile = smem + off_d;
+  const uint32_t xf_s = smem_addr(smem + off_xf);
   const uint32_t x_s = smem_addr(x_tile), d_s = smem_addr(d_tile), h_s0 = smem_addr(smem + off_h);
   auto h_tile = [&](int l) { return smem + off_h + static_cast<uint32_t>(l - 1) * kT; };  // H_l, l >= 1
   auto h_addr = [&](int l) { return h_s0 + static_cast<uint32_t>(l - 1) * kT; };
@@ -217,10 +232,10 @@ __global__ void __launch_bounds__(128, 1) df_train_bwd_kernel(const __grid_const
   constexpr uint32_t kIdDgrad = idesc_f16(128, 64, 0, 0, 1);    // B = W^T read MN-major
   constexpr uint32_t kIdDx = idesc_f16(128, LF, 0, 0, 1);
   constexpr uint32_t kIdWg64 = idesc_f16(64, 64, 0, 1, 1);      // A, B MN-major
-  constexpr uint32_t kIdWgK0 = idesc_f16(64, K0, 0, 1, 1);
+  constexpr uint32_t kIdWgF = idesc_f16(64, LF, 0, 1, 1);
+  constexpr uint32_t kIdWgR = idesc_f16(64, KR0, 0, 1, 1);
   constexpr uint32_t kIdWgOut = idesc_f16(64, NB, 0, 1, 1);
 
-  const int64_t n_tiles = (p.n + 127) / 128;
   bool first = true;
   for (int64_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
     const int64_t row = t * 128 + c.row;
@@ -239,31 +254,30 @@ __global__ void __launch_bounds__(128, 1) df_train_bwd_kernel(const __grid_const
       u_own = 0.5f;
     }
 
-    // ---- forward: X | H_1 .. H_H | logits
-#pragma unroll 1
-    for (int l = 0; l < L; ++l) {
-      float f[F];
-      tile::grid_level<F>(p.gl, l, p.gl.interp, p.grid, q[0], q[1], q[2], f);
-#pragma unroll
-      for (int j = 0; j < F; j += 2) tile::store_h2(x_tile, c.row, l * F + j, K0, f[j], f[j + 1]);
-    }
-    tile::sh_ob_to_tile(q, x_tile, c.row, LF, K0);
+    // ---- forward: X = [XF | XR] | H_1 .. H_H | logits
+    tile::sh_ob_to_tile(q, x_tile, c.row, 0, KR0);
     if constexpr (PHI) {
       float tw[12];
       triangle_wave_encode<12>(q[9], tw);
-      tile::store_run(x_tile, c.row, LF + 28, K0, tw, 12);
-      tile::ones_to_tile(x_tile, c.row, LF + 40, K0, K0);
+      tile::store_run(x_tile, c.row, 28, KR0, tw, 12);
+      tile::ones_to_tile(x_tile, c.row, 40, KR0, KR0);
     } else {
-      tile::ones_to_tile(x_tile, c.row, LF + 28, K0, K0);
+      tile::ones_to_tile(x_tile, c.row, 28, KR0, KR0);
     }
+    mbar_wait(&bars[2], fphase, p.err, kErrMbarTimeout);
+    fphase ^= 1u;
     for (int l = 0; l <= H; ++l) {
       tile::publish(c);
       if (c.leader) {
         tc_fence_after();
-        const uint32_t a_s = l == 0 ? x_s : h_addr(l);
-        const uint32_t ka = l == 0 ? K0 : 64u;
-        mma_steps(t_work, a_s, 128, ka * 16u, 256, w_addr(l), 128, ka * 16u, 256,
-                  l == H ? kIdFwdNB : kIdFwd64, static_cast<int>(ka / 16), false);
+        if (l == 0) {
+          mma_steps(t_work, xf_s, 128, LF * 16u, 256, w_addr(0), 128, K0 * 16u, 256, kIdFwd64, LF / 16, false);
+          mma_steps(t_work, x_s, 128, KR0 * 16u, 256, w_addr(0) + (LF / 16) * 256u, 128, K0 * 16u, 256,
+                    kIdFwd64, KR0 / 16, true);
+        } else {
+          mma_steps(t_work, h_addr(l), 128, 64u * 16u, 256, w_addr(l), 128, 64u * 16u, 256,
+                    l == H ? kIdFwdNB : kIdFwd64, 4, false);
+        }
         mma_commit(c.bar);
       }
       tile::wait_mma(c);
@@ -292,9 +306,11 @@ __global__ void __launch_bounds__(128, 1) df_train_bwd_kernel(const __grid_const
           mma_steps(t_work, d_s, 128, 64u * 16u, 256, w_addr(l), 64u * 16u, 128, 2u * 64u * 16u,
                     kIdDgrad, 4, false);
         } else {
-          // G_0 (o x K0) += D^T X ; dX = D W_0[:, :LF]
-          mma_steps(t_g(0), d_s, 64u * 16u, 128, 2u * 64u * 16u, x_s, K0 * 16u, 128, 2u * K0 * 16u,
-                    kIdWgK0, 8, acc);
+          // G_0 (o x K0) += D^T X, as its XF and XR column blocks ; dX = D W_0[:, :LF]
+          mma_steps(t_g(0), d_s, 64u * 16u, 128, 2u * 64u * 16u, xf_s, LF * 16u, 128, 2u * LF * 16u,
+                    kIdWgF, 8, acc);
+          mma_steps(t_g(0) + LF, d_s, 64u * 16u, 128, 2u * 64u * 16u, x_s, KR0 * 16u, 128, 2u * KR0 * 16u,
+                    kIdWgR, 8, acc);
           mma_steps(t_dx, d_s, 128, 64u * 16u, 256, w_addr(0), K0 * 16u, 128, 2u * K0 * 16u, kIdDx, 4,
                     false);
         }
@@ -303,6 +319,8 @@ __global__ void __launch_bounds__(128, 1) df_train_bwd_kernel(const __grid_const
       tile::wait_mma(c);
       if (l > 0) dgrad_relu_to_tile(c, t_work + lane, h_tile(l), d_tile);
     }
+    // every MMA reading XF has completed: the next tile's features
+    if (c.leader && t + gridDim.x < n_tiles) fetch_features(t + gridDim.x);
     // ---- grid backward
     {
       float dx[LF];
@@ -360,6 +378,7 @@ template <int L, int F, int NB, bool LIN, bool PHI>
 cudaError_t launch_bwd_t(const DfBwdParams& p, int ctas, cudaStream_t st) {
   constexpr int LF = L * F;
   constexpr int K0 = PHI ? pad16t(LF + 40) : pad16t(LF + 28);
+  if (p.feat == nullptr) return cudaErrorInvalidValue;
   const size_t smem = ((p.blob_bytes + 127u) & ~127u) + 128u * K0 * 2u +
                       static_cast<size_t>(p.hidden + 1) * 128u * 64u * 2u + 64u;
   auto k = df_train_bwd_kernel<L, F, NB, LIN, PHI>;

@@ -20,6 +20,7 @@ struct DfBwdParams {
   const __half* blob;       // fp16 training weights, canonical layout
   uint32_t blob_bytes;
   const __half* grid;       // fp16 training grid tables
+  const __half* feat;       // [tiles][128 x L*F] canonical grid features of the training forward
   float* grid_grad;         // fp32 gradient of the grid tables (zeroed by the optimizer)
   float* wgrad_partial;     // [gridDim.x][n_mlp] per-CTA weight-gradient sums
   int64_t n_mlp;
