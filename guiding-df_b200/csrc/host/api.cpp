@@ -264,6 +264,7 @@ void free_ws(gdf::TrainWorkspace& w) {
   cudaFree(w.dropped);
   cudaFree(w.feat[0]);
   cudaFree(w.feat[1]);
+  cudaFree(w.dx);
   w = gdf::TrainWorkspace{};
 }
 
@@ -329,7 +330,10 @@ gdf_status alloc_ws(Context& c) {
     return s;
   const size_t feat = static_cast<size_t>((cap + 127) / 128 * 128) * static_cast<size_t>(c.net[0].levels) *
                       static_cast<size_t>(c.net[0].features);
-  if ((s = dalloc(&w.feat[0], feat)) || (s = dalloc(&w.feat[1], feat))) return s;
+  if ((s = dalloc(&w.feat[0], feat)) || (s = dalloc(&w.feat[1], feat)) ||
+      (s = dalloc(&w.dx, static_cast<size_t>(cap) * static_cast<size_t>(c.net[0].levels) *
+                             static_cast<size_t>(c.net[0].features))))
+    return s;
   return GDF_OK;
 }
 
@@ -635,7 +639,8 @@ gdf_status gdf_ctx_bytes(const gdf_ctx* ctx, int64_t* bytes) {
   b += c.net[0].n_grid * 2 * 2;                               // interleaved inference grid
   b += c.feat_tiles * 128 * lf * 2 * 2;                       // inference feature tiles
   b += c.ws.capacity * 16 + 3 * static_cast<int64_t>(c.num_sms) * (c.net[0].n_mlp + c.net[1].n_mlp) +
-       3 * gdf::kAdamBlocks * 8 + 64 + (c.ws.capacity + 127) / 128 * 128 * lf * 2 * 2;  // training workspace
+       3 * gdf::kAdamBlocks * 8 + 64 + (c.ws.capacity + 127) / 128 * 128 * lf * 2 * 2 +
+       c.ws.capacity * lf * 4;                                 // training workspace
   b += (c.lr_table_n[0] + c.lr_table_n[1]) * 4;
   b += c.host_cap * (9 * 4 + 1 + 4 * 4 + 4 * 4) + c.tool_cap * (9 + 2 + 4) * 4;
   b += c.pw.pixels * 2 + c.pw.df_cap * 28 * 4 + c.pw.nrc_cap * (15 + 1 + 1 + 3 + 15 + 3) * 4;
@@ -1104,6 +1109,8 @@ gdf_status gdf_train_step(gdf_ctx* ctx, const float* in_theta, const float* in_p
     b.blob_bytes = nt.blob_bytes;
     b.grid = nt.w16 + nt.n_mlp;
     b.feat = c.ws.feat[id];
+    b.dx = c.ws.dx;
+    b.dx_rows = c.ws.capacity;
     b.grid_grad = nt.grad + nt.n_mlp;
     b.wgrad_partial = c.ws.partial[id];
     b.n_mlp = nt.n_mlp;
@@ -1112,6 +1119,17 @@ gdf_status gdf_train_step(gdf_ctx* ctx, const float* in_theta, const float* in_p
     b.gl = nt.gl;
     e = gdf::launch_df_train_bwd(shape, id == 1, b, c.num_sms, st);
     if (e != cudaSuccess) return cuda_fail(e, "df_train_bwd");
+    gdf::GridScatterParams g;
+    g.in = b.in;
+    g.in_stride = b.in_stride;
+    g.fwd = c.ws.fwd;
+    g.n = n;
+    g.dx = c.ws.dx;
+    g.dx_rows = c.ws.capacity;
+    g.grid_grad = b.grid_grad;
+    g.gl = nt.gl;
+    e = gdf::launch_grid_scatter(nt.levels, nt.features, g, st);
+    if (e != cudaSuccess) return cuda_fail(e, "grid_scatter");
   }
   // 3. Adam + EMA, re-layout of the weights
   for (int id = 0; id < 2; ++id) {

@@ -54,6 +54,7 @@ struct TrainWorkspace {
   double* stats = nullptr;                // [2]: loss sum, squared gradient norm
   unsigned long long* dropped = nullptr;  // [1]
   __half* feat[2] = {nullptr, nullptr};   // [capacity rounded to 128 x L*F] per DF network
+  float* dx = nullptr;                    // [L][capacity][F] dL/dgrid-features of one network
 };
 
 constexpr int kAdamBlocks = 1184;  // 8 x 148 SMs

@@ -14,8 +14,10 @@
 //      tcgen05 MMA for the data gradient (M=128) and one for the weight
 //      gradient (M=64, operands read MN-major from the same tiles), the
 //      weight gradients accumulating across all of the CTA's tiles in TMEM;
-//   4. scatters dL/dgrid-feature * corner weight into the fp32 grid
-//      gradient with vector atomics (grid.h:395-520; tcnn uses fp16 atomics).
+//   4. writes dL/dgrid-features (level-major) for grid_scatter_kernel, which
+//      scatters them times the corner weights into the fp32 grid gradient
+//      with vector atomics at full occupancy (grid.h:395-520; tcnn uses fp16
+//      atomics).
 // At the end each CTA writes its weight-gradient partial sums; the optimizer
 // kernel reduces them in fixed CTA order (deterministic).
 //
@@ -106,49 +108,70 @@ __device__ __noinline__ void dlogits_to_tile(uint32_t taddr, float u, float pdf_
   }
 }
 
-// Grid backward of one row: dX (LF fp32 values in TMEM) scattered into the
-// fp32 gradient table (kernel_grid_backward, grid.h:395-520).
-template <int L, int F>
-__device__ __forceinline__ void grid_backward_row(const GridLevels& g, const float* pos,
-                                                  const float* dx, float* __restrict__ grad) {
+// Grid backward of one level of one row: dL/dfeatures (F fp32 values)
+// times each corner's weight scattered into the fp32 gradient table
+// (kernel_grid_backward, grid.h:395-520).
+template <int F>
+__device__ __forceinline__ void grid_backward_level(const GridLevels& g, int l, const float* pos,
+                                                    const float* dl, float* __restrict__ grad) {
+  const float scale = g.scale[l];
+  float fr[3];
+  uint32_t pg[3];
 #pragma unroll
-  for (int l = 0; l < L; ++l) {
-    const float scale = g.scale[l];
-    float fr[3];
-    uint32_t pg[3];
+  for (int d = 0; d < 3; ++d) {
+    float pp = fmaf(pos[d], scale, 0.5f);
+    const float t = floorf(pp);
+    pg[d] = static_cast<uint32_t>(static_cast<int>(t));
+    pp -= t;
+    if (g.interp == 1) pp = pp * pp * (3.0f - 2.0f * pp);
+    fr[d] = pp;
+  }
+  float* gl = grad + static_cast<size_t>(g.offset[l]) * F;
+  if (g.interp == 2) {
+    const uint32_t e = grid_entry(g, l, pg[0], pg[1], pg[2]);
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      float pp = fmaf(pos[d], scale, 0.5f);
-      const float t = floorf(pp);
-      pg[d] = static_cast<uint32_t>(static_cast<int>(t));
-      pp -= t;
-      if (g.interp == 1) pp = pp * pp * (3.0f - 2.0f * pp);
-      fr[d] = pp;
-    }
-    float* gl = grad + static_cast<size_t>(g.offset[l]) * F;
-    float dl[F];
+    for (int f = 0; f < F; ++f) atomicAdd(gl + static_cast<size_t>(e) * F + f, dl[f]);
+    return;
+  }
 #pragma unroll
-    for (int f = 0; f < F; ++f) dl[f] = dx[l * F + f];
-    if (g.interp == 2) {
-      const uint32_t e = grid_entry(g, l, pg[0], pg[1], pg[2]);
-#pragma unroll
-      for (int f = 0; f < F; ++f) atomicAdd(gl + static_cast<size_t>(e) * F + f, dl[f]);
-      continue;
-    }
-#pragma unroll
-    for (int c = 0; c < 8; ++c) {
-      float w = 1.f;
-      w *= (c & 1) ? fr[0] : 1.f - fr[0];
-      w *= (c & 2) ? fr[1] : 1.f - fr[1];
-      w *= (c & 4) ? fr[2] : 1.f - fr[2];
-      const uint32_t e = grid_entry(g, l, pg[0] + (c & 1), pg[1] + ((c >> 1) & 1), pg[2] + ((c >> 2) & 1));
-      if constexpr (F == 2) {
-        atomicAdd(reinterpret_cast<float2*>(gl) + e, make_float2(w * dl[0], w * dl[1]));
-      } else {
-        atomicAdd(reinterpret_cast<float4*>(gl) + e, make_float4(w * dl[0], w * dl[1], w * dl[2], w * dl[3]));
-      }
+  for (int c = 0; c < 8; ++c) {
+    float w = 1.f;
+    w *= (c & 1) ? fr[0] : 1.f - fr[0];
+    w *= (c & 2) ? fr[1] : 1.f - fr[1];
+    w *= (c & 4) ? fr[2] : 1.f - fr[2];
+    const uint32_t e = grid_entry(g, l, pg[0] + (c & 1), pg[1] + ((c >> 1) & 1), pg[2] + ((c >> 2) & 1));
+    if constexpr (F == 2) {
+      atomicAdd(reinterpret_cast<float2*>(gl) + e, make_float2(w * dl[0], w * dl[1]));
+    } else {
+      atomicAdd(reinterpret_cast<float4*>(gl) + e, make_float4(w * dl[0], w * dl[1], w * dl[2], w * dl[3]));
     }
   }
+}
+
+// The grid backward of a batch at full occupancy: one thread per (level,
+// record), level-major so a warp reads 32 records' dL/dfeatures of one
+// level in one 256-byte line. Records the forward rejected (prefix 0, as
+// the backward's `ok`) are skipped.
+template <int L, int F>
+__global__ void __launch_bounds__(256) grid_scatter_kernel(const __grid_constant__ GridScatterParams p) {
+  const int64_t gid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (gid >= p.n * L) return;
+  const int l = static_cast<int>(gid / p.n);
+  const int64_t row = gid - static_cast<int64_t>(l) * p.n;
+  if (__ldg(p.fwd + row * 4 + 2) == 0.f) return;
+  float pos[3], dl[F];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) pos[d] = __ldg(p.in + row * p.in_stride + d);
+  const float* src = p.dx + (static_cast<int64_t>(l) * p.dx_rows + row) * F;
+  if constexpr (F == 2) {
+    const float2 v = __ldg(reinterpret_cast<const float2*>(src));
+    dl[0] = v.x;
+    dl[1] = v.y;
+  } else {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(src));
+    dl[0] = v.x; dl[1] = v.y; dl[2] = v.z; dl[3] = v.w;
+  }
+  grid_backward_level<F>(p.gl, l, pos, dl, p.grid_grad);
 }
 
 template <int L, int F, int NB, bool LINEAR, bool PHI>
@@ -321,7 +344,7 @@ __global__ void __launch_bounds__(128, 1) df_train_bwd_kernel(const __grid_const
     }
     // every MMA reading XF has completed: the next tile's features
     if (c.leader && t + gridDim.x < n_tiles) fetch_features(t + gridDim.x);
-    // ---- grid backward
+    // ---- dL/dfeatures, level-major, for grid_scatter_kernel
     {
       float dx[LF];
       if constexpr (LF == 16) {
@@ -338,7 +361,14 @@ __global__ void __launch_bounds__(128, 1) df_train_bwd_kernel(const __grid_const
         for (int i = 0; i < 32; ++i) dx[i] = __uint_as_float(r[i]);
       }
       tc_fence_before();
-      if (ok) grid_backward_row<L, F>(p.gl, q, dx, p.grid_grad);
+      if (valid) {
+#pragma unroll
+        for (int l = 0; l < L; ++l) {
+          float* dst = p.dx + (static_cast<int64_t>(l) * p.dx_rows + row) * F;
+          if constexpr (F == 2) *reinterpret_cast<float2*>(dst) = make_float2(dx[l * F], dx[l * F + 1]);
+          else *reinterpret_cast<float4*>(dst) = make_float4(dx[l * F], dx[l * F + 1], dx[l * F + 2], dx[l * F + 3]);
+        }
+      }
     }
     first = false;
   }
@@ -573,6 +603,16 @@ cudaError_t launch_df_train_bwd(const DfShape& s, bool phi, const DfBwdParams& p
   GDF_BWD(8, 4, 16, 32)
 #undef GDF_BWD
   return cudaErrorNotSupported;
+}
+
+cudaError_t launch_grid_scatter(int levels, int features, const GridScatterParams& p, cudaStream_t st) {
+  if (p.n <= 0) return cudaSuccess;
+  const unsigned blocks = static_cast<unsigned>((p.n * levels + 255) / 256);
+  if (levels == 8 && features == 2) grid_scatter_kernel<8, 2><<<blocks, 256, 0, st>>>(p);
+  else if (levels == 16 && features == 2) grid_scatter_kernel<16, 2><<<blocks, 256, 0, st>>>(p);
+  else if (levels == 8 && features == 4) grid_scatter_kernel<8, 4><<<blocks, 256, 0, st>>>(p);
+  else return cudaErrorNotSupported;
+  return cudaGetLastError();
 }
 
 size_t df_train_bwd_smem_bytes(int levels, int features, bool phi, uint32_t blob_bytes, int hidden) {

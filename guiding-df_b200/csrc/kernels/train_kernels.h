@@ -21,11 +21,25 @@ struct DfBwdParams {
   uint32_t blob_bytes;
   const __half* grid;       // fp16 training grid tables
   const __half* feat;       // [tiles][128 x L*F] canonical grid features of the training forward
+  float* dx;                // [L][dx_rows][F] dL/dgrid-features out, level-major
+  int64_t dx_rows;
   float* grid_grad;         // fp32 gradient of the grid tables (zeroed by the optimizer)
   float* wgrad_partial;     // [gridDim.x][n_mlp] per-CTA weight-gradient sums
   int64_t n_mlp;
   int32_t hidden;           // tcnn n_hidden_layers
   uint32_t* err;
+  GridLevels gl;
+};
+
+// Grid backward of a batch (grid_scatter_kernel): dx from the backward.
+struct GridScatterParams {
+  const float* in;          // records (positions in columns 0-2), stride in_stride
+  int32_t in_stride;
+  const float* fwd;         // n x 4 from the training forward (prefix 0: rejected record)
+  int64_t n;
+  const float* dx;          // [L][dx_rows][F]
+  int64_t dx_rows;
+  float* grid_grad;
   GridLevels gl;
 };
 
@@ -60,6 +74,7 @@ struct AdamParams {
   bool blob_ema_bf16;       // the inference blob holds bf16 (bf16 inference form)
 };
 
+cudaError_t launch_grid_scatter(int levels, int features, const GridScatterParams& p, cudaStream_t st);
 cudaError_t launch_df_train_bwd(const DfShape& s, bool phi, const DfBwdParams& p, int ctas,
                                 cudaStream_t st);
 size_t df_train_bwd_smem_bytes(int levels, int features, bool phi, uint32_t blob_bytes, int hidden);
