@@ -1057,6 +1057,7 @@ static gdf::AdamParams adam_params(Context& c, int id, const gdf_adam_config& a,
   p.lr_table = c.lr_table[id < 2 ? 0 : 1];
   p.lr_table_n = c.lr_table_n[id < 2 ? 0 : 1];
   p.blob_ema_bf16 = n.infer_bf16;
+  p.err = c.d_err;
   return p;
 }
 

@@ -454,7 +454,24 @@ __global__ void adam_lr_table_kernel(float lr, float beta1, float beta2, float* 
   table[k] = lr * sqrtf(1 - powf(beta2, cs)) / (1 - powf(beta1, cs));
 }
 
-__global__ void adam_ema_kernel(const __grid_constant__ AdamParams p) {
+constexpr int kAdamTile = 1024;                     // grid parameters per staged tile
+constexpr uint32_t kAdamStage = 24u * kAdamTile;    // grad, master, m, v, step (4 B) + w16, ema (2 B)
+constexpr size_t kAdamSmem = 2u * kAdamStage + 16u;
+
+// Four EMA halves of grid parameters j..j+3 into the interleaved inference
+// table: entry e = [theta F | phi F].
+__device__ __forceinline__ void write_il(const AdamParams& p, int64_t j, uint2 e4) {
+  if (p.il_features == 2) {
+    const int64_t e = j >> 1;
+    *reinterpret_cast<uint32_t*>(p.grid_il + e * 4 + p.il_net * 2) = e4.x;
+    *reinterpret_cast<uint32_t*>(p.grid_il + (e + 1) * 4 + p.il_net * 2) = e4.y;
+  } else {
+    const int64_t e = j >> 2;
+    *reinterpret_cast<uint2*>(p.grid_il + e * 8 + p.il_net * 4) = e4;
+  }
+}
+
+__global__ void __launch_bounds__(256) adam_ema_kernel(const __grid_constant__ AdamParams p) {
   double local_sq = 0.0;
   const int64_t tid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   const int64_t nth = static_cast<int64_t>(gridDim.x) * blockDim.x;
@@ -487,12 +504,94 @@ __global__ void adam_ema_kernel(const __grid_constant__ AdamParams p) {
       p.blob_ema[off] = emah;
     }
   }
-  // grid tables: 4 parameters per thread and step, 16-byte accesses (the
-  // grid part starts at a multiple of 1024 parameters and has a multiple of
-  // 8 entries per level); the gradient is read and re-zeroed
+  // grid tables, staged: tiles of kAdamTile parameters move global ->
+  // shared by bulk copies (two stages: the next tile loads while this one
+  // is updated), 4 parameters per thread, and back by bulk stores; the
+  // gradient is re-zeroed by the threads. Needs n_mlp % 8 == 0 (16-byte
+  // aligned grid parts); the rest goes through the register path below.
+  extern __shared__ __align__(128) uint8_t stage_mem[];
+  uint64_t* sbar = reinterpret_cast<uint64_t*>(stage_mem + 2 * kAdamStage);
   const int64_t ng = p.n - p.n_mlp;
+  const int64_t n_tiles = (p.n_mlp % 8 == 0) ? ng / kAdamTile : 0;
+  if (threadIdx.x == 0) {
+    mbar_init(&sbar[0], 1);
+    mbar_init(&sbar[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  uint32_t inflight = 0u;  // thread 0: bit k = a load of stage k not yet waited for
+  auto issue_load = [&](int64_t tile, int st) {
+    uint8_t* b = stage_mem + st * kAdamStage;
+    const int64_t j = tile * kAdamTile, i = p.n_mlp + j;
+    mbar_arrive_expect_tx(&sbar[st], kAdamStage);
+    bulk_g2s(b, p.grid_grad + j, 4 * kAdamTile, &sbar[st]);
+    bulk_g2s(b + 4 * kAdamTile, p.master + i, 4 * kAdamTile, &sbar[st]);
+    bulk_g2s(b + 8 * kAdamTile, p.m + i, 4 * kAdamTile, &sbar[st]);
+    bulk_g2s(b + 12 * kAdamTile, p.v + i, 4 * kAdamTile, &sbar[st]);
+    bulk_g2s(b + 16 * kAdamTile, p.step + i, 4 * kAdamTile, &sbar[st]);
+    bulk_g2s(b + 20 * kAdamTile, p.w16 + i, 2 * kAdamTile, &sbar[st]);
+    bulk_g2s(b + 22 * kAdamTile, p.ema16 + i, 2 * kAdamTile, &sbar[st]);
+    inflight |= 1u << st;
+  };
+  uint32_t phase = 0u;  // bit k: parity of stage k's barrier
+  int st = 0;
+  if (threadIdx.x == 0 && blockIdx.x < n_tiles) issue_load(blockIdx.x, 0);
+  for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x, st ^= 1) {
+    const int64_t next = tile + gridDim.x;
+    if (threadIdx.x == 0 && next < n_tiles) {
+      bulk_wait_read();  // the other stage's stores have read it
+      issue_load(next, st ^ 1);
+    }
+    const bool ok = mbar_wait(&sbar[st], (phase >> st) & 1u, p.err, kErrMbarTimeout);
+    phase ^= 1u << st;
+    if (threadIdx.x == 0 && ok) inflight &= ~(1u << st);
+    if (__syncthreads_or(!ok)) break;
+    uint8_t* b = stage_mem + st * kAdamStage;
+    const int t = threadIdx.x;
+    const int64_t j = tile * kAdamTile + 4 * t;
+    const float4 g4 = reinterpret_cast<const float4*>(b)[t];
+    float4 w4 = reinterpret_cast<const float4*>(b + 4 * kAdamTile)[t];
+    float4 m4 = reinterpret_cast<const float4*>(b + 8 * kAdamTile)[t];
+    float4 v4 = reinterpret_cast<const float4*>(b + 12 * kAdamTile)[t];
+    uint4 s4 = reinterpret_cast<const uint4*>(b + 16 * kAdamTile)[t];
+    uint2 h4 = reinterpret_cast<const uint2*>(b + 20 * kAdamTile)[t];
+    uint2 e4 = reinterpret_cast<const uint2*>(b + 22 * kAdamTile)[t];
+    __half* hh = reinterpret_cast<__half*>(&h4);
+    __half* ee = reinterpret_cast<__half*>(&e4);
+    const float gg[4] = {g4.x, g4.y, g4.z, g4.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) adam_param(p, false, gg[k], (&w4.x)[k], (&m4.x)[k], (&v4.x)[k], (&s4.x)[k], hh[k], ee[k], local_sq);
+    reinterpret_cast<float4*>(b + 4 * kAdamTile)[t] = w4;
+    reinterpret_cast<float4*>(b + 8 * kAdamTile)[t] = m4;
+    reinterpret_cast<float4*>(b + 12 * kAdamTile)[t] = v4;
+    reinterpret_cast<uint4*>(b + 16 * kAdamTile)[t] = s4;
+    reinterpret_cast<uint2*>(b + 20 * kAdamTile)[t] = h4;
+    reinterpret_cast<uint2*>(b + 22 * kAdamTile)[t] = e4;
+    *reinterpret_cast<float4*>(p.grid_grad + j) = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (p.grid_il != nullptr) write_il(p, j, e4);
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const int64_t i = p.n_mlp + tile * kAdamTile;
+      bulk_s2g(p.master + i, b + 4 * kAdamTile, 4 * kAdamTile);
+      bulk_s2g(p.m + i, b + 8 * kAdamTile, 4 * kAdamTile);
+      bulk_s2g(p.v + i, b + 12 * kAdamTile, 4 * kAdamTile);
+      bulk_s2g(p.step + i, b + 16 * kAdamTile, 4 * kAdamTile);
+      bulk_s2g(p.w16 + i, b + 20 * kAdamTile, 2 * kAdamTile);
+      bulk_s2g(p.ema16 + i, b + 22 * kAdamTile, 2 * kAdamTile);
+      bulk_commit();
+    }
+  }
+  if (threadIdx.x == 0) {
+    // loads abandoned after a timed-out wait land before the block exits
+    for (int k = 0; k < 2; ++k)
+      if ((inflight >> k) & 1u) mbar_wait(&sbar[k], (phase >> k) & 1u, p.err, kErrMbarTimeout);
+    bulk_wait();
+  }
+  // the rest of the grid part: 4 parameters per thread and step
+  const int64_t g0 = n_tiles * kAdamTile;
   const int64_t ng4 = ng >> 2;
-  for (int64_t q = tid; q < ng4; q += nth) {
+  for (int64_t q = (g0 >> 2) + tid; q < ng4; q += nth) {
     const int64_t j = q * 4, i = p.n_mlp + j;
     const float4 g4 = *reinterpret_cast<const float4*>(p.grid_grad + j);
     *reinterpret_cast<float4*>(p.grid_grad + j) = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -505,29 +604,15 @@ __global__ void adam_ema_kernel(const __grid_constant__ AdamParams p) {
     __half* hh = reinterpret_cast<__half*>(&h4);
     __half* ee = reinterpret_cast<__half*>(&e4);
     const float gg[4] = {g4.x, g4.y, g4.z, g4.w};
-    float* ww = &w4.x;
-    float* mm = &m4.x;
-    float* vv = &v4.x;
-    uint32_t* ss = &s4.x;
 #pragma unroll
-    for (int t = 0; t < 4; ++t) adam_param(p, false, gg[t], ww[t], mm[t], vv[t], ss[t], hh[t], ee[t], local_sq);
+    for (int k = 0; k < 4; ++k) adam_param(p, false, gg[k], (&w4.x)[k], (&m4.x)[k], (&v4.x)[k], (&s4.x)[k], hh[k], ee[k], local_sq);
     *reinterpret_cast<float4*>(p.master + i) = w4;
     *reinterpret_cast<float4*>(p.m + i) = m4;
     *reinterpret_cast<float4*>(p.v + i) = v4;
     *reinterpret_cast<uint4*>(p.step + i) = s4;
     *reinterpret_cast<uint2*>(p.w16 + i) = h4;
     *reinterpret_cast<uint2*>(p.ema16 + i) = e4;
-    if (p.grid_il != nullptr) {
-      // interleaved inference copy: entry e = [theta F | phi F]
-      if (p.il_features == 2) {
-        const int64_t e = j >> 1;
-        *reinterpret_cast<uint32_t*>(p.grid_il + e * 4 + p.il_net * 2) = e4.x;
-        *reinterpret_cast<uint32_t*>(p.grid_il + (e + 1) * 4 + p.il_net * 2) = e4.y;
-      } else {
-        const int64_t e = j >> 2;
-        *reinterpret_cast<uint2*>(p.grid_il + e * 8 + p.il_net * 4) = e4;
-      }
-    }
+    if (p.grid_il != nullptr) write_il(p, j, e4);
   }
   for (int64_t j = ng4 * 4 + tid; j < ng; j += nth) {  // remainder (none for tcnn grid sizes)
     const int64_t i = p.n_mlp + j;
@@ -629,7 +714,10 @@ cudaError_t launch_adam_lr_table(float lr, float beta1, float beta2, float* tabl
 
 cudaError_t launch_adam_ema(const AdamParams& p, cudaStream_t st) {
   if (p.n <= 0) return cudaSuccess;
-  adam_ema_kernel<<<p.n_blocks, 256, 0, st>>>(p);
+  cudaError_t e = cudaFuncSetAttribute(adam_ema_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(kAdamSmem));
+  if (e != cudaSuccess) return e;
+  adam_ema_kernel<<<p.n_blocks, 256, kAdamSmem, st>>>(p);
   return cudaGetLastError();
 }
 

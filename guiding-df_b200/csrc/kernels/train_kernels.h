@@ -72,6 +72,7 @@ struct AdamParams {
   const float* lr_table;
   int32_t lr_table_n;
   bool blob_ema_bf16;       // the inference blob holds bf16 (bf16 inference form)
+  uint32_t* err;            // device error word (bounded waits of the staged grid part)
 };
 
 cudaError_t launch_grid_scatter(int levels, int features, const GridScatterParams& p, cudaStream_t st);
