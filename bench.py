@@ -597,7 +597,7 @@ def _report(args, rank, world, dist, dev, n, cfg, params, times, e2e_times, trai
                 "metric": "train samples/s", "value": nb * world / (ms_train * 1e-3),
                 "unit": "records/s", "batch": nb, "ms_per_step": ms_train,
                 "achieved_tflops": TRAIN_FLOP_PER_RECORD[args.workload] * nb / (ms_train * 1e-3) / 1e12,
-                "loss": last.loss, "launches_per_step": 8}
+                "loss": last.loss, "launches_per_step": 9}
         if rec_times:
             line["records"] = {
                 "metric": "training records/s (generate_training_data_AR)",

@@ -291,7 +291,7 @@ struct Wg {
   uint32_t row;
   bool leader;
   uint32_t* err;
-  bool bf16;           // MLP operands in bf16 (inference form); fp16 otherwise
+  bool bf16 = false;   // MLP operands in bf16 (inference form); fp16 otherwise
 };
 
 // One K segment of an MMA's A operand: `ksteps` K=16 steps read from a

@@ -1084,8 +1084,8 @@ gdf_status gdf_train_step(gdf_ctx* ctx, const float* in_theta, const float* in_p
   p.blob_theta_bytes = c.net[0].blob_bytes;
   p.blob_phi_bytes = c.net[1].blob_bytes;
   p.bf16 = p.fp8 = 0;
-  p.feat_out_theta = c.ws.feat[0];
-  p.feat_out_phi = c.ws.feat[1];
+  p.feat_theta = c.ws.feat[0];
+  p.feat_phi = c.ws.feat[1];
   p.queries = in_theta;
   p.in_phi = in_phi;
   p.target = target;
@@ -1093,7 +1093,21 @@ gdf_status gdf_train_step(gdf_ctx* ctx, const float* in_theta, const float* in_p
   p.n_dropped = c.ws.dropped;
   p.loss_scale_per_record = c.cfg.loss_scale / static_cast<float>(n);
   p.n = n;
-  cudaError_t e = gdf::launch_df_fused(shape, gdf::kModeTrainFwd, p, c.num_sms, st);
+  gdf::TrainFeatParams tf;
+  tf.in_theta = in_theta;
+  tf.in_phi = in_phi;
+  tf.target = target;
+  tf.n = n;
+  tf.n_tiles = (n + 127) / 128;
+  tf.grid_theta = p.grid_theta;
+  tf.grid_phi = p.grid_phi;
+  tf.gl_theta = c.net[0].gl;
+  tf.gl_phi = c.net[1].gl;
+  tf.feat_theta = c.ws.feat[0];
+  tf.feat_phi = c.ws.feat[1];
+  cudaError_t e = gdf::launch_train_features(shape, tf, st);
+  if (e != cudaSuccess) return cuda_fail(e, "train_features");
+  e = gdf::launch_df_fused(shape, gdf::kModeTrainFeat, p, c.num_sms, st);
   if (e != cudaSuccess) return cuda_fail(e, "df_fused (train forward)");
 
   // 2. backward of each network

@@ -68,9 +68,11 @@ __global__ void __launch_bounds__(128 * WGS, 1) df_fused_kernel(const __grid_con
   constexpr uint32_t KT = Wd::kTheta;            // theta input width
   constexpr uint32_t KR = Wd::kPhi - LF;         // phi input minus its grid part
   constexpr uint32_t KTR = KT - LF;              // theta input minus its grid part
-  // Inference and pdf evaluation read both grids' features precomputed
-  // (launch_grid_features); the training forward gathers them itself.
+  // Inference, pdf evaluation and the training step read both grids'
+  // features precomputed (launch_grid_features, launch_train_features);
+  // kModeTrainFwd gathers them itself.
   constexpr bool kFeat = MODE != kModeTrainFwd;
+  constexpr bool kTrain = MODE == kModeTrainFwd || MODE == kModeTrainFeat;
   constexpr uint32_t KA = kFeat ? DfWidths<L, F>::tile_a(KTR, KR) : DfWidths<L, F>::tile_a(KT, KR);
   static_assert(LF % 16 == 0 && KT % 16 == 0 && KR % 16 == 0 && KTR % 16 == 0,
                 "K segments must be multiples of 16");
@@ -176,7 +178,7 @@ __global__ void __launch_bounds__(128 * WGS, 1) df_fused_kernel(const __grid_con
     }
     bool record_ok = true;
     float tg[9];
-    if constexpr (MODE == kModeTrainFwd) {
+    if constexpr (kTrain) {
       // the phi network reads its own record (GuidedInputPhi, slot 9 = theta)
 #pragma unroll
       for (int i = 0; i < 10; ++i) qp[i] = valid ? __ldg(p.in_phi + row * 10 + i) : 0.5f;
@@ -211,17 +213,6 @@ __global__ void __launch_bounds__(128 * WGS, 1) df_fused_kernel(const __grid_con
     } else {
       tile::grids_to_tiles<L, F>(p.gl_theta, p.grid_theta, p.gl_phi, p.grid_phi, q, qp, c.tile_a, KT,
                                  c.tile_p, c.row);
-      if (p.feat_out_theta != nullptr) {
-        // the row's feature chunks, as written above, for the backward
-        uint8_t* const ot = reinterpret_cast<uint8_t*>(p.feat_out_theta + t * (128 * LF));
-        uint8_t* const op = reinterpret_cast<uint8_t*>(p.feat_out_phi + t * (128 * LF));
-#pragma unroll
-        for (uint32_t kc = 0; kc < LF / 8; ++kc) {
-          const uint32_t o = tile::chunk_off(c.row, kc, LF);
-          *reinterpret_cast<uint4*>(ot + o) = *reinterpret_cast<const uint4*>(c.tile_a + tile::chunk_off(c.row, kc, KT));
-          *reinterpret_cast<uint4*>(op + o) = *reinterpret_cast<const uint4*>(c.tile_p + o);
-        }
-      }
       tile::sh_ob_to_tile(q, c.tile_a, c.row, LF, KT);
       tile::ones_to_tile(c.tile_a, c.row, LF + 28, KT, KT);
       tile::publish(c);
@@ -254,7 +245,7 @@ __global__ void __launch_bounds__(128 * WGS, 1) df_fused_kernel(const __grid_con
       }
     }
     float u_theta, pdf_theta, cond;
-    if constexpr (MODE == kModeTrainFwd) {
+    if constexpr (kTrain) {
       u_theta = tg[0];
       pdf_theta = tile::row_pdf_train<NBT, LINEAR>(c.tmem + c.lane_base, tg[0]);
       cond = qp[9];
@@ -290,7 +281,7 @@ __global__ void __launch_bounds__(128 * WGS, 1) df_fused_kernel(const __grid_con
       const int64_t next = t + static_cast<int64_t>(gridDim.x) * WGS;
       if (next < n_tiles) fetch_features(next);
     }
-    if constexpr (MODE == kModeTrainFwd) {
+    if constexpr (kTrain) {
       const float pdf_phi = tile::row_pdf_train<NBP, LINEAR>(c.tmem + c.lane_base, tg[1]);
       // combine_AR_pdf_and_dl_doutput (train.h:956-963): AutoRegressive takes
       // |pdf|, pdf() = pt * pp * (1/4pi), times its inverse, + M_EPSILON
@@ -411,7 +402,7 @@ cudaError_t launch_t(int mode, const DfKernelParams& p, size_t smem, int num_sms
   int64_t ctas = (n_tiles + kDfWarpgroups - 1) / kDfWarpgroups;
   if (ctas > num_sms) ctas = num_sms;
   if (ctas < 1) ctas = 1;
-  const int fmt = mode == kModeTrainFwd ? 0 : (p.fp8 ? 2 : (p.bf16 ? 1 : 0));
+  const int fmt = (mode == kModeTrainFwd || mode == kModeTrainFeat) ? 0 : (p.fp8 ? 2 : (p.bf16 ? 1 : 0));
   auto pick = [&](auto k16, auto kb16, auto k8) { return fmt == 2 ? k8 : (fmt == 1 ? kb16 : k16); };
   auto kern = mode == kModeInfer
                   ? pick(df_fused_kernel<L, F, NBT, NBP, LIN, kModeInfer, kDfWarpgroups, 0>,
@@ -421,7 +412,8 @@ cudaError_t launch_t(int mode, const DfKernelParams& p, size_t smem, int num_sms
                   ? pick(df_fused_kernel<L, F, NBT, NBP, LIN, kModeEval, kDfWarpgroups, 0>,
                          df_fused_kernel<L, F, NBT, NBP, LIN, kModeEval, kDfWarpgroups, 1>,
                          df_fused_kernel<L, F, NBT, NBP, LIN, kModeEval, kDfWarpgroups, 2>)
-                  : df_fused_kernel<L, F, NBT, NBP, LIN, kModeTrainFwd, kDfWarpgroups, 0>;
+              : mode == kModeTrainFeat ? df_fused_kernel<L, F, NBT, NBP, LIN, kModeTrainFeat, kDfWarpgroups, 0>
+                                       : df_fused_kernel<L, F, NBT, NBP, LIN, kModeTrainFwd, kDfWarpgroups, 0>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
   if (e != cudaSuccess) return e;

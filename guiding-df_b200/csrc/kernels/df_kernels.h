@@ -15,7 +15,9 @@ namespace gdf {
 constexpr int kDfWarpgroups = 4;
 constexpr int kDfThreads = 128 * kDfWarpgroups;
 
-enum DfMode : int { kModeInfer = 0, kModeEval = 1, kModeTrainFwd = 2 };
+// kModeTrainFwd gathers the grid features in the kernel (gdf_train_loss_static);
+// kModeTrainFeat reads them from launch_train_features' tiles (the training step).
+enum DfMode : int { kModeInfer = 0, kModeEval = 1, kModeTrainFwd = 2, kModeTrainFeat = 3 };
 
 struct DfKernelParams {
   const float* queries;      // n x 9
@@ -52,10 +54,19 @@ struct DfKernelParams {
   int32_t bf16;                      // inference form with bf16 MLP operands
   int32_t fp8;                       // FP8 inference form: blobs from launch_pack_fp8
   unsigned long long* norm_err;      // FP64 CDF normalisation check (double bits, max-merged), nullable
-  // training forward: both networks' grid features, [tiles][128 x L*F]
-  // canonical, for the backward (nullable)
-  __half* feat_out_theta;
-  __half* feat_out_phi;
+};
+
+// Both networks' grid features of a training batch (launch_train_features).
+struct TrainFeatParams {
+  const float* in_theta;     // n x 9 GuidedInput
+  const float* in_phi;       // n x 10 GuidedInputPhi
+  const float* target;       // n x 9 GuidedOutput (the validity filter reads it)
+  int64_t n, n_tiles;
+  const __half* grid_theta;  // fp16 training tables
+  const __half* grid_phi;
+  GridLevels gl_theta, gl_phi;
+  __half* feat_theta;        // [n_tiles][128 x L*F] canonical
+  __half* feat_phi;
 };
 
 struct GridFeatParams {
@@ -83,6 +94,7 @@ bool df_shape_supported(const DfShape& s);
 
 // Both grids' features for inference / pdf evaluation.
 cudaError_t launch_grid_features(const DfShape& s, const GridFeatParams& p, cudaStream_t st);
+cudaError_t launch_train_features(const DfShape& s, const TrainFeatParams& p, cudaStream_t st);
 // (Re)builds the interleaved inference table from the two EMA grids.
 cudaError_t launch_interleave_grids(const __half* theta, const __half* phi, __half* il,
                                     int64_t n_entries, int features, cudaStream_t st);

@@ -64,6 +64,64 @@ __global__ void __launch_bounds__(256, 4) grid_features_kernel(const __grid_cons
   *reinterpret_cast<uint4*>(p.feat_phi + off) = make_uint4(pp[0], pp[1], pp[2], pp[3]);
 }
 
+// Both networks' grid features of a training batch from the fp16 training
+// tables (one table per network, each network at its own record's
+// position), in the tile layout the training forward and backward read;
+// same arithmetic as the training forward's own gathers
+// (tile::grids_to_tiles). Rows the forward's validity filter rejects (a NaN
+// in any field of the three records, or wi_pdf = 0; train.cu:77-81) and
+// padding rows use position 0.5, as the forward does.
+template <int L, int F>
+__global__ void __launch_bounds__(256, 4) train_features_kernel(const __grid_constant__ TrainFeatParams p) {
+  constexpr int LPC = 8 / F;
+  constexpr int NCH = L / LPC;
+  constexpr uint32_t LF = L * F;
+  const int64_t rows = p.n_tiles * 128;
+  const int64_t gid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (gid >= rows * NCH) return;
+  const int64_t row = gid % rows;
+  const int chunk = static_cast<int>(gid / rows);
+  float pt[3] = {0.5f, 0.5f, 0.5f}, pp[3] = {0.5f, 0.5f, 0.5f};
+  if (row < p.n) {
+    bool ok = true;
+    float a[3], b[3];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+      const float x = __ldg(p.in_theta + row * 9 + i), y = __ldg(p.target + row * 9 + i);
+      ok &= !isnan(x) && !isnan(y);
+      if (i < 3) a[i] = x;
+      if (i == 5) ok &= y != 0.0f;
+    }
+#pragma unroll
+    for (int i = 0; i < 10; ++i) {
+      const float x = __ldg(p.in_phi + row * 10 + i);
+      ok &= !isnan(x);
+      if (i < 3) b[i] = x;
+    }
+    if (ok) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) { pt[k] = a[k]; pp[k] = b[k]; }
+    }
+  }
+  uint32_t ot[4], op[4];
+#pragma unroll
+  for (int j = 0; j < LPC; ++j) {
+    float ft[F], fp[F];
+    const int l = chunk * LPC + j;
+    tile::grid_level<F>(p.gl_theta, l, p.gl_theta.interp, p.grid_theta, pt[0], pt[1], pt[2], ft);
+    tile::grid_level<F>(p.gl_phi, l, p.gl_phi.interp, p.grid_phi, pp[0], pp[1], pp[2], fp);
+#pragma unroll
+    for (int k = 0; k < F; k += 2) {
+      ot[(j * F + k) / 2] = tile::pack2(ft[k], ft[k + 1], false);
+      op[(j * F + k) / 2] = tile::pack2(fp[k], fp[k + 1], false);
+    }
+  }
+  const int64_t off = (row >> 7) * (128 * LF) +
+                      sm100::canon_offset(static_cast<uint32_t>(row & 127), static_cast<uint32_t>(chunk * 8), LF);
+  *reinterpret_cast<uint4*>(p.feat_theta + off) = make_uint4(ot[0], ot[1], ot[2], ot[3]);
+  *reinterpret_cast<uint4*>(p.feat_phi + off) = make_uint4(op[0], op[1], op[2], op[3]);
+}
+
 // il[e][0..F) = theta[e][..], il[e][F..2F) = phi[e][..]
 __global__ void interleave_grids_kernel(const __half* __restrict__ t, const __half* __restrict__ ph,
                                         __half* __restrict__ il, int64_t n_entries, int F) {
@@ -91,6 +149,17 @@ cudaError_t launch_grid_features(const DfShape& s, const GridFeatParams& p, cuda
   if (s.levels == 16 && s.features == 2) return launch_l<16, 2>(p, st);
   if (s.levels == 8 && s.features == 4) return launch_l<8, 4>(p, st);
   return cudaErrorNotSupported;
+}
+
+cudaError_t launch_train_features(const DfShape& s, const TrainFeatParams& p, cudaStream_t st) {
+  if (p.n_tiles <= 0) return cudaSuccess;
+  const int nch = s.levels * s.features / 8;
+  const unsigned blocks = static_cast<unsigned>((p.n_tiles * 128 * nch + 255) / 256);
+  if (s.levels == 8 && s.features == 2) train_features_kernel<8, 2><<<blocks, 256, 0, st>>>(p);
+  else if (s.levels == 16 && s.features == 2) train_features_kernel<16, 2><<<blocks, 256, 0, st>>>(p);
+  else if (s.levels == 8 && s.features == 4) train_features_kernel<8, 4><<<blocks, 256, 0, st>>>(p);
+  else return cudaErrorNotSupported;
+  return cudaGetLastError();
 }
 
 cudaError_t launch_interleave_grids(const __half* theta, const __half* phi, __half* il,

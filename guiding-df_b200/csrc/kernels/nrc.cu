@@ -85,6 +85,7 @@ __global__ void __launch_bounds__(128 * kNrcWgs, 1) nrc_query_kernel(const __gri
   c.row = tid & 127u;
   c.leader = c.row == 0;
   c.err = p.err;
+  c.bf16 = false;  // the NRC runs in fp16 (tile::issue and mlp_tail read it)
   const uint32_t w0 = smem_addr(smem);
 
   const int64_t n_tiles = (p.n + 127) / 128;
