@@ -280,6 +280,28 @@ def main():
         e.synchronize()
         if i >= args.warmup:
             e2e_times.append(s.elapsed_time(e))
+    # the box's pinned-copy bandwidth for the same byte counts: the floor of
+    # the end-to-end step (the copies, one direction at a time)
+    pcie = None
+    if e2e_times:
+        pcie = {}
+        for name, nbytes in (("h2d", q_h.nbytes + wi_h.nbytes + guided_h.nbytes), ("d2h", wi_h.nbytes)):
+            hbuf = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+            dbuf = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+            ts = []
+            for _ in range(4):
+                s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                with torch.cuda.stream(stream):
+                    s.record(stream)
+                    if name == "h2d":
+                        dbuf.copy_(hbuf, non_blocking=True)
+                    else:
+                        hbuf.copy_(dbuf, non_blocking=True)
+                    e.record(stream)
+                e.synchronize()
+                ts.append(s.elapsed_time(e))
+            pcie[name + "_gbs"] = nbytes / (min(ts[1:]) * 1e-3) / 1e9
+            del hbuf, dbuf
     # ---- training step (gdf_train_step on one batch of synthetic records)
     nb = TRAIN_BATCH[args.workload]
     train_times, rec_times, last, n_rec, rec_bytes = [], [], None, 0, 0
@@ -319,7 +341,7 @@ def main():
     ctx.sync(stream)
     _report(args, rank, world, dist, dev, n, cfg, params, times, e2e_times, train_times, rec_times,
             last, n_rec, rec_bytes, clk, nb, workload_name, threads, q_h, wi_h, guided_h, form_times,
-            grouped, serving)
+            grouped, serving, pcie)
     ctx.close()
     if dist:
         dist.destroy_process_group()
@@ -550,7 +572,7 @@ def time_records(ctx, W, n, rank, dev, stream, flush, args):
 
 def _report(args, rank, world, dist, dev, n, cfg, params, times, e2e_times, train_times, rec_times,
             last, n_rec, rec_bytes, clk, nb, workload_name, threads, q_h, wi_h, guided_h, form_times,
-            grouped, serving):
+            grouped, serving, pcie=None):
     import torch
     ms = statistics.mean(times)
     ms_e2e = statistics.mean(e2e_times) if e2e_times else float("nan")
@@ -597,7 +619,7 @@ def _report(args, rank, world, dist, dev, n, cfg, params, times, e2e_times, trai
                 "metric": "train samples/s", "value": nb * world / (ms_train * 1e-3),
                 "unit": "records/s", "batch": nb, "ms_per_step": ms_train,
                 "achieved_tflops": TRAIN_FLOP_PER_RECORD[args.workload] * nb / (ms_train * 1e-3) / 1e12,
-                "loss": last.loss, "launches_per_step": 9}
+                "loss": last.loss, "launches_per_step": 10}
         if rec_times:
             line["records"] = {
                 "metric": "training records/s (generate_training_data_AR)",
@@ -606,6 +628,13 @@ def _report(args, rank, world, dist, dev, n, cfg, params, times, e2e_times, trai
                 "achieved_gbs": rec_bytes / (ms_rec * 1e-3) / 1e9,
                 "frac_hbm": rec_bytes / (ms_rec * 1e-3) / 1e9 / peaks["hbm_gbs"],
                 "launches_per_step": 3}
+        if pcie:
+            # the copies alone, one direction after the other, at the box's
+            # pinned-copy bandwidth; the step overlaps them with each other
+            # and with the kernels, so its floor is the slower direction
+            floor = max(h2d / (pcie["h2d_gbs"] * 1e9), d2h / (pcie["d2h_gbs"] * 1e9)) * 1e3
+            line["e2e"].update({"pinned_copy_gbs": pcie, "copy_floor_ms": floor,
+                                "frac_of_copy_floor": floor / ms_e2e})
         what = {"bf16": "bf16 MLP operands (fp32 accumulation)",
                 "fp8": "e4m3 hidden matrices, per-matrix and per-row power-of-two scales (fp32 accumulation)"}
         for name, ts in form_times.items():

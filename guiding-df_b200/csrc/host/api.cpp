@@ -265,6 +265,7 @@ void free_ws(gdf::TrainWorkspace& w) {
   cudaFree(w.feat[0]);
   cudaFree(w.feat[1]);
   cudaFree(w.dx);
+  cudaFree(w.stat_part);
   w = gdf::TrainWorkspace{};
 }
 
@@ -332,7 +333,8 @@ gdf_status alloc_ws(Context& c) {
                       static_cast<size_t>(c.net[0].features);
   if ((s = dalloc(&w.feat[0], feat)) || (s = dalloc(&w.feat[1], feat)) ||
       (s = dalloc(&w.dx, static_cast<size_t>(cap) * static_cast<size_t>(c.net[0].levels) *
-                             static_cast<size_t>(c.net[0].features))))
+                             static_cast<size_t>(c.net[0].features))) ||
+      (s = dalloc(&w.stat_part, gdf::kStatBlocks)))
     return s;
   return GDF_OK;
 }
@@ -640,7 +642,7 @@ gdf_status gdf_ctx_bytes(const gdf_ctx* ctx, int64_t* bytes) {
   b += c.feat_tiles * 128 * lf * 2 * 2;                       // inference feature tiles
   b += c.ws.capacity * 16 + 3 * static_cast<int64_t>(c.num_sms) * (c.net[0].n_mlp + c.net[1].n_mlp) +
        3 * gdf::kAdamBlocks * 8 + 64 + (c.ws.capacity + 127) / 128 * 128 * lf * 2 * 2 +
-       c.ws.capacity * lf * 4;                                 // training workspace
+       c.ws.capacity * lf * 4 + gdf::kStatBlocks * 8;          // training workspace
   b += (c.lr_table_n[0] + c.lr_table_n[1]) * 4;
   b += c.host_cap * (9 * 4 + 1 + 4 * 4 + 4 * 4) + c.tool_cap * (9 + 2 + 4) * 4;
   b += c.pw.pixels * 2 + c.pw.df_cap * 28 * 4 + c.pw.nrc_cap * (15 + 1 + 1 + 3 + 15 + 3) * 4;
@@ -1157,7 +1159,7 @@ gdf_status gdf_train_step(gdf_ctx* ctx, const float* in_theta, const float* in_p
       return cuda_fail(e, "pack fp8");
   }
   // 4. FP64 loss and gradient-norm reductions
-  e = gdf::launch_train_stats(c.ws.fwd, n, c.ws.sq, 2 * gdf::kAdamBlocks, c.ws.stats, st);
+  e = gdf::launch_train_stats_mb(c.ws.fwd, n, c.ws.sq, 2 * gdf::kAdamBlocks, c.ws.stat_part, c.ws.stats, st);
   if (e != cudaSuccess) return cuda_fail(e, "train_stats");
   if (stats) {
     double h[2];
@@ -1254,7 +1256,8 @@ gdf_status gdf_nrc_train_step(gdf_ctx* ctx, const float* in, const float* target
   a.grid_grad = nullptr;
   e = gdf::launch_adam_ema(a, st);
   if (e != cudaSuccess) return cuda_fail(e, "adam_ema (nrc)");
-  e = gdf::launch_train_stats(c.ws.fwd, m, c.ws.sq + 2 * gdf::kAdamBlocks, gdf::kAdamBlocks, c.ws.stats, st);
+  e = gdf::launch_train_stats_mb(c.ws.fwd, m, c.ws.sq + 2 * gdf::kAdamBlocks, gdf::kAdamBlocks, c.ws.stat_part,
+                                 c.ws.stats, st);
   if (e != cudaSuccess) return cuda_fail(e, "train_stats (nrc)");
   if (stats) {
     double h[2];

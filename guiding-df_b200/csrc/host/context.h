@@ -55,6 +55,7 @@ struct TrainWorkspace {
   unsigned long long* dropped = nullptr;  // [1]
   __half* feat[2] = {nullptr, nullptr};   // [capacity rounded to 128 x L*F] per DF network
   float* dx = nullptr;                    // [L][capacity][F] dL/dgrid-features of one network
+  double* stat_part = nullptr;            // [kStatBlocks] per-block loss sums
 };
 
 constexpr int kAdamBlocks = 1184;  // 8 x 148 SMs

@@ -670,6 +670,46 @@ __global__ void train_stats_kernel(const float* __restrict__ fwd, int64_t n, con
   if (threadIdx.x == 0) out[1] = red[0];
 }
 
+// The same two FP64 sums over many blocks: each block sums the likelihood
+// column over one contiguous range of records (fixed order) ...
+__global__ void __launch_bounds__(512) loss_partials_kernel(const float* __restrict__ fwd, int64_t n,
+                                                            double* __restrict__ part) {
+  __shared__ double red[512];
+  const int64_t per = (n + gridDim.x - 1) / gridDim.x;
+  const int64_t b = static_cast<int64_t>(blockIdx.x) * per;
+  const int64_t e = min(n, b + per);
+  double a = 0.0;
+  for (int64_t i = b + threadIdx.x; i < e; i += blockDim.x) a += fwd[i * 4 + 3];
+  red[threadIdx.x] = a;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+// ... and one block adds the block sums and the optimizer's partials.
+__global__ void __launch_bounds__(256) stats_final_kernel(const double* __restrict__ part, int n_part,
+                                                          const double* __restrict__ sq, int n_sq,
+                                                          double* out) {
+  __shared__ double red[256];
+  for (int k = 0; k < 2; ++k) {
+    const double* v = k == 0 ? part : sq;
+    const int m = k == 0 ? n_part : n_sq;
+    double a = 0.0;
+    for (int i = threadIdx.x; i < m; i += blockDim.x) a += v[i];
+    red[threadIdx.x] = a;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+      if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) out[k] = red[0];
+    __syncthreads();
+  }
+}
+
 }  // namespace
 
 cudaError_t launch_df_train_bwd(const DfShape& s, bool phi, const DfBwdParams& p, int ctas,
@@ -724,6 +764,13 @@ cudaError_t launch_adam_ema(const AdamParams& p, cudaStream_t st) {
 cudaError_t launch_train_stats(const float* fwd, int64_t n, const double* sq, int n_sq, double* out,
                                cudaStream_t st) {
   train_stats_kernel<<<1, 1024, 0, st>>>(fwd, n, sq, n_sq, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_train_stats_mb(const float* fwd, int64_t n, const double* sq, int n_sq, double* part,
+                                  double* out, cudaStream_t st) {
+  loss_partials_kernel<<<kStatBlocks, 512, 0, st>>>(fwd, n, part);
+  stats_final_kernel<<<1, 256, 0, st>>>(part, kStatBlocks, sq, n_sq, out);
   return cudaGetLastError();
 }
 

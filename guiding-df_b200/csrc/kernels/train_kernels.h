@@ -82,6 +82,11 @@ size_t df_train_bwd_smem_bytes(int levels, int features, bool phi, uint32_t blob
 cudaError_t launch_adam_ema(const AdamParams& p, cudaStream_t st);
 cudaError_t launch_adam_lr_table(float lr, float beta1, float beta2, float* table, int32_t n,
                                  cudaStream_t st);
+// The same two sums with the loss over kStatBlocks blocks; part holds
+// kStatBlocks doubles of scratch.
+constexpr int kStatBlocks = 148;
+cudaError_t launch_train_stats_mb(const float* fwd, int64_t n, const double* sq, int n_sq, double* part,
+                                  double* out, cudaStream_t stream);
 cudaError_t launch_train_stats(const float* fwd, int64_t n, const double* sq, int n_sq, double* out,
                                cudaStream_t st);
 
