@@ -249,7 +249,7 @@ gdf_status gdf_infer_ex(gdf_ctx* ctx, const gdf_infer_args* args, void* stream);
 
 /* gdf_infer on HOST buffers, for callers whose queries live in host memory:
  * the inputs are copied in, inferred and the guiding data copied back in
- * chunks of 131,072 queries pipelined over two internal streams, so the
+ * chunks of 524,288 queries pipelined over two internal streams, so the
  * transfers overlap the kernels. Results are identical to gdf_infer on the
  * same data (the in-kernel Philox counter continues across chunks).
  *   queries_h [n x 9], guided_h [n] (nullable), uniforms_h [n x 4]
