@@ -12,8 +12,9 @@ device->host read of the guiding data. L2 is flushed (256 MiB write) between
 timed steps, outside the timed events.
 
 With --impl reference the CPU implementation of the same path runs on the
-host cores (the restated reference path) on a bounded sample
-of the workload per step.
+host cores (the oracle's restatement of the reference path: its encodings,
+an fp32 forward of the same MLPs and the reference's epilogue, on all host
+threads) on a bounded sample of the workload per step.
 
 Multi-GPU: the path has no exchange step; each rank runs an independent
 replica of the full workload (weak scaling), timed on the device, max over
