@@ -232,7 +232,9 @@ __global__ void __launch_bounds__(kScanThreads) scan_blocks_kernel(const int32_t
 // GuidedOutput 9]; NRC list A [GuidedInputNRC 15 | depth | pixel], list B
 // [GuidedInputNRC 15 | RGB 3].
 template <int KIND> struct Stage;
-template <> struct Stage<kRecordsDf> { static constexpr int A = 28, B = 0; };
+// DF: [in (9) | theta of the phi record (1) | out (9)]; the phi record is
+// words 0..9, the theta input's 9 words plus its theta
+template <> struct Stage<kRecordsDf> { static constexpr int A = 19, B = 0; };
 template <> struct Stage<kRecordsNrcTrain> { static constexpr int A = 17, B = 18; };
 template <> struct Stage<kRecordsNrcQuery> { static constexpr int A = 17, B = 0; };
 // Staged records per warp: 32 pixels average about 2.3 records each with a
@@ -308,10 +310,9 @@ __global__ void __launch_bounds__(kProduceBlock) produce_emit_kernel(const __gri
 #pragma unroll
           for (int k = 0; k < 9; ++k) {
             o[k] = __float_as_uint(in[k]);
-            o[9 + k] = __float_as_uint(in[k]);
-            o[19 + k] = __float_as_uint(out[k]);
+            o[10 + k] = __float_as_uint(out[k]);
           }
-          o[18] = __float_as_uint(pt);
+          o[9] = __float_as_uint(pt);
         } else if (base_a + ra < P.cap_a) {
           const int64_t g = base_a + ra;
 #pragma unroll
@@ -371,8 +372,8 @@ __global__ void __launch_bounds__(kProduceBlock) produce_emit_kernel(const __gri
   const int nb = wtot.y < kWarpRecords ? wtot.y : kWarpRecords;
   if constexpr (KIND == kRecordsDf) {
     warp_copy(sa, SA, 0, 9, na, base_a, P.cap_a, P.out_a0, lane);
-    warp_copy(sa, SA, 9, 10, na, base_a, P.cap_a, P.out_a1, lane);
-    warp_copy(sa, SA, 19, 9, na, base_a, P.cap_a, P.out_a2, lane);
+    warp_copy(sa, SA, 0, 10, na, base_a, P.cap_a, P.out_a1, lane);
+    warp_copy(sa, SA, 10, 9, na, base_a, P.cap_a, P.out_a2, lane);
   } else {
     warp_copy(sa, SA, 0, 15, na, base_a, P.cap_a, P.out_a0, lane);
     warp_copy_i(sa, SA, 15, na, base_a, P.cap_a, P.a_depth, lane);
