@@ -238,9 +238,11 @@ template <> struct Stage<kRecordsDf> { static constexpr int A = 19, B = 0; };
 template <> struct Stage<kRecordsNrcTrain> { static constexpr int A = 17, B = 18; };
 template <> struct Stage<kRecordsNrcQuery> { static constexpr int A = 17, B = 0; };
 // Staged records per warp: 32 pixels average about 2.3 records each with a
-// 0.7 survival per bounce, so 96 slots hold a warp's records nearly always;
-// records past slot 96 are written straight to memory.
-constexpr int kWarpRecords = 96;
+// 0.7 survival per bounce, so 80 slots hold most warps' records; records
+// past slot 80 are written straight to memory. Fewer slots than that would
+// not raise occupancy (registers then allow 9 blocks per SM, as the staging
+// does at 80); 96 slots allowed 7 (a 1080p frame: 0.71 ms, 0.64 ms at 80).
+constexpr int kWarpRecords = 80;
 
 template <int KIND>
 constexpr size_t emit_smem_bytes() {
