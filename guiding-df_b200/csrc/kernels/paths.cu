@@ -110,7 +110,7 @@ __device__ __forceinline__ void nrc_target(const gdf_record_fields& r, uint32_t 
 // finite vectors finite), so the validity tests of the producers need no
 // trigonometry: they test the stored angles.
 __device__ __forceinline__ bool angles_ok(const float* a, uint32_t p) {
-  return isfinite(a[2ull * p]) && isfinite(a[2ull * p + 1]);
+  return isfinite(a[2ull * p]) & isfinite(a[2ull * p + 1]);
 }
 
 __device__ __forceinline__ bool position_ok(const gdf_record_fields& r, uint32_t p, const rec::SceneFrame& f) {
@@ -121,26 +121,32 @@ __device__ __forceinline__ bool position_ok(const gdf_record_fields& r, uint32_t
 }
 
 // The depths of one pixel that emit a record (bits 0-4: list A, 8-12: list
-// B); the same decisions as df_record / nrc_input / nrc_target make.
+// B); the same decisions as df_record / nrc_input / nrc_target make. Every
+// visited depth's fields are read whatever its delta / miss flags, so the
+// loads of all depths go out together instead of one flag round trip
+// before each depth's fields.
 template <int KIND>
 __device__ __forceinline__ uint32_t pixel_mask(const ProduceParams& P, uint32_t p, int depth,
                                                const rec::SceneFrame& f) {
   uint32_t mask = 0;
   const int dmax = depth < GDF_MAX_TRAIN_DEPTH ? depth : GDF_MAX_TRAIN_DEPTH;
-  for (int d = 0; d < dmax; ++d) {
+#pragma unroll
+  for (int d = 0; d < GDF_MAX_TRAIN_DEPTH; ++d) {
+    if (d >= dmax) break;
     const gdf_record_fields& r = P.st.depth[d];
-    if (r.delta[p]) continue;
+    const bool skip = r.delta[p] != 0;
     if constexpr (KIND == kRecordsDf) {
       // train.cu:77-81: pos, wi, wo direction, wiPdf, L / thp * misWeight
       float L[3];
       local_radiance(r, p, L);
       const float wi_pdf = r.wi_pdf[p];
-      const bool ok = position_ok(r, p, f) && angles_ok(r.dir, p) && angles_ok(r.wo, p) &&
-                      !isnan(wi_pdf) && wi_pdf != 0.0f && !rec::any_nan(L, 3);
-      if (ok) mask |= 1u << d;
+      // & rather than &&: every term is evaluated, so no load waits on another
+      const bool ok = position_ok(r, p, f) & angles_ok(r.dir, p) & angles_ok(r.wo, p) &
+                      !isnan(wi_pdf) & (wi_pdf != 0.0f) & !rec::any_nan(L, 3);
+      if (ok && !skip) mask |= 1u << d;
     } else {
-      if (r.miss[p]) continue;
-      bool ok = position_ok(r, p, f) && angles_ok(r.wo, p);
+      bool ok = !skip & (r.miss[p] == 0);
+      ok &= position_ok(r, p, f) & angles_ok(r.wo, p);
       if constexpr (KIND == kRecordsNrcTrain) {
         float L[3];
         nrc_target(r, p, L);
@@ -228,8 +234,8 @@ __global__ void __launch_bounds__(kScanThreads) scan_blocks_kernel(const int32_t
   }
 }
 
-// Words staged per record: DF [GuidedInput 9 | GuidedInputPhi 10 |
-// GuidedOutput 9]; NRC list A [GuidedInputNRC 15 | depth | pixel], list B
+// Words staged per record: DF [GuidedInput 9 | theta 1 | GuidedOutput 9]
+// (GuidedInputPhi is the first 10); NRC list A [GuidedInputNRC 15 | depth | pixel], list B
 // [GuidedInputNRC 15 | RGB 3].
 template <int KIND> struct Stage;
 // DF: [in (9) | theta of the phi record (1) | out (9)]; the phi record is
