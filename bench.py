@@ -573,6 +573,23 @@ def time_records(ctx, W, n, rank, dev, stream, flush, args):
     return rec_times, n_rec, rec_bytes
 
 
+def max_over_ranks(values, dist, device):
+    """Each timing's maximum over all ranks: one all-reduce, which every rank
+    calls with the same number of values (a single process returns them)."""
+    if dist is None:
+        return [float(v) for v in values]
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t]
+
+
+def job_rate(units_per_rank, world, ms):
+    """Whole-job throughput: the units all ranks processed (each rank runs
+    the same replica workload) over the slowest rank's step time in ms."""
+    return units_per_rank * world / (ms * 1e-3)
+
+
 def _report(args, rank, world, dist, dev, n, cfg, params, times, e2e_times, train_times, rec_times,
             last, n_rec, rec_bytes, clk, nb, workload_name, threads, q_h, wi_h, guided_h, form_times,
             grouped, serving, pcie=None):
@@ -581,12 +598,9 @@ def _report(args, rank, world, dist, dev, n, cfg, params, times, e2e_times, trai
     ms_e2e = statistics.mean(e2e_times) if e2e_times else float("nan")
     ms_train = statistics.mean(train_times) if train_times else float("nan")
     ms_rec = statistics.mean(rec_times) if rec_times else float("nan")
-    if dist:
-        t = torch.tensor([ms, ms_e2e, ms_train, ms_rec], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, ms_e2e, ms_train, ms_rec = (float(x) for x in t)
-    value = n * world / (ms * 1e-3)
-    e2e_value = n * world / (ms_e2e * 1e-3)
+    ms, ms_e2e, ms_train, ms_rec = max_over_ranks([ms, ms_e2e, ms_train, ms_rec], dist, dev)
+    value = job_rate(n, world, ms)
+    e2e_value = job_rate(n, world, ms_e2e)
     h2d = q_h.nbytes + wi_h.nbytes + guided_h.nbytes
     d2h = wi_h.nbytes
 
@@ -619,14 +633,14 @@ def _report(args, rank, world, dist, dev, n, cfg, params, times, e2e_times, trai
         }
         if train_times:
             line["train"] = {
-                "metric": "train samples/s", "value": nb * world / (ms_train * 1e-3),
+                "metric": "train samples/s", "value": job_rate(nb, world, ms_train),
                 "unit": "records/s", "batch": nb, "ms_per_step": ms_train,
                 "achieved_tflops": TRAIN_FLOP_PER_RECORD[args.workload] * nb / (ms_train * 1e-3) / 1e12,
                 "loss": last.loss, "launches_per_step": 10}
         if rec_times:
             line["records"] = {
                 "metric": "training records/s (generate_training_data_AR)",
-                "value": n_rec * world / (ms_rec * 1e-3), "unit": "records/s",
+                "value": job_rate(n_rec, world, ms_rec), "unit": "records/s",
                 "pixels": n, "records": n_rec, "ms_per_step": ms_rec, "algorithmic_bytes": rec_bytes,
                 "achieved_gbs": rec_bytes / (ms_rec * 1e-3) / 1e9,
                 "frac_hbm": rec_bytes / (ms_rec * 1e-3) / 1e9 / peaks["hbm_gbs"],
@@ -643,7 +657,7 @@ def _report(args, rank, world, dist, dev, n, cfg, params, times, e2e_times, trai
         for name, ts in form_times.items():
             mb = statistics.mean(ts)
             line[name] = {"metric": "guided queries/s, " + what[name],
-                          "value": n * world / (mb * 1e-3), "unit": "queries/s", "ms_per_step": mb,
+                          "value": job_rate(n, world, mb), "unit": "queries/s", "ms_per_step": mb,
                           "vs_fp16": ms / mb}
         if grouped:
             line["grouped"] = grouped
