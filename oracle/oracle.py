@@ -90,6 +90,7 @@ def lib():
             ("go_softmax2_times_n", [P, C.c_int], None),
             ("go_round_f16", [C.c_double], C.c_float),
             ("go_round_e4m3", [C.c_double], C.c_double),
+            ("go_mlp_forward", [P, C.c_int, C.c_int, C.c_int, C.c_int, P, P, P], None),
             ("go_e4m3_scale_exp", [C.c_double], C.c_int),
             ("go_df_pdf_tables", [C.POINTER(DfCfg), P, P, P, P, P, P, C.c_int64], None),
             ("go_set_accumulation", [C.c_int], None),
@@ -233,6 +234,16 @@ def eval_pdf(d: DfCfg, p_theta, p_phi, queries, u, n_threads=0, storage: str = "
     out = np.empty((q.shape[0], 2), dtype=np.float32)
     with _storage(storage):
         lib().go_eval_pdf(C.byref(d), _p(pt), _p(pp), _p(q), _p(uu), _p(out), q.shape[0], n_threads)
+    return out
+
+
+def mlp_forward(w16, k0: int, width: int, n_hidden: int, n_out_pad: int, x16, storage: str = "fp16"):
+    """One row through go_mlp_forward: w16 the MLP matrices (row-major,
+    back to back), x16 the k0 encoded inputs; returns the n_out_pad logits."""
+    w, x = f32(w16), f32(x16)
+    out = np.empty(n_out_pad, dtype=np.float32)
+    with _storage(storage):
+        lib().go_mlp_forward(_p(w), k0, width, n_hidden, n_out_pad, _p(x), _p(out), None)
     return out
 
 
