@@ -90,6 +90,7 @@ def lib():
             ("go_softmax2_times_n", [P, C.c_int], None),
             ("go_round_f16", [C.c_double], C.c_float),
             ("go_round_e4m3", [C.c_double], C.c_double),
+            ("go_round_bf16", [C.c_float], C.c_float),
             ("go_mlp_forward", [P, C.c_int, C.c_int, C.c_int, C.c_int, P, P, P], None),
             ("go_e4m3_scale_exp", [C.c_double], C.c_int),
             ("go_df_pdf_tables", [C.POINTER(DfCfg), P, P, P, P, P, P, C.c_int64], None),
