@@ -84,7 +84,11 @@ __device__ __forceinline__ void cartesian_to_spherical_normalized(const float v[
   const float theta = acosf(z);
   float phi = atan2f(vn[1], vn[0]);
   if (phi < 0.0f) phi += k2Pi;
-  o[0] = theta / kPi;
+  // cartesianToSphericalNormalized divides theta by M_PI, which the C math
+  // header defines as a double before krrmath/constants.h could define its
+  // float one, so that quotient is a double rounded to float; M_2PI is
+  // krrmath's float constant.
+  o[0] = (float)((double)theta / 3.14159265358979323846);
   o[1] = phi / k2Pi;
 }
 

@@ -73,8 +73,10 @@ __device__ __forceinline__ bool df_record(const gdf_record_fields& r, uint32_t p
 #pragma unroll
   for (int c = 0; c < 3; ++c) out[2 + c] = L[c] * bv[c];
   out[5] = wi_pdf;
+  // GuidedOutput::bsdfVal stays as value-initialised (train.cu:21 never
+  // assigns it; bsdfVal enters only through L above)
 #pragma unroll
-  for (int c = 0; c < 3; ++c) out[6 + c] = bv[c];
+  for (int c = 0; c < 3; ++c) out[6 + c] = 0.0f;
   return !(rec::any_nan(in, 3) || rec::any_nan(wi, 2) || rec::any_nan(in + 3, 3) ||
            isnan(wi_pdf) || wi_pdf == 0.0f || rec::any_nan(L, 3));
 }

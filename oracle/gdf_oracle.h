@@ -162,6 +162,9 @@ void go_build_nrc_records(go_paths* s, const float aabb[6], int64_t n_train, uin
                           int64_t t_cap, int64_t* counts);
 void go_apply_nrc(go_paths* s, const float* out, const int32_t* depth, const int32_t* pixel,
                   int64_t m);
+/* AutoRegressive view of guiding records [n x 4]: out [n x 4] =
+ * (solid-angle pdf, world direction). */
+void go_autoregressive(const float* wi4, int64_t n, float* out);
 
 #ifdef __cplusplus
 }

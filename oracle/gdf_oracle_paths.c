@@ -14,6 +14,8 @@
  *   - apply_NRCoutput_to_training_data / divide_training_data_by_NRCoutput
  *     train.cu:265-308 with GuidedPixelStateBuffer::
  *     replaceIndirectRadianceSkipDelta / divideRadiance (workqueue.h:100-129)
+ *   - AutoRegressive::pdf / sample (AR.h:25-48), the consumer view of a
+ *     guiding record
  *   - normalizeSpatialCoord (train.h:272-276), warp_direction_for_sh /
  *     warp_roughness_for_ob (train.h:1243-1249), sphericalToCartesian,
  *     cartesianToSphericalNormalized, uniformSphereToSquare
@@ -96,9 +98,27 @@ void go_prepare_queries(const float* pos, const float* wo, const float* nrm, con
     const float theta = acosf(z);
     float phi = atan2f(nn[1], nn[0]);
     if (phi < 0.0f) phi += P_2PI;
-    r[6] = theta / P_PI;
+    /* math_utils.h:194: sph[0] / M_PI with the C library's double M_PI
+       (defined before krrmath/constants.h, whose float M_PI is #ifndef'd) */
+    r[6] = (float)((double)theta / 3.14159265358979323846);
     r[7] = phi / P_2PI;
     r[8] = warp_rough(rough[i]);
+  }
+}
+
+void go_autoregressive(const float* wi4, int64_t n, float* out) {
+  for (int64_t i = 0; i < n; ++i) {
+    const float* w = wi4 + i * 4;
+    /* AR.h:25-43: pdf = |pdf_theta| * |pdf_phi| * squareToUniformSpherePdf() */
+    out[i * 4] = fabsf(w[2]) * fabsf(w[3]) * 0.07957747154594766788f;
+    /* squareToUniformSphere (math_utils.h:226-231) */
+    const float z = 1.0f - 2.0f * w[0];
+    const float t = 1.0f - z * z;
+    const float r = sqrtf(t > 0.0f ? t : 0.0f);
+    const float phi = P_2PI * w[1];
+    out[i * 4 + 1] = r * cosf(phi);
+    out[i * 4 + 2] = r * sinf(phi);
+    out[i * 4 + 3] = z;
   }
 }
 
@@ -170,7 +190,9 @@ int64_t go_build_df_records(const go_paths* s, const float aabb[6], int64_t n_tr
         o[1] = wi[1];
         for (int c = 0; c < 3; ++c) o[2 + c] = L[c] * bv[c];
         o[5] = wpdf;
-        for (int c = 0; c < 3; ++c) o[6 + c] = bv[c];
+        /* GuidedOutput::bsdfVal is value-initialised and never assigned
+           (train.cu:21-81); bsdfVal enters only through L */
+        for (int c = 0; c < 3; ++c) o[6 + c] = 0.0f;
       }
       ++k;
     }

@@ -396,6 +396,14 @@ def ref_lib():
             ("ref_theta_condition16", [C.c_float], C.c_float),
             ("ref_grads_linear", [C.c_float, C.c_float, C.c_float, P, C.c_int, C.c_int, P], C.c_int),
             ("ref_combine", [P, C.c_int64, P, P, P, P, P, C.c_float], None),
+            ("ref_input_warps", [P, P, P, C.c_int64, P, P], None),
+            ("ref_autoregressive", [P, C.c_int64, P], None),
+            ("ref_generate_inference_data", [P, P, P, P, C.c_int64, P, P, P], None),
+            ("ref_generate_training_data", [C.c_void_p, P, C.c_int64, C.c_uint32, C.c_uint32, P, P, P,
+                                            C.c_int64], C.c_int64),
+            ("ref_generate_nrc_records", [C.c_void_p, P, C.c_int64, C.c_uint32, C.c_uint32, C.c_int, P, P, P,
+                                          C.c_int64, P, P, C.c_int64, P], None),
+            ("ref_apply_nrc", [C.c_void_p, P, P, P, C.c_int64], None),
         ]:
             f = getattr(L, name)
             f.argtypes = args
@@ -493,3 +501,14 @@ def apply_nrc(fields, cur_depth, out, depth, pixel):
     s = _paths(fields, cur_depth)
     o, d, p = f32(out), np.ascontiguousarray(depth, np.int32), np.ascontiguousarray(pixel, np.int32)
     L.go_apply_nrc(C.byref(s), _p(o), _p(d), _p(p), o.shape[0])
+
+
+def autoregressive(wi4) -> np.ndarray:
+    """AutoRegressive view (AR.h:25-48) of guiding records [n x 4]:
+    [n x 4] = (solid-angle pdf, world direction)."""
+    w = f32(wi4)
+    out = np.empty((w.shape[0], 4), np.float32)
+    L = lib()
+    L.go_autoregressive.argtypes = [C.c_void_p, C.c_int64, C.c_void_p]
+    L.go_autoregressive(_p(w), w.shape[0], _p(out))
+    return out

@@ -1,0 +1,524 @@
+// harness.cu -- the reference's own GPU path, run on the B200 as a checker and
+// as the speed baseline of the guiding module.
+//
+// TEST INFRASTRUCTURE ONLY: nothing in the product links or loads this file's
+// library. It is compiled by oracle/build_ref_gpu.py from the unmodified
+// reference sources, which stay where they lie in the reference tree:
+//   - tiny-cuda-nn v1.6 (src/ext/tcnn: encodings, FullyFusedMLP, CUTLASS
+//     last layers, Adam/EMA optimizers, losses, Trainer), built for sm_100a;
+//   - the reference DF kernels of src/render/guided/train.h and train.cu
+//     (generate_inference_data_AR, thetaPostInference, phiPostInference,
+//     softmaxMultFactor, combine_AR_pdf_and_dl_doutput), with AR.h;
+//   - oracle/ref_stub/ as the stand-in framework headers and
+//     oracle/ref_gpu/parameters_shadow.h as parameters.h with the bin
+//     counts of this build (GDF_REF_BINS_THETA / GDF_REF_BINS_PHI).
+// The functions below replay the call sequences of
+//   LearnedDistribution::inferenceStep (learnedDistribution.cpp:167-206),
+//   LearnedDistribution::trainStep's batch body (learnedDistribution.cpp:230-289),
+//   NRC::inferenceStep (nrc.cpp:172-181) and NRC::trainStep's batch body
+//   (nrc.cpp:136-166)
+// on caller-provided device buffers, with weights loaded through
+// Trainer::set_params_full_precision (trainer.h:238) and the per-pixel
+// sampler replaced by a scripted one: query i draws its theta uniforms from
+// uniforms[4i + 0, 1] and its phi uniforms from uniforms[4i + 2, 3].
+#include <tiny-cuda-nn/common.h>
+#include <tiny-cuda-nn/gpu_matrix.h>
+#include <tiny-cuda-nn/gpu_memory.h>
+#include <tiny-cuda-nn/loss.h>
+#include <tiny-cuda-nn/network_with_input_encoding.h>
+#include <tiny-cuda-nn/optimizer.h>
+#include <tiny-cuda-nn/trainer.h>
+
+#include <thrust/execution_policy.h>
+#include <thrust/reduce.h>
+
+#include <cstdint>
+#include <memory>
+#include <stdexcept>
+#include <string>
+
+#include "train.cu"
+
+using krr::AuxInfo;
+using krr::GuidedOutput;
+using krr::PCGSampler;
+using krr::PixelStateBuffer;
+using krr::ScatterRayQueue;
+using krr::ScatterRayWorkItem;
+using nlohmann::json;
+using tcnn::GPUMatrix;
+using tcnn::GPUMemory;
+
+namespace {
+
+// KRR_DEFAULT_RND_SEED (src/lib/src/core/config.in.h:15).
+constexpr uint32_t kReferenceSeed = 7272;
+
+thread_local std::string g_error;
+
+// LinearKernel (src/lib/src/core/device/cuda.h:79-92): one thread per
+// element, block size from the occupancy calculator.
+template <typename K, typename... Args>
+void linear_kernel(K kernel, cudaStream_t stream, int64_t n, Args... args) {
+  if (n <= 0) return;
+  int min_grid = 0, block = 0;
+  CUDA_CHECK_THROW(cudaOccupancyMaxPotentialBlockSize(&min_grid, &block, kernel, 0, 0));
+  const int64_t grid = (n + block - 1) / block;
+  kernel<<<(unsigned)grid, block, 0, stream>>>((size_t)n, args...);
+  CUDA_CHECK_THROW(cudaGetLastError());
+}
+
+// LearnedDistribution::getDistribution (learnedDistribution.h:72-82) for the
+// training layout, the template argument combine_AR_pdf_and_dl_doutput takes.
+struct LearnedDistributionView {
+  template <typename T, bool isNEE = true, bool isTrain = true>
+  KRR_CALLABLE static krr::AutoRegressive getDistribution(T* data, size_t idx, uint32_t = 0) {
+    return krr::AutoRegressive(data + idx * N_DIM_WI);
+  }
+};
+
+// --- harness kernels: queue, sampler and input plumbing around the reference
+
+__global__ void setup_queue_kernel(size_t n, ScatterRayWorkItem* items, PCGSampler* samplers, AuxInfo* aux,
+                                   const float* uniforms, const uint8_t* guided, const float* pos,
+                                   const float* wo, const float* normal, const float* rough) {
+  const size_t i = threadIdx.x + (size_t)blockIdx.x * blockDim.x;
+  if (i >= n) return;
+  ScatterRayWorkItem w;
+  w.pixelId = (unsigned)i;
+  if (pos) {
+    w.sd.pos = krr::Vector3f(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+    w.sd.wo = krr::Vector3f(wo[3 * i], wo[3 * i + 1], wo[3 * i + 2]);
+    w.sd.frame.N = krr::Vector3f(normal[3 * i], normal[3 * i + 1], normal[3 * i + 2]);
+    w.sd.roughness = rough[i];
+  }
+  items[i] = w;
+  samplers[i].seq = uniforms + 4 * i;
+  samplers[i].pos = 0;
+  aux[i].guided_pass = guided ? guided[i] != 0 : true;
+}
+
+// Theta draws are slots 0-1 of a query's uniforms, phi draws slots 2-3.
+__global__ void phi_uniforms_kernel(size_t n, PCGSampler* samplers) {
+  const size_t i = threadIdx.x + (size_t)blockIdx.x * blockDim.x;
+  if (i < n) samplers[i].pos = 2;
+}
+
+// The inputs generate_inference_data_AR writes, from prepared query rows.
+__global__ void queries_to_inputs_kernel(size_t n, const float* q, float* in_theta, float* in_phi) {
+  const size_t i = threadIdx.x + (size_t)blockIdx.x * blockDim.x;
+  if (i >= n) return;
+  for (int k = 0; k < (int)N_DIM_INPUT; ++k) {
+    const float v = q[i * N_DIM_INPUT + k];
+    in_theta[i * N_DIM_INPUT + k] = v;
+    in_phi[i * N_DIM_INPUT_PHI + k] = v;
+  }
+}
+
+struct DfState {
+  cudaStream_t stream_phi = nullptr;
+  std::shared_ptr<tcnn::Loss<precision_t>> loss;
+  std::shared_ptr<tcnn::Optimizer<precision_t>> opt_theta, opt_phi;
+  std::shared_ptr<tcnn::NetworkWithInputEncoding<precision_t>> net_theta, net_phi;
+  std::shared_ptr<tcnn::Trainer<float, precision_t, precision_t>> tr_theta, tr_phi;
+  int64_t cap = 0, cap_train = 0;
+  // inference buffers (learnedDistribution.cpp:69-83)
+  GPUMemory<float> in_theta, in_phi, out_theta, out_phi;
+  GPUMemory<ScatterRayWorkItem> items;
+  GPUMemory<PCGSampler> samplers;
+  GPUMemory<AuxInfo> aux;
+  GPUMemory<ScatterRayQueue> queue;
+  GPUMemory<PixelStateBuffer> pixel_state;
+  GPUMemory<float> zero_uniforms;
+  int64_t last_n = 0;
+  // training buffers
+  GPUMemory<precision_t> train_out_theta, train_out_phi, grad_theta, grad_phi;
+  GPUMemory<float> loss_buf;
+};
+
+struct NrcState {
+  std::shared_ptr<tcnn::Loss<precision_t>> loss;
+  std::shared_ptr<tcnn::Optimizer<precision_t>> opt;
+  std::shared_ptr<tcnn::NetworkWithInputEncoding<precision_t>> net;
+  std::shared_ptr<tcnn::Trainer<float, precision_t, precision_t>> tr;
+  GPUMemory<precision_t> train_out, grad;
+  GPUMemory<float> loss_buf;
+};
+
+template <typename F>
+int guarded(F&& f) {
+  try {
+    f();
+    return 0;
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return -1;
+  }
+}
+
+void ensure_inference_capacity(DfState& s, int64_t n) {
+  const int64_t padded = tcnn::next_multiple<int64_t>(n, 128);
+  if (padded <= s.cap) return;
+  s.cap = padded;
+  s.in_theta = GPUMemory<float>(N_DIM_INPUT * padded);
+  s.in_phi = GPUMemory<float>(N_DIM_INPUT_PHI * padded);
+  s.out_theta = GPUMemory<float>(N_DIM_OUTPUT * padded);
+  s.out_phi = GPUMemory<float>(N_DIM_OUTPUT_PHI * padded);
+  s.in_theta.memset(0);
+  s.in_phi.memset(0);
+  s.items = GPUMemory<ScatterRayWorkItem>(padded);
+  s.samplers = GPUMemory<PCGSampler>(padded);
+  s.aux = GPUMemory<AuxInfo>(padded);
+  s.zero_uniforms = GPUMemory<float>(4 * padded);
+  s.zero_uniforms.memset(0);
+}
+
+void ensure_train_capacity(DfState& s, int64_t n) {
+  if (n <= s.cap_train) return;
+  s.cap_train = n;
+  s.train_out_theta = GPUMemory<precision_t>(N_DIM_PADDED_OUTPUT * n);
+  s.train_out_phi = GPUMemory<precision_t>(N_DIM_PADDED_OUTPUT_PHI * n);
+  s.grad_theta = GPUMemory<precision_t>(N_DIM_PADDED_OUTPUT * n);
+  s.grad_phi = GPUMemory<precision_t>(N_DIM_PADDED_OUTPUT_PHI * n);
+  s.loss_buf = GPUMemory<float>(n);
+}
+
+std::shared_ptr<tcnn::Trainer<float, precision_t, precision_t>>& df_trainer(DfState& s, int net) {
+  if (net == 0) return s.tr_theta;
+  if (net == 1) return s.tr_phi;
+  throw std::runtime_error{"net must be 0 (theta) or 1 (phi)"};
+}
+
+void copy_params_out(const precision_t* src, float* dst_host, int64_t n) {
+  std::vector<precision_t> h(n);
+  CUDA_CHECK_THROW(cudaMemcpy(h.data(), src, sizeof(precision_t) * n, cudaMemcpyDeviceToHost));
+  for (int64_t i = 0; i < n; ++i) dst_host[i] = (float)h[i];
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* tref_last_error() { return g_error.c_str(); }
+
+// Bin counts this library was compiled with (N_DIM_OUTPUT, N_DIM_OUTPUT_PHI).
+void tref_bins(int32_t* theta, int32_t* phi) {
+  *theta = (int32_t)N_DIM_OUTPUT;
+  *phi = (int32_t)N_DIM_OUTPUT_PHI;
+}
+
+// LearnedDistribution::resetNetwork (learnedDistribution.cpp:64-130) from the
+// "nn" object of a DF config (base_product_df.json layout): loss, optimizer,
+// encoding / phi_encoding, network.
+int tref_df_create(const char* nn_json, void** out) {
+  return guarded([&] {
+    json config = json::parse(nn_json);
+    auto s = std::make_unique<DfState>();
+    CUDA_CHECK_THROW(cudaStreamCreate(&s->stream_phi));
+    json& theta_enc = config.contains("theta_encoding") ? config["theta_encoding"] : config["encoding"];
+    json& theta_opt = config.contains("theta_optimizer") ? config["theta_optimizer"] : config["optimizer"];
+    json& theta_net = config.contains("theta_network") ? config["theta_network"] : config["network"];
+    json& phi_enc = config.contains("phi_encoding") ? config["phi_encoding"] : config["encoding"];
+    json& phi_opt = config.contains("phi_optimizer") ? config["phi_optimizer"] : config["optimizer"];
+    json& phi_net = config.contains("phi_network") ? config["phi_network"] : config["network"];
+    s->loss.reset(tcnn::create_loss<precision_t>(config["loss"]));
+    s->opt_theta.reset(tcnn::create_optimizer<precision_t>(theta_opt));
+    s->opt_phi.reset(tcnn::create_optimizer<precision_t>(phi_opt));
+    s->net_theta = std::make_shared<tcnn::NetworkWithInputEncoding<precision_t>>(N_DIM_INPUT, N_DIM_OUTPUT,
+                                                                                   theta_enc, theta_net);
+    s->net_phi = std::make_shared<tcnn::NetworkWithInputEncoding<precision_t>>(N_DIM_INPUT_PHI, N_DIM_OUTPUT_PHI,
+                                                                                 phi_enc, phi_net);
+    s->tr_theta = std::make_shared<tcnn::Trainer<float, precision_t, precision_t>>(s->net_theta, s->opt_theta,
+                                                                                   s->loss, kReferenceSeed);
+    s->tr_phi = std::make_shared<tcnn::Trainer<float, precision_t, precision_t>>(s->net_phi, s->opt_phi,
+                                                                                 s->loss, kReferenceSeed);
+    if (s->net_theta->padded_output_width() != N_DIM_PADDED_OUTPUT ||
+        s->net_phi->padded_output_width() != N_DIM_PADDED_OUTPUT_PHI)
+      throw std::runtime_error{"padded network output width differs from the compiled bin counts"};
+    s->tr_theta->initialize_params();
+    s->tr_phi->initialize_params();
+    s->queue = GPUMemory<ScatterRayQueue>(1);
+    s->pixel_state = GPUMemory<PixelStateBuffer>(1);
+    CUDA_CHECK_THROW(cudaDeviceSynchronize());
+    *out = s.release();
+  });
+}
+
+void tref_df_destroy(void* h) {
+  auto* s = static_cast<DfState*>(h);
+  if (!s) return;
+  cudaDeviceSynchronize();
+  cudaStream_t sp = s->stream_phi;
+  delete s;
+  if (sp) cudaStreamDestroy(sp);
+}
+
+int64_t tref_df_n_params(void* h, int32_t net) {
+  auto* s = static_cast<DfState*>(h);
+  return (int64_t)(net == 0 ? s->net_theta->n_params() : s->net_phi->n_params());
+}
+
+// Encoded (padded) input width of a network: the first matrix's fan-in.
+int64_t tref_df_encoded_width(void* h, int32_t net) {
+  auto* s = static_cast<DfState*>(h);
+  return (int64_t)(net == 0 ? s->net_theta->num_encoded_dims() : s->net_phi->num_encoded_dims());
+}
+
+// Trainer::set_params_full_precision (trainer.h:238-250): fp32 master, fp16
+// training and fp16 inference (EMA) copies all set from params_host.
+int tref_df_set_params(void* h, int32_t net, const float* params_host, int64_t n) {
+  return guarded([&] { df_trainer(*static_cast<DfState*>(h), net)->set_params_full_precision(params_host, (size_t)n); });
+}
+
+int tref_df_get_params(void* h, int32_t net, float* params_host, int64_t n) {
+  return guarded([&] {
+    auto& tr = df_trainer(*static_cast<DfState*>(h), net);
+    if ((size_t)n != tr->n_params()) throw std::runtime_error{"wrong parameter count"};
+    CUDA_CHECK_THROW(cudaMemcpy(params_host, tr->params_full_precision(), sizeof(float) * n, cudaMemcpyDeviceToHost));
+  });
+}
+
+// The fp16 weights inference reads (the EMA copy, trainer.h:317-332), as fp32.
+int tref_df_get_inference_params(void* h, int32_t net, float* params_host, int64_t n) {
+  return guarded([&] {
+    auto& tr = df_trainer(*static_cast<DfState*>(h), net);
+    if ((size_t)n != tr->n_params()) throw std::runtime_error{"wrong parameter count"};
+    copy_params_out(tr->params_inference(), params_host, n);
+  });
+}
+
+// LearnedDistribution::inferenceStep (learnedDistribution.cpp:167-206).
+//   Inputs: either query rows (queries_dev [n x 9], the layout
+//   generate_inference_data_AR writes) or raw shading points (pos, wo,
+//   normal [n x 3], rough [n]) with the scene box aabb[6] = lo, hi, in which
+//   case the reference's generate_inference_data_AR builds the rows.
+//   guided_dev [n] (NULL = all guided), uniforms_dev [n x 4],
+//   wi_dev [n x 4] in/out (slots 2, 3 preset to the caller's sign).
+// Runs on `stream` (and a second stream of the harness is not used by
+// inference, as in the reference, which keeps both nets on one stream).
+int tref_df_infer(void* h, const float* queries_dev, const float* pos, const float* wo, const float* normal,
+                  const float* rough, const float* aabb, const uint8_t* guided_dev, const float* uniforms_dev,
+                  float* wi_dev, int64_t n, void* stream_ptr) {
+  return guarded([&] {
+    auto& s = *static_cast<DfState*>(h);
+    cudaStream_t stream = (cudaStream_t)stream_ptr;
+    if (n <= 0) return;
+    ensure_inference_capacity(s, n);
+    const int64_t padded = tcnn::next_multiple<int64_t>(n, 128);
+    // The queue holds n items; the padded rows of the batch are computed but
+    // neither sampled nor written (train.h:425 returns for i >= size()).
+    ScatterRayQueue q;
+    q.items_ = s.items.data();
+    q.size_ = (int)n;
+    q.cap_ = (int)padded;
+    PixelStateBuffer ps;
+    ps.sampler = s.samplers.data();
+    CUDA_CHECK_THROW(cudaMemcpyAsync(s.queue.data(), &q, sizeof(q), cudaMemcpyHostToDevice, stream));
+    CUDA_CHECK_THROW(cudaMemcpyAsync(s.pixel_state.data(), &ps, sizeof(ps), cudaMemcpyHostToDevice, stream));
+    const float* u = uniforms_dev ? uniforms_dev : s.zero_uniforms.data();
+    linear_kernel(setup_queue_kernel, stream, n, s.items.data(), s.samplers.data(), s.aux.data(), u, guided_dev,
+                  queries_dev ? nullptr : pos, wo, normal, rough);
+
+    if (queries_dev) {
+      linear_kernel(queries_to_inputs_kernel, stream, n, queries_dev, s.in_theta.data(), s.in_phi.data());
+    } else {
+      krr::AABB box;
+      box.mn = krr::Vector3f(aabb[0], aabb[1], aabb[2]);
+      box.mx = krr::Vector3f(aabb[3], aabb[4], aabb[5]);
+      // generate_inference_data_AR returns for i >= queue size itself.
+      linear_kernel(krr::generate_inference_data_AR, stream, n, s.queue.data(), (const float*)wi_dev,
+                    s.in_theta.data(), s.in_phi.data(), box);
+    }
+
+    GPUMatrix<float> inputs(s.in_theta.data(), N_DIM_INPUT, padded);
+    GPUMatrix<float> outputs(s.out_theta.data(), N_DIM_OUTPUT, padded);
+    GPUMatrix<float> inputs_phi(s.in_phi.data(), N_DIM_INPUT_PHI, padded);
+    GPUMatrix<float> outputs_phi(s.out_phi.data(), N_DIM_OUTPUT_PHI, padded);
+
+    s.net_theta->inference(stream, inputs, outputs);
+    linear_kernel(krr::thetaPostInference<float, N_DIM_OUTPUT, N_DIM_OUTPUT, N_DIM_OUTPUT>, stream, padded,
+                  outputs.data(), s.in_phi.data(), (const ScatterRayQueue*)s.queue.data(),
+                  (const PixelStateBuffer*)s.pixel_state.data(), (const AuxInfo*)s.aux.data(), wi_dev);
+    linear_kernel(phi_uniforms_kernel, stream, n, s.samplers.data());
+    s.net_phi->inference(stream, inputs_phi, outputs_phi);
+    linear_kernel(krr::phiPostInference<float, N_DIM_OUTPUT, N_DIM_OUTPUT, N_DIM_OUTPUT_PHI, N_DIM_OUTPUT_PHI,
+                                        N_DIM_OUTPUT_PHI>,
+                  stream, padded, outputs.data(), outputs_phi.data(), (const ScatterRayQueue*)s.queue.data(),
+                  (const PixelStateBuffer*)s.pixel_state.data(), (const AuxInfo*)s.aux.data(), wi_dev);
+    s.last_n = n;
+  });
+}
+
+// The per-bin pdfs (softmax x N, in place in the network outputs) of the
+// last inference call: theta [n x N_DIM_OUTPUT], phi [n x N_DIM_OUTPUT_PHI];
+// and the phi network's inputs [n x N_DIM_INPUT_PHI] (slot 9 = the theta
+// condition). Any pointer may be NULL. Synchronises.
+int tref_df_last_pdfs(void* h, float* theta_host, float* phi_host, float* in_phi_host, int64_t n) {
+  return guarded([&] {
+    auto& s = *static_cast<DfState*>(h);
+    if (n > s.last_n) throw std::runtime_error{"n exceeds the last inference call"};
+    CUDA_CHECK_THROW(cudaDeviceSynchronize());
+    if (theta_host)
+      CUDA_CHECK_THROW(cudaMemcpy(theta_host, s.out_theta.data(), sizeof(float) * N_DIM_OUTPUT * n, cudaMemcpyDeviceToHost));
+    if (phi_host)
+      CUDA_CHECK_THROW(cudaMemcpy(phi_host, s.out_phi.data(), sizeof(float) * N_DIM_OUTPUT_PHI * n, cudaMemcpyDeviceToHost));
+    if (in_phi_host)
+      CUDA_CHECK_THROW(cudaMemcpy(in_phi_host, s.in_phi.data(), sizeof(float) * N_DIM_INPUT_PHI * n, cudaMemcpyDeviceToHost));
+  });
+}
+
+// One batch of LearnedDistribution::trainStep (learnedDistribution.cpp:
+// 230-289): theta forward on `stream` and phi forward on the harness's second
+// stream, softmaxMultFactor (fp16 pdfs), combine_AR_pdf_and_dl_doutput,
+// backward + optimizer step of each net on its stream, loss reduction.
+//   in_theta_dev [n x 9], in_phi_dev [n x 10], target_dev [n x 9]
+//   (GuidedOutput); n a multiple of 128 (the reference rounds down).
+//   loss_host: the batch's mean loss (learnedDistribution.cpp:288).
+//   grad_*_host (nullable): the parameter gradients of this batch (fp16, x
+//   the loss scale, tcnn's param_gradients) widened to fp32; when both are
+//   NULL and do_step != 0 the optimizer steps as in the reference.
+// Synchronises (the reference synchronises the device three times per batch).
+int tref_df_train_step(void* h, const float* in_theta_dev, const float* in_phi_dev, const float* target_dev,
+                       int64_t n, int32_t do_step, float* loss_host, float* grad_theta_host, float* grad_phi_host,
+                       float* loss_per_record_host, void* stream_ptr) {
+  return guarded([&] {
+    auto& s = *static_cast<DfState*>(h);
+    cudaStream_t stream = (cudaStream_t)stream_ptr;
+    cudaStream_t stream_phi = s.stream_phi;
+    if (n <= 0 || n % 128 != 0) throw std::runtime_error{"batch size must be a positive multiple of 128"};
+    ensure_train_capacity(s, n);
+    GPUMatrix<float> inputs((float*)in_theta_dev, N_DIM_INPUT, n);
+    GPUMatrix<float> inputs_phi((float*)in_phi_dev, N_DIM_INPUT_PHI, n);
+    GPUMatrix<precision_t> outputs(s.train_out_theta.data(), N_DIM_PADDED_OUTPUT, n);
+    GPUMatrix<precision_t> outputs_phi(s.train_out_phi.data(), N_DIM_PADDED_OUTPUT_PHI, n);
+    GPUMatrix<precision_t> dl_theta(s.grad_theta.data(), N_DIM_PADDED_OUTPUT, n);
+    GPUMatrix<precision_t> dl_phi(s.grad_phi.data(), N_DIM_PADDED_OUTPUT_PHI, n);
+
+    // The phi stream starts after the caller's prior work on `stream`.
+    cudaEvent_t ev;
+    CUDA_CHECK_THROW(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    CUDA_CHECK_THROW(cudaEventRecord(ev, stream));
+    CUDA_CHECK_THROW(cudaStreamWaitEvent(stream_phi, ev, 0));
+
+    auto ctx_theta = s.net_theta->forward(stream, inputs, &outputs, false, false);
+    linear_kernel(krr::softmaxMultFactor<precision_t, N_DIM_OUTPUT, N_DIM_PADDED_OUTPUT, N_DIM_OUTPUT>, stream, n,
+                  outputs.data());
+    auto ctx_phi = s.net_phi->forward(stream_phi, inputs_phi, &outputs_phi, false, false);
+    linear_kernel(krr::softmaxMultFactor<precision_t, N_DIM_OUTPUT_PHI, N_DIM_PADDED_OUTPUT_PHI, N_DIM_OUTPUT_PHI>,
+                  stream_phi, n, outputs_phi.data());
+    CUDA_CHECK_THROW(cudaDeviceSynchronize());
+    linear_kernel(krr::combine_AR_pdf_and_dl_doutput<LearnedDistributionView>, stream, n,
+                  (GuidedOutput*)target_dev, outputs.data(), outputs_phi.data(), dl_theta.data(), dl_phi.data(),
+                  s.loss_buf.data(), TRAIN_LOSS_SCALE);
+    CUDA_CHECK_THROW(cudaDeviceSynchronize());
+    s.net_theta->backward(stream, *ctx_theta, inputs, outputs, dl_theta, nullptr, false,
+                          tcnn::EGradientMode::Overwrite);
+    s.net_phi->backward(stream_phi, *ctx_phi, inputs_phi, outputs_phi, dl_phi, nullptr, false,
+                        tcnn::EGradientMode::Overwrite);
+    if (grad_theta_host || grad_phi_host) {
+      CUDA_CHECK_THROW(cudaDeviceSynchronize());
+      if (grad_theta_host) copy_params_out(s.tr_theta->param_gradients(), grad_theta_host, s.tr_theta->n_params());
+      if (grad_phi_host) copy_params_out(s.tr_phi->param_gradients(), grad_phi_host, s.tr_phi->n_params());
+    }
+    if (do_step) {
+      s.tr_theta->optimizer_step(stream, TRAIN_LOSS_SCALE);
+      s.tr_phi->optimizer_step(stream_phi, TRAIN_LOSS_SCALE);
+    }
+    const float sum = thrust::reduce(thrust::cuda::par.on(stream), s.loss_buf.data(), s.loss_buf.data() + n, 0.f,
+                                     thrust::plus<float>());
+    if (loss_host) *loss_host = sum / (float)n;
+    if (loss_per_record_host)
+      CUDA_CHECK_THROW(cudaMemcpy(loss_per_record_host, s.loss_buf.data(), sizeof(float) * n, cudaMemcpyDeviceToHost));
+    CUDA_CHECK_THROW(cudaDeviceSynchronize());
+    CUDA_CHECK_THROW(cudaEventDestroy(ev));
+  });
+}
+
+// NRC::resetNetwork (nrc.cpp:35-56) from the "nn" object of
+// base_hashgrid_nrc_df.json.
+int tref_nrc_create(const char* nn_json, void** out) {
+  return guarded([&] {
+    json config = json::parse(nn_json);
+    auto s = std::make_unique<NrcState>();
+    s->opt.reset(tcnn::create_optimizer<precision_t>(config["optimizer"]));
+    s->loss.reset(tcnn::create_loss<precision_t>(config["loss"]));
+    s->net = std::make_shared<tcnn::NetworkWithInputEncoding<precision_t>>(N_DIM_INPUT_NRC, N_DIM_OUTPUT_NRC,
+                                                                            config["encoding"], config["network"]);
+    s->tr = std::make_shared<tcnn::Trainer<float, precision_t, precision_t>>(s->net, s->opt, s->loss,
+                                                                            kReferenceSeed);
+    if (s->net->padded_output_width() != N_DIM_PADDED_OUTPUT_NRC)
+      throw std::runtime_error{"NRC padded output width is not 16"};
+    s->tr->initialize_params();
+    CUDA_CHECK_THROW(cudaDeviceSynchronize());
+    *out = s.release();
+  });
+}
+
+void tref_nrc_destroy(void* h) {
+  cudaDeviceSynchronize();
+  delete static_cast<NrcState*>(h);
+}
+
+int64_t tref_nrc_n_params(void* h) { return (int64_t) static_cast<NrcState*>(h)->net->n_params(); }
+
+int tref_nrc_set_params(void* h, const float* params_host, int64_t n) {
+  return guarded([&] { static_cast<NrcState*>(h)->tr->set_params_full_precision(params_host, (size_t)n); });
+}
+
+int tref_nrc_get_params(void* h, float* params_host, int64_t n) {
+  return guarded([&] {
+    auto& tr = static_cast<NrcState*>(h)->tr;
+    if ((size_t)n != tr->n_params()) throw std::runtime_error{"wrong parameter count"};
+    CUDA_CHECK_THROW(cudaMemcpy(params_host, tr->params_full_precision(), sizeof(float) * n, cudaMemcpyDeviceToHost));
+  });
+}
+
+// NRC::inferenceStep (nrc.cpp:172-181): in_dev [m x 15] -> out_dev [m x 3];
+// m must be a multiple of 128 (the reference pads its buffers to 128).
+int tref_nrc_query(void* h, const float* in_dev, float* out_dev, int64_t m, void* stream_ptr) {
+  return guarded([&] {
+    auto& s = *static_cast<NrcState*>(h);
+    if (m <= 0 || m % 128 != 0) throw std::runtime_error{"query count must be a positive multiple of 128"};
+    GPUMatrix<float> inputs((float*)in_dev, N_DIM_INPUT_NRC, m);
+    GPUMatrix<float> outputs(out_dev, N_DIM_OUTPUT_NRC, m);
+    s.net->inference((cudaStream_t)stream_ptr, inputs, outputs);
+  });
+}
+
+// One batch of NRC::trainStep (nrc.cpp:136-166): forward, RelativeL2Luminance
+// loss with TRAIN_LOSS_SCALE_NRC, backward, optimizer step, loss reduction.
+// in_dev [m x 15], target_dev [m x 3], m a multiple of 128. grad_host
+// (nullable) receives the parameter gradients (fp16 x loss scale, widened).
+int tref_nrc_train_step(void* h, const float* in_dev, const float* target_dev, int64_t m, int32_t do_step,
+                        float* loss_host, float* grad_host, void* stream_ptr) {
+  return guarded([&] {
+    auto& s = *static_cast<NrcState*>(h);
+    cudaStream_t stream = (cudaStream_t)stream_ptr;
+    if (m <= 0 || m % 128 != 0) throw std::runtime_error{"batch size must be a positive multiple of 128"};
+    if ((int64_t)(s.train_out.size() / N_DIM_PADDED_OUTPUT_NRC) < m) {
+      s.train_out = GPUMemory<precision_t>(N_DIM_PADDED_OUTPUT_NRC * m);
+      s.grad = GPUMemory<precision_t>(N_DIM_PADDED_OUTPUT_NRC * m);
+      s.loss_buf = GPUMemory<float>(N_DIM_PADDED_OUTPUT_NRC * m);
+    }
+    GPUMatrix<float> inputs((float*)in_dev, N_DIM_INPUT_NRC, m);
+    GPUMatrix<float> targets((float*)target_dev, N_DIM_OUTPUT_NRC, m);
+    GPUMatrix<precision_t> outputs(s.train_out.data(), N_DIM_PADDED_OUTPUT_NRC, m);
+    GPUMatrix<precision_t> dl(s.grad.data(), N_DIM_PADDED_OUTPUT_NRC, m);
+    GPUMatrix<float> L(s.loss_buf.data(), N_DIM_PADDED_OUTPUT_NRC, m);
+    auto ctx = s.net->forward(stream, inputs, &outputs, false, false);
+    s.loss->evaluate(stream, N_DIM_PADDED_OUTPUT_NRC, N_DIM_OUTPUT_NRC, TRAIN_LOSS_SCALE_NRC, outputs, targets, L, dl,
+                     nullptr);
+    s.net->backward(stream, *ctx, inputs, outputs, dl, nullptr, false, tcnn::EGradientMode::Overwrite);
+    if (grad_host) {
+      CUDA_CHECK_THROW(cudaStreamSynchronize(stream));
+      copy_params_out(s.tr->param_gradients(), grad_host, s.tr->n_params());
+    }
+    if (do_step) s.tr->optimizer_step(stream, TRAIN_LOSS_SCALE_NRC);
+    const float sum = thrust::reduce(thrust::cuda::par.on(stream), L.data(), L.data() + L.n_elements(), 0.f,
+                                     thrust::plus<float>());
+    if (loss_host) *loss_host = sum / (float)m;
+    CUDA_CHECK_THROW(cudaStreamSynchronize(stream));
+  });
+}
+
+}  // extern "C"

@@ -1,4 +1,5 @@
-// Stand-in for render/shared.h: shading data and BSDF sample records.
+// Stand-in for render/shared.h: shading data, BSDF sample records and the
+// per-pixel sampler.
 #pragma once
 #include "../common.h"
 namespace krr {
@@ -10,20 +11,22 @@ struct ShadingData {
   Frame frame;
   float roughness = 0.f;
   Vector3f diffuse, specular;
-  bool isTwoSided() const { return true; }
-  unsigned getBsdfType() const { return BSDF_SMOOTH; }
+  KRR_STUB_HD bool isTwoSided() const { return true; }
+  KRR_STUB_HD unsigned getBsdfType() const { return BSDF_SMOOTH; }
 };
 struct BSDFSample { Vector3f wi; float pdf = 0.f; };
 struct PCGSampler {
-  // the reference's sampler returns its next uniform; here a fixed script
+  // The reference's PCG sampler returns its next uniform (sampler.h:77-86);
+  // here each pixel's sampler walks a scripted sequence of uniforms, so both
+  // sides of a comparison consume identical random numbers.
   const float* seq = nullptr;
   int pos = 0;
-  float get1D() { return seq[pos++]; }
+  KRR_STUB_HD float get1D() { return seq[pos++]; }
 };
 class Sampler {
  public:
-  Sampler(PCGSampler* s) : s_(s) {}
-  float get1D() { return s_->get1D(); }
+  KRR_STUB_HD Sampler(PCGSampler* s) : s_(s) {}
+  KRR_STUB_HD float get1D() { return s_->get1D(); }
  private:
   PCGSampler* s_;
 };
