@@ -104,6 +104,19 @@ __global__ void phi_uniforms_kernel(size_t n, PCGSampler* samplers) {
   if (i < n) samplers[i].pos = 2;
 }
 
+// Rows n..padded of the harness's guiding-data buffer: the reference's
+// post-inference kernels run over the 128-padded batch and read u_theta /
+// u_phi of every row to index the pdf tables, so those rows hold in-range
+// values (its own buffer keeps the previous bounce's there).
+__global__ void pad_rows_kernel(size_t n_pad, float* wi_pad_rows) {
+  const size_t i = threadIdx.x + (size_t)blockIdx.x * blockDim.x;
+  if (i >= n_pad) return;
+  wi_pad_rows[4 * i] = 0.5f;
+  wi_pad_rows[4 * i + 1] = 0.5f;
+  wi_pad_rows[4 * i + 2] = 1.f;
+  wi_pad_rows[4 * i + 3] = 1.f;
+}
+
 // The inputs generate_inference_data_AR writes, from prepared query rows.
 __global__ void queries_to_inputs_kernel(size_t n, const float* q, float* in_theta, float* in_phi) {
   const size_t i = threadIdx.x + (size_t)blockIdx.x * blockDim.x;
@@ -123,7 +136,7 @@ struct DfState {
   std::shared_ptr<tcnn::Trainer<float, precision_t, precision_t>> tr_theta, tr_phi;
   int64_t cap = 0, cap_train = 0;
   // inference buffers (learnedDistribution.cpp:69-83)
-  GPUMemory<float> in_theta, in_phi, out_theta, out_phi;
+  GPUMemory<float> in_theta, in_phi, out_theta, out_phi, wi;
   GPUMemory<ScatterRayWorkItem> items;
   GPUMemory<PCGSampler> samplers;
   GPUMemory<AuxInfo> aux;
@@ -164,6 +177,7 @@ void ensure_inference_capacity(DfState& s, int64_t n) {
   s.in_phi = GPUMemory<float>(N_DIM_INPUT_PHI * padded);
   s.out_theta = GPUMemory<float>(N_DIM_OUTPUT * padded);
   s.out_phi = GPUMemory<float>(N_DIM_OUTPUT_PHI * padded);
+  s.wi = GPUMemory<float>(N_DIM_WI * padded);
   s.in_theta.memset(0);
   s.in_phi.memset(0);
   s.items = GPUMemory<ScatterRayWorkItem>(padded);
@@ -315,6 +329,11 @@ int tref_df_infer(void* h, const float* queries_dev, const float* pos, const flo
     ps.sampler = s.samplers.data();
     CUDA_CHECK_THROW(cudaMemcpyAsync(s.queue.data(), &q, sizeof(q), cudaMemcpyHostToDevice, stream));
     CUDA_CHECK_THROW(cudaMemcpyAsync(s.pixel_state.data(), &ps, sizeof(ps), cudaMemcpyHostToDevice, stream));
+    // The kernels below run over the padded batch and write guiding data
+    // for every row of it: they work on the harness's padded copy.
+    float* wi = s.wi.data();
+    CUDA_CHECK_THROW(cudaMemcpyAsync(wi, wi_dev, sizeof(float) * N_DIM_WI * n, cudaMemcpyDeviceToDevice, stream));
+    linear_kernel(pad_rows_kernel, stream, padded - n, wi + N_DIM_WI * n);
     const float* u = uniforms_dev ? uniforms_dev : s.zero_uniforms.data();
     linear_kernel(setup_queue_kernel, stream, n, s.items.data(), s.samplers.data(), s.aux.data(), u, guided_dev,
                   queries_dev ? nullptr : pos, wo, normal, rough);
@@ -326,7 +345,7 @@ int tref_df_infer(void* h, const float* queries_dev, const float* pos, const flo
       box.mn = krr::Vector3f(aabb[0], aabb[1], aabb[2]);
       box.mx = krr::Vector3f(aabb[3], aabb[4], aabb[5]);
       // generate_inference_data_AR returns for i >= queue size itself.
-      linear_kernel(krr::generate_inference_data_AR, stream, n, s.queue.data(), (const float*)wi_dev,
+      linear_kernel(krr::generate_inference_data_AR, stream, n, s.queue.data(), (const float*)wi,
                     s.in_theta.data(), s.in_phi.data(), box);
     }
 
@@ -338,13 +357,14 @@ int tref_df_infer(void* h, const float* queries_dev, const float* pos, const flo
     s.net_theta->inference(stream, inputs, outputs);
     linear_kernel(krr::thetaPostInference<float, N_DIM_OUTPUT, N_DIM_OUTPUT, N_DIM_OUTPUT>, stream, padded,
                   outputs.data(), s.in_phi.data(), (const ScatterRayQueue*)s.queue.data(),
-                  (const PixelStateBuffer*)s.pixel_state.data(), (const AuxInfo*)s.aux.data(), wi_dev);
+                  (const PixelStateBuffer*)s.pixel_state.data(), (const AuxInfo*)s.aux.data(), wi);
     linear_kernel(phi_uniforms_kernel, stream, n, s.samplers.data());
     s.net_phi->inference(stream, inputs_phi, outputs_phi);
     linear_kernel(krr::phiPostInference<float, N_DIM_OUTPUT, N_DIM_OUTPUT, N_DIM_OUTPUT_PHI, N_DIM_OUTPUT_PHI,
                                         N_DIM_OUTPUT_PHI>,
                   stream, padded, outputs.data(), outputs_phi.data(), (const ScatterRayQueue*)s.queue.data(),
-                  (const PixelStateBuffer*)s.pixel_state.data(), (const AuxInfo*)s.aux.data(), wi_dev);
+                  (const PixelStateBuffer*)s.pixel_state.data(), (const AuxInfo*)s.aux.data(), wi);
+    CUDA_CHECK_THROW(cudaMemcpyAsync(wi_dev, wi, sizeof(float) * N_DIM_WI * n, cudaMemcpyDeviceToDevice, stream));
     s.last_n = n;
   });
 }
