@@ -515,6 +515,11 @@ static void mlp_forward_f32(const float* w16, int k0, int width, int n_hidden, i
   }
 }
 
+void go_mlp_forward_f32(const float* w16, int k0, int width, int n_hidden, int n_out,
+                        const float* x16, float* out) {
+  mlp_forward_f32(w16, k0, width, n_hidden, n_out, x16, out);
+}
+
 /* ------------------------------------------------------ DF epilogue */
 
 /* softmax2 (src/render/guided/train.h:845-862) followed by the x N factor of

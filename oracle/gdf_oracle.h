@@ -92,6 +92,9 @@ void go_mlp_forward(const float* w16, int k0, int width, int n_hidden, int n_out
                     const float* x16, float* out, float* hidden_out /* nullable, n_hidden x width */);
 
 void go_set_accumulation(int acc32);
+/* The same forward in plain fp32 (sequential sums), the CPU baseline's MLP. */
+void go_mlp_forward_f32(const float* w16, int k0, int width, int n_hidden, int n_out,
+                        const float* x16, float* out);
 
 /* ---- DF epilogue, reference float semantics ---- */
 void go_softmax2_times_n(float* v, int n);

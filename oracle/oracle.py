@@ -503,6 +503,35 @@ def apply_nrc(fields, cur_depth, out, depth, pixel):
     L.go_apply_nrc(C.byref(s), _p(o), _p(d), _p(p), o.shape[0])
 
 
+_refcpu = {}
+
+
+def refcpu_available(bins_theta: int, bins_phi: int) -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", f"libgdf_refcpu_{bins_theta}x{bins_phi}.so"))
+
+
+def refcpu_infer(d: DfCfg, p_theta16, p_phi16, queries, wi, guided=None, uniforms=None, n_threads=0):
+    """The CPU baseline: the reference's thetaPostInference / phiPostInference
+    compiled for the host (oracle/ref_cpu.cpp) after the oracle's fp32
+    encodings + MLP forward. Returns the guiding data [n x 4]."""
+    key = (d.n_bins_theta, d.n_bins_phi)
+    if key not in _refcpu:
+        path = os.path.join(HERE, "_ref", f"libgdf_refcpu_{key[0]}x{key[1]}.so")
+        L = C.CDLL(path)
+        L.refcpu_infer.argtypes = [C.c_void_p, P, P, P, P, P, P, C.c_int64, C.c_int]
+        L.refcpu_infer.restype = C.c_int
+        _refcpu[key] = L
+    q = f32(queries)
+    out = f32(wi).copy()
+    g = None if guided is None else np.ascontiguousarray(guided, np.uint8)
+    u = f32(uniforms)
+    rc = _refcpu[key].refcpu_infer(C.byref(d), _p(f32(p_theta16)), _p(f32(p_phi16)), _p(q), _p(g), _p(u),
+                                   _p(out), q.shape[0], n_threads)
+    if rc != 0:
+        raise ValueError("refcpu_infer: configuration differs from the library's bin counts")
+    return out
+
+
 def autoregressive(wi4) -> np.ndarray:
     """AutoRegressive view (AR.h:25-48) of guiding records [n x 4]:
     [n x 4] = (solid-angle pdf, world direction)."""

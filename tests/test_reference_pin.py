@@ -268,3 +268,25 @@ def test_nrc_substitution_bit_exact():
     O.apply_nrc(f_or, d_or, out, r["q_depth"], r["q_pixel"])
     assert not np.array_equal(f_ref["L"], fields["L"])
     assert np.array_equal(f_ref["L"].view(np.uint32), f_or["L"].view(np.uint32))
+
+
+@pytest.mark.parametrize("preset", [0, 1])
+def test_cpu_baseline_equals_oracle_fp32_path(preset):
+    """The CPU baseline bench.py times (oracle/ref_cpu.cpp: the reference's
+    thetaPostInference / phiPostInference compiled for the host after the
+    oracle's fp32 encodings and MLP forward) gives the oracle fp32 path's
+    guiding data bit for bit."""
+    import pygdf
+    from gdf_testutil import gen_weights
+    cfg = pygdf.default_config(preset)
+    d = O.df_cfg_from(cfg)
+    if not O.refcpu_available(cfg.n_bins_theta, cfg.n_bins_phi):
+        pytest.skip("CPU baseline library not built")
+    pt, pp = O.round_f16(gen_weights(cfg, 0, 3)), O.round_f16(gen_weights(cfg, 1, 4))
+    n = 3000
+    q = W.queries(n, 1)
+    wi, g = W.wi_init(n, 1, 0.8, 0.2)
+    u = W.uniforms(n, 1)
+    a = O.refcpu_infer(d, pt, pp, q, wi, g, u, 4)
+    b = O.infer_fp32(d, pt, pp, q, wi, g, u, 4)
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
