@@ -11,10 +11,16 @@ host->device copy of the queries, guided mask and guiding data and the
 device->host read of the guiding data. L2 is flushed (256 MiB write) between
 timed steps, outside the timed events.
 
-With --impl reference the CPU implementation of the same path runs on the
-host cores (the oracle's restatement of the reference path: its encodings,
-an fp32 forward of the same MLPs and the reference's epilogue, on all host
-threads) on a bounded sample of the workload per step.
+With --impl reference the CPU implementation of the same path runs on all
+host cores, one whole bounce per step, with the same weights and query rows:
+the reference's own interpolation and sampling code (train.h
+thetaPostInference / phiPostInference, compiled for the host from the
+reference tree) after a scalar fp32 forward of the same encodings and MLPs.
+
+The side object `reference_gpu` times the reference's own GPU path --
+tiny-cuda-nn v1.6 plus the reference DF kernels, rebuilt from the reference
+tree for sm_100a (oracle/build_ref_gpu.py) -- on the same bounce and the same
+training batch with the same weights, and the ratios of this library to it.
 
 Multi-GPU: the path has no exchange step; each rank runs an independent
 replica of the full workload (weak scaling), timed on the device, max over
@@ -113,52 +119,110 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sms)}
 
 
-def mlp_params(cfg, net: int) -> int:
-    """MLP parameters of a DF network in tcnn order: first layer 64 x k0
-    (encoded width padded to 16), hidden 64 x 64, output padded to 16 rows."""
+def mlp_dims(cfg, net: int) -> list[tuple[int, int]]:
+    """(rows, cols) of each MLP matrix of a DF network in tcnn order: first
+    layer 64 x k0 (encoded width padded to 16), hidden 64 x 64, output rows
+    padded to 16."""
     lf = cfg.grid_theta.n_levels * cfg.grid_theta.n_features_per_level
     k0 = (lf + 28 + (12 if net == 1 else 0) + 15) // 16 * 16
     h = cfg.mlp_theta.n_hidden_layers if net == 0 else cfg.mlp_phi.n_hidden_layers
     bins = cfg.n_bins_theta if net == 0 else cfg.n_bins_phi
-    return 64 * k0 + (h - 1) * 64 * 64 + (bins + 15) // 16 * 16 * 64
+    return [(64, k0)] + [(64, 64)] * (h - 1) + [((bins + 15) // 16 * 16, 64)]
+
+
+def bench_weights(cfg, net: int, n_params: int, seed: int) -> np.ndarray:
+    """The benchmark's network weights, from numpy only so that every arm
+    (this library, the reference GPU path, the CPU baseline) runs the same
+    ones: Xavier-uniform MLP matrices x 2.5 (peaked distributions, so the
+    sampling does real work) and grid tables U(-0.5, 0.5)."""
+    rng = np.random.default_rng(seed * 2 + net)
+    parts = []
+    for r, c in mlp_dims(cfg, net):
+        a = 2.5 * np.sqrt(6.0 / (r + c))
+        parts.append(rng.uniform(-a, a, r * c))
+    n_mlp = sum(r * c for r, c in mlp_dims(cfg, net))
+    parts.append(rng.uniform(-0.5, 0.5, n_params - n_mlp))
+    return np.concatenate(parts).astype(np.float32)
+
+
+def workload_config(workload: str):
+    """The networks of a workload as plain values (what the CPU arm needs,
+    without loading this library): hash grids with tcnn's default base
+    resolution 16 and per-level scale 2, SH degree 4, OneBlob 4 bins,
+    TriangleWave 12 frequencies, linear pdf interpolation."""
+    from types import SimpleNamespace as NS
+    full = workload == "full"
+    grid = NS(type=0, n_levels=16 if full else 8, n_features_per_level=2, log2_hashmap_size=19 if full else 16,
+              base_resolution=16, per_level_scale=2.0, interpolation=0)
+    mlp = NS(n_neurons=64, n_hidden_layers=4 if full else 3)
+    bins = 64 if full else 32
+    return NS(n_bins_theta=bins, n_bins_phi=bins, pdf_interp=0, grid_theta=grid, grid_phi=grid, sh_degree=4,
+              oneblob_bins=4, tw_frequencies=12, mlp_theta=mlp, mlp_phi=mlp)
+
+
+def bench_config(workload: str, precision: int = 0):
+    """The library's preset for the workload, checked against workload_config."""
+    import pygdf
+    cfg = pygdf.default_config(pygdf.PRESET_FULL if workload == "full" else pygdf.PRESET_SMALL)
+    cfg.precision = precision
+    ref = workload_config(workload)
+    for k in ("n_bins_theta", "n_bins_phi", "pdf_interp", "sh_degree", "oneblob_bins", "tw_frequencies"):
+        assert getattr(cfg, k) == getattr(ref, k), k
+    for g in ("grid_theta", "grid_phi"):
+        for k in vars(ref.grid_theta):
+            assert abs(getattr(getattr(cfg, g), k) - getattr(ref.grid_theta, k)) < 1e-6, (g, k)
+    for m in ("mlp_theta", "mlp_phi"):
+        for k in vars(ref.mlp_theta):
+            assert getattr(getattr(cfg, m), k) == getattr(ref.mlp_theta, k), (m, k)
+    return cfg
 
 
 def make_context(workload: str, seed: int, precision: int = 0):
     import pygdf
-    preset = pygdf.PRESET_FULL if workload == "full" else pygdf.PRESET_SMALL
-    cfg = pygdf.default_config(preset)
-    cfg.precision = precision
+    cfg = bench_config(workload, precision)
     ctx = pygdf.Context(cfg)
-    rng = np.random.default_rng(seed)
     params = []
     for net in (0, 1):
-        p = ctx.get_params(net)
-        n_mlp = mlp_params(cfg, net)
-        p[:n_mlp] *= 2.5
-        p[n_mlp:] = rng.uniform(-0.5, 0.5, p.size - n_mlp).astype(np.float32)
+        p = bench_weights(cfg, net, ctx.n_params(net), seed)
         ctx.set_params(net, p)
         params.append(p)
     return ctx, cfg, params
 
 
-def cpu_reference(workload: str, cfg, params, seconds: float, threads: int):
-    """Times the CPU restatement (fp32 forward + reference epilogue) on the host."""
-    import oracle as O
+def cpu_inputs(n: int, seed: int):
+    """Query rows, guiding data, guided mask and uniforms of a bounce."""
     from pygdf import workload as W
+    q = W.queries(n, seed)
+    wi, guided = W.wi_init(n, seed, guided_frac=0.7, one_sided_frac=0.1)
+    u = W.uniforms(n, seed)
+    return q, wi, guided, u
+
+
+def cpu_reference(cfg, params, inputs, threads: int):
+    """The CPU baseline on one batch of queries: the reference's
+    thetaPostInference / phiPostInference compiled for the host
+    (oracle/_ref/libgdf_refcpu_*.so) after a scalar fp32 forward of the same
+    encodings and MLPs. Returns (queries/s, queries, seconds)."""
+    import oracle as O
     d = O.df_cfg_from(cfg)
     p16 = [O.round_f16(p) for p in params]
-    chunk = 16384
-    q = W.queries(chunk, 99)
-    wi, guided = W.wi_init(chunk, 99, 1.0, 0.0)
-    u = W.uniforms(chunk, 99)
-    O.infer_fp32(d, p16[0], p16[1], q[:256], wi[:256], guided[:256], u[:256], threads)  # warm
-    done, t0 = 0, time.perf_counter()
-    while True:
-        O.infer_fp32(d, p16[0], p16[1], q, wi, guided, u, threads)
-        done += chunk
-        el = time.perf_counter() - t0
-        if el >= seconds:
-            break
+    q, wi, guided, u = inputs
+    t0 = time.perf_counter()
+    O.refcpu_infer(d, p16[0], p16[1], q, wi, guided, u, threads)
+    el = time.perf_counter() - t0
+    return q.shape[0] / el, q.shape[0], el
+
+
+def cpu_sample(cfg, params, seconds: float, threads: int, chunk: int = 131072):
+    """A bounded sample (about `seconds` of CPU work) of the CPU baseline on
+    the bounce's first `chunk` queries, repeated."""
+    inputs = cpu_inputs(chunk, 42)
+    cpu_reference(cfg, params, tuple(x[:1024] for x in inputs), threads)  # warm
+    done, el = 0, 0.0
+    while el < seconds:
+        _, k, t = cpu_reference(cfg, params, inputs, threads)
+        done += k
+        el += t
     return done / el, done, el
 
 
@@ -172,7 +236,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="CPU-baseline sample length; 0 skips it (profiling runs)")
     ap.add_argument("--skip-e2e", action="store_true", help="profiling runs: kernel timing only")
-    ap.add_argument("--stages", default="infer,train,records,forms,grouped,serve",
+    ap.add_argument("--stages", default="infer,train,refgpu,records,forms,grouped,serve",
                     help="comma list of infer, train, records (profiling runs select one)")
     args = ap.parse_args()
     stages = set(args.stages.split(","))
@@ -188,28 +252,30 @@ def main():
     threads = os.cpu_count() or 1
 
     if args.impl == "reference":
+        # The reference's own CPU implementation of the path: its epilogue
+        # (train.h) compiled for the host after a scalar fp32 forward of the
+        # same networks, on every host thread; each step is one whole bounce
+        # with this arm's weights and inputs.
         if rank != 0:
             return
-        import pygdf
-        cfg = pygdf.default_config(pygdf.PRESET_FULL if args.workload == "full" else pygdf.PRESET_SMALL)
         import oracle as O
+        cfg = workload_config(args.workload)
         d = O.df_cfg_from(cfg)
-        rng = np.random.default_rng(0)
-        params = []
-        for net in (0, 1):
-            p = rng.uniform(-0.1, 0.1, O.df_n_params(d, net)).astype(np.float32)
-            params.append(p)
-        per_step = max(1.0, args.cpu_seconds / max(1, args.steps + args.warmup))
+        params = [bench_weights(cfg, net, O.df_n_params(d, net), 1234) for net in (0, 1)]
+        inputs = cpu_inputs(n, 42)
         for _ in range(args.warmup):
-            cpu_reference(args.workload, cfg, params, per_step, threads)
-        vals = [cpu_reference(args.workload, cfg, params, per_step, threads) for _ in range(args.steps)]
-        v = statistics.median(x[0] for x in vals)
-        sample = f"{vals[0][1]} queries per step of the {n}-query workload, {threads} threads"
+            cpu_reference(cfg, params, inputs, threads)
+        vals = [cpu_reference(cfg, params, inputs, threads) for _ in range(args.steps)]
+        ms = statistics.mean(x[2] for x in vals) * 1e3
+        v = n / (ms * 1e-3)
+        sample = (f"the whole {n}-query bounce per step, {threads} threads: reference epilogue (train.h "
+                  f"thetaPostInference / phiPostInference compiled for the host) after a scalar fp32 forward of "
+                  f"the same encodings and MLPs, same weights and inputs as the GPU arm")
         line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "queries/s", "n_gpus": args.gpus,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": n / v * 1e3,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic", "config": {"workload": workload_name, "queries": n},
-                "cpu_baseline": {"value": v, "unit": "queries/s", "cores": threads, "kind": "port",
+                "cpu_baseline": {"value": v, "unit": "queries/s", "cores": threads, "kind": "reference",
                                  "sample": sample},
                 "e2e": {"value": v, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
@@ -310,6 +376,11 @@ def main():
     train_times, rec_times, last, n_rec, rec_bytes = [], [], None, 0, 0
     if "train" in stages:
         train_times, last = time_train(ctx, cfg, W, nb, rank, dev, stream, flush, args)
+    refgpu = None
+    if "refgpu" in stages:
+        refgpu = time_reference_gpu(ctx, cfg, params, q, wi0, guided, nb, rank, dev, stream, flush, args,
+                                    statistics.mean(times),
+                                    statistics.mean(train_times) if train_times else None)
     if "records" in stages:
         rec_times, n_rec, rec_bytes = time_records(ctx, W, n, rank, dev, stream, flush, args)
     form_times = {}
@@ -344,7 +415,7 @@ def main():
     ctx.sync(stream)
     _report(args, rank, world, dist, dev, n, cfg, params, times, e2e_times, train_times, rec_times,
             last, n_rec, rec_bytes, clk, nb, workload_name, threads, q_h, wi_h, guided_h, form_times,
-            grouped, serving, pcie)
+            grouped, serving, pcie, refgpu)
     ctx.close()
     if dist:
         dist.destroy_process_group()
@@ -413,6 +484,62 @@ def time_grouped(W, rank, dev, stream, flush, args):
     for c in ctxs:
         c.close()
     return res
+
+
+def time_reference_gpu(ctx, cfg, params, q, wi0, guided, nb, rank, dev, stream, flush, args, ms_ours,
+                       ms_ours_train):
+    """The reference's own GPU path on this box: tiny-cuda-nn v1.6 and the
+    reference DF kernels rebuilt for sm_100a (oracle/_ref/libgdf_tcnnref_*),
+    with this arm's weights. Inference: the same bounce, query rows and
+    guided mask, with explicit uniforms (the reference draws from a per-pixel
+    sampler in memory; this library is also timed on the same explicit
+    uniforms). Training: one batch of the same size as the `train` object."""
+    import torch
+    import oracle as O
+    import tcnnref as T
+    from pygdf import workload as W
+    if not T.available(cfg.n_bins_theta, cfg.n_bins_phi):
+        return {"unavailable": "reference GPU harness not built (oracle/build_ref_gpu.py)"}
+    R = T.DfRef(cfg)
+    for net in (0, 1):
+        R.set_params(net, params[net])
+    n = q.shape[0]
+    u = torch.from_numpy(O.philox_uniforms(7, 0, n)).to(dev)
+    wi = wi0.clone()
+    sp = stream.cuda_stream
+
+    def timed(fn, reps, warm):
+        for _ in range(warm):
+            wi.copy_(wi0)
+            fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            wi.copy_(wi0)
+            flush.zero_()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            fn()
+            e.record(stream)
+            e.synchronize()
+            ts.append(s.elapsed_time(e))
+        return statistics.mean(ts)
+
+    ms_ref = timed(lambda: R.infer(wi, u, queries=q, guided=guided, stream=sp), args.steps, args.warmup)
+    ms_same_u = timed(lambda: ctx.infer(q, wi, guided=guided, uniforms=u, n=n, stream=stream), args.steps,
+                      args.warmup)
+    ta, tb, tt = W.training_batch(nb, 77 + rank, cfg.n_bins_theta)
+    da, db, dt = (torch.from_numpy(x).to(dev) for x in (ta, tb, tt))
+    ms_ref_train = timed(lambda: R.train_step(da, db, dt, stream=sp), args.steps, args.warmup)
+    R.close()
+    return {"what": "tiny-cuda-nn v1.6 + reference DF kernels (train.h / train.cu), rebuilt from the reference "
+                    "tree for sm_100a; LearnedDistribution::inferenceStep and one trainStep batch, same weights",
+            "infer_ms": ms_ref, "infer_queries_s": n / (ms_ref * 1e-3),
+            "ours_same_uniforms_ms": ms_same_u,
+            "ratio_infer": ms_ref / ms_ours, "ratio_infer_same_uniforms": ms_ref / ms_same_u,
+            "train_ms": ms_ref_train, "train_records_s": nb / (ms_ref_train * 1e-3),
+            "ratio_train": ms_ref_train / ms_ours_train if ms_ours_train else None,
+            "batch": nb, "queries": n}
 
 
 SERVE_SLOTS, SERVE_TRAIN_SLOTS = 8, 2
@@ -592,7 +719,7 @@ def job_rate(units_per_rank, world, ms):
 
 def _report(args, rank, world, dist, dev, n, cfg, params, times, e2e_times, train_times, rec_times,
             last, n_rec, rec_bytes, clk, nb, workload_name, threads, q_h, wi_h, guided_h, form_times,
-            grouped, serving, pcie=None):
+            grouped, serving, pcie=None, refgpu=None):
     import torch
     ms = statistics.mean(times)
     ms_e2e = statistics.mean(e2e_times) if e2e_times else float("nan")
@@ -613,7 +740,7 @@ def _report(args, rank, world, dist, dev, n, cfg, params, times, e2e_times, trai
         if os.path.exists(prof):
             traffic = json.load(open(prof)).get("dram_bytes_per_step")
         if args.cpu_seconds > 0:
-            cpu_v, cpu_n, cpu_s = cpu_reference(args.workload, cfg, params, args.cpu_seconds, threads)
+            cpu_v, cpu_n, cpu_s = cpu_sample(cfg, params, args.cpu_seconds, threads)
         else:
             cpu_v, cpu_n, cpu_s = None, 0, 0.0
         line = {
@@ -628,8 +755,10 @@ def _report(args, rank, world, dist, dev, n, cfg, params, times, e2e_times, trai
                          "unit": "TFLOP/s", "frac": achieved / peaks["bf16_tflops"], "traffic": traffic,
                          "peak_source": peaks["source"], "kernel": "gdf_infer: grid_features_kernel + df_fused_kernel",
                          "flop_per_query": FLOP_PER_QUERY[args.workload]},
-            "cpu_baseline": {"value": cpu_v, "unit": "queries/s", "cores": threads, "kind": "port",
-                             "sample": f"{cpu_n} queries ({cpu_s:.1f} s) of the same workload"},
+            "cpu_baseline": {"value": cpu_v, "unit": "queries/s", "cores": threads, "kind": "reference",
+                             "sample": f"{cpu_n} queries ({cpu_s:.1f} s): the bounce's first 131,072 queries "
+                                       f"repeated; reference epilogue (train.h) compiled for the host after a "
+                                       f"scalar fp32 forward of the same networks and weights"},
         }
         if train_times:
             line["train"] = {
@@ -659,6 +788,8 @@ def _report(args, rank, world, dist, dev, n, cfg, params, times, e2e_times, trai
             line[name] = {"metric": "guided queries/s, " + what[name],
                           "value": job_rate(n, world, mb), "unit": "queries/s", "ms_per_step": mb,
                           "vs_fp16": ms / mb}
+        if refgpu:
+            line["reference_gpu"] = refgpu
         if grouped:
             line["grouped"] = grouped
         if serving:
