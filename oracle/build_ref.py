@@ -46,7 +46,7 @@ def build(force: bool = False) -> str | None:
     if not force and os.path.exists(SO) and os.path.getmtime(SO) >= max(os.path.getmtime(p) for p in deps):
         return SO
     os.makedirs(OUT_DIR, exist_ok=True)
-    cmd = ["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared", "-w",
+    cmd = ["g++", "-std=c++17", "-O2", "-DNDEBUG", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared", "-w",
            "-I", os.path.join(HERE, "ref_stub"), "-I", guided, "-I", os.path.join(ref, "src"),
            "-I", "/usr/local/cuda/include", "-o", SO + ".tmp", *srcs]
     subprocess.run(cmd, check=True)
@@ -84,7 +84,7 @@ def build_cpu_baseline(force: bool = False) -> list[str]:
         if force or not os.path.exists(so) or os.path.getmtime(so) < newest:
             # a portable x86-64 server ISA (the GPU box's host CPU is not this
             # one); no contraction, so the forward equals the oracle's fp32 one
-            flags = ["-O3", "-mavx2", "-mfma", "-ffp-contract=off", "-fopenmp", "-fPIC", "-w"]
+            flags = ["-O3", "-DNDEBUG", "-mavx2", "-mfma", "-ffp-contract=off", "-fopenmp", "-fPIC", "-w"]
             obj = so + ".oracle.o"
             subprocess.run(["gcc", "-std=c11", *flags, "-c", srcs[1], "-o", obj], check=True)
             subprocess.run(["g++", "-std=c++17", *flags, "-shared", f"-DGDF_REF_BINS_THETA={t}",

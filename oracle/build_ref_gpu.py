@@ -8,7 +8,10 @@ sources are read where they lie; nothing is copied into this repository):
     reduce_sum}.cu with its vendored CUTLASS 2.9 and fmt headers, the flags of
     tcnn/CMakeLists.txt (C++17, --extended-lambda, --expt-relaxed-constexpr,
     TCNN_MIN_GPU_ARCH=90: the newest architecture its CMake accepts, which
-    it would pick on a B200) and fmt's format.cc / os.cc;
+    it would pick on a B200) and fmt's format.cc / os.cc, in the Release
+    configuration the reference is built in (-O3 -DNDEBUG: its device-side
+    assert(mIsTwoSided) in AR.h:33 is compiled out, as in the reference's
+    own build, so a record whose fp16 pdf underflows to zero trains on);
   - oracle/ref_gpu/harness.cu, which includes the reference's unmodified
     src/render/guided/train.cu (and through it train.h, AR.h, guideditem.h,
     workqueue.h), once per bin configuration.
@@ -34,7 +37,7 @@ from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
-OBJ = os.path.join(OUT, "tcnn_obj")
+OBJ = os.path.join(OUT, "tcnn_obj_release")
 SHADOW = os.path.join(OUT, "shadow")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -58,7 +61,7 @@ def lib_path(theta: int, phi: int) -> str:
 
 def _tcnn_flags(ref: str) -> list[str]:
     t = os.path.join(ref, "src", "ext", "tcnn")
-    return ["-std=c++17", "-O3", "--extended-lambda", "--expt-relaxed-constexpr", "-DTCNN_MIN_GPU_ARCH=90",
+    return ["-std=c++17", "-O3", "-DNDEBUG", "--extended-lambda", "--expt-relaxed-constexpr", "-DTCNN_MIN_GPU_ARCH=90",
             "-Xcompiler", "-fPIC", "-Xcompiler", "-fno-strict-aliasing", "-Xcompiler", "-mf16c", "-w",
             "-Xcudafe", "--diag_suppress=unrecognized_gcc_pragma",
             "-I", os.path.join(t, "include"), "-I", os.path.join(t, "dependencies"),

@@ -265,6 +265,18 @@ def test_infer_ex_shading_equals_prepared_queries():
     ctx.infer_ex(w_b, shading=sh, aabb=box, seed=9, offset=2)
     torch.cuda.synchronize()
     np.testing.assert_array_equal(_host(w_a), _host(w_b))
+    # the pipelined path (chunks of 32 tiles) takes the same shading points
+    # chunk by chunk, with the consumer view alongside
+    dp_a, dp_b = dev(np.zeros((n, 4), np.float32)), dev(np.zeros((n, 4), np.float32))
+    w_c, w_d = dev(wi0), dev(wi0)
+    ctx.set_infer_pipeline(0, 2)
+    ctx.infer_ex(w_c, shading=sh, aabb=box, seed=9, offset=2, dir_pdf=dp_a)
+    ctx.set_infer_pipeline(32, 2)
+    ctx.infer_ex(w_d, shading=sh, aabb=box, seed=9, offset=2, dir_pdf=dp_b)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(_host(w_a), _host(w_c))
+    np.testing.assert_array_equal(_host(w_c), _host(w_d))
+    np.testing.assert_array_equal(_host(dp_a), _host(dp_b))
     ctx.close()
 
 
@@ -278,14 +290,13 @@ def test_infer_ex_dir_pdf_is_the_autoregressive_view():
     ctx.infer_ex(wi, queries=q, guided=dev(guided), seed=1, offset=0, dir_pdf=dp)
     torch.cuda.synchronize()
     w, d = _host(wi), _host(dp)
-    # squareToUniformSphere (math_utils.h:226-231), pdf = |pt| |pp| / (4 pi) (AR.h:41-43)
-    z = 1.0 - 2.0 * w[:, 0].astype(np.float64)
-    r = np.sqrt(np.maximum(0.0, 1.0 - z * z))
-    ph = 2.0 * np.pi * w[:, 1].astype(np.float64)
-    ref = np.stack([r * np.cos(ph), r * np.sin(ph), z], axis=1)
-    np.testing.assert_allclose(d[:, :3], ref, rtol=0, atol=4e-6)
-    pdf = (np.abs(w[:, 2]) * np.abs(w[:, 3])) * np.float32(0.0795774715459476678844)
-    np.testing.assert_array_equal(d[:, 3], pdf.astype(np.float32))
+    # the oracle's AutoRegressive view, bit-exact to AR.h:25-48 compiled from
+    # the reference (test_reference_pin.py): squareToUniformSphere and
+    # pdf = |pt| |pp| / (4 pi); directions within the sinf/cosf difference
+    # between the GPU and the host C library
+    ref = O.autoregressive(w)
+    np.testing.assert_array_equal(d[:, 3], ref[:, 0])
+    np.testing.assert_allclose(d[:, :3], ref[:, 1:], rtol=0, atol=4e-6)
     np.testing.assert_allclose(np.linalg.norm(d[:, :3], axis=1), 1.0, atol=4e-6)
     ctx.close()
 
