@@ -277,6 +277,34 @@ __device__ __forceinline__ void ones_to_tile(uint8_t* tile, uint32_t row, uint32
   for (uint32_t c = col0; c < col1; c += 2) store_h2(tile, row, c, K, 1.f, 1.f, bf16);
 }
 
+// The theta network's input after its grid features, at columns [col, K):
+// SH(16) of q[3..5], OneBlob(4 bins) of q[6..8], then K - col - 28 alignment
+// columns -- as the reference computes them. In the theta composite OneBlob
+// is the last encoding, so it takes the alignment padding, and tiny-cuda-nn
+// v1.6 writes that padding (encodings/oneblob.h:223-226, SoA layout) starting
+// n_dims_to_encode = 3 rows into OneBlob's own outputs instead of after its
+// 12: OneBlob outputs [3, 3 + pad) read 1, and the pad columns keep what the
+// fresh buffer holds, 0. (The phi composite ends with TriangleWave, whose
+// kernel pads correctly: ones_to_tile.)
+__device__ __forceinline__ void theta_rest_to_tile(const float* q, uint8_t* tile, uint32_t row,
+                                                   uint32_t col, uint32_t K, bool bf16 = false) {
+  constexpr uint32_t kObFirst = 16, kObWidth = 12, kObDims = 3;
+  float v[28];
+  sh4_encode(q[3], q[4], q[5], v);
+  oneblob_encode<4>(q[6], v + 16);
+  oneblob_encode<4>(q[7], v + 20);
+  oneblob_encode<4>(q[8], v + 24);
+  const uint32_t pad = K - col - 28;
+#pragma unroll
+  for (uint32_t j = kObDims; j < kObWidth; ++j)
+    if (j < kObDims + pad) v[kObFirst + j] = 1.f;
+  store_run(tile, row, col, K, v, 28, bf16);
+  for (uint32_t c = col + 28; c < K; c += 2) {
+    const uint32_t j = c - col - kObFirst;  // row within OneBlob's padded output
+    store_h2(tile, row, c, K, j < kObDims + pad ? 1.f : 0.f, j + 1 < kObDims + pad ? 1.f : 0.f, bf16);
+  }
+}
+
 // ------------------------------------------------------------- warpgroup
 struct Wg {
   uint8_t* tile_a;     // activations / first-layer input (generic pointer)

@@ -200,10 +200,9 @@ __global__ void __launch_bounds__(128 * WGS, 4 / WGS) df_fused_kernel(const __gr
       for (int i = 0; i < 9; ++i) qp[i] = q[i];
     }
 
-    // ---- 1. theta input (grid features | SH | OneBlob | 1-pad), layer 0
+    // ---- 1. theta input (grid features | SH | OneBlob | padding), layer 0
     if constexpr (kFeat) {
-      tile::sh_ob_to_tile(q, c.tile_a, c.row, 0, KTR, c.bf16);
-      tile::ones_to_tile(c.tile_a, c.row, 28, KTR, KTR, c.bf16);
+      tile::theta_rest_to_tile(q, c.tile_a, c.row, 0, KTR, c.bf16);
       mbar_wait(fbar, fphase, p.err, kErrMbarTimeout);
       fphase ^= 1u;
       tile::publish(c);
@@ -213,8 +212,7 @@ __global__ void __launch_bounds__(128 * WGS, 4 / WGS) df_fused_kernel(const __gr
     } else {
       tile::grids_to_tiles<L, F>(p.gl_theta, p.grid_theta, p.gl_phi, p.grid_phi, q, qp, c.tile_a, KT,
                                  c.tile_p, c.row);
-      tile::sh_ob_to_tile(q, c.tile_a, c.row, LF, KT);
-      tile::ones_to_tile(c.tile_a, c.row, LF + 28, KT, KT);
+      tile::theta_rest_to_tile(q, c.tile_a, c.row, LF, KT);
       tile::publish(c);
       const tile::ASeg a{c.tile_a_s, KT, static_cast<int>(KT / 16)};
       tile::issue(c, &a, 1, w_theta, KT, 64);

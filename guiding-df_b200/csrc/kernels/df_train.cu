@@ -278,14 +278,14 @@ __global__ void __launch_bounds__(128, 1) df_train_bwd_kernel(const __grid_const
     }
 
     // ---- forward: X = [XF | XR] | H_1 .. H_H | logits
-    tile::sh_ob_to_tile(q, x_tile, c.row, 0, KR0);
     if constexpr (PHI) {
+      tile::sh_ob_to_tile(q, x_tile, c.row, 0, KR0);
       float tw[12];
       triangle_wave_encode<12>(q[9], tw);
       tile::store_run(x_tile, c.row, 28, KR0, tw, 12);
       tile::ones_to_tile(x_tile, c.row, 40, KR0, KR0);
     } else {
-      tile::ones_to_tile(x_tile, c.row, 28, KR0, KR0);
+      tile::theta_rest_to_tile(q, x_tile, c.row, 0, KR0);
     }
     mbar_wait(&bars[2], fphase, p.err, kErrMbarTimeout);
     fphase ^= 1u;

@@ -216,9 +216,8 @@ __global__ void __launch_bounds__(128 * WGS, 1) group_fused_kernel(const __grid_
     float q[9];
 #pragma unroll
     for (int i = 0; i < 9; ++i) q[i] = valid ? __ldg(J.queries + row * 9 + i) : 0.5f;
-    // theta input (grid features | SH | OneBlob | 1-pad), layer 0
-    tile::sh_ob_to_tile(q, c.tile_a, c.row, 0, KTR, BF16);
-    tile::ones_to_tile(c.tile_a, c.row, 28, KTR, KTR, BF16);
+    // theta input (grid features | SH | OneBlob | padding), layer 0
+    tile::theta_rest_to_tile(q, c.tile_a, c.row, 0, KTR, BF16);
     mbar_wait(fbar, fphase, g.err, kErrMbarTimeout);
     fphase ^= 1u;
     tile::publish(c);

@@ -320,8 +320,9 @@ int64_t go_nrc_n_params(const go_nrc_config* c) {
 
 /* Composite input of the theta (9 dims) or phi (10 dims) network:
  * [grid(pos) | SH(wo') | OneBlob(n_theta', n_phi', r') | (phi: TriangleWave(theta'))
- *  | 1.0 padding], base_product_df.json order; the last nested encoding pads
- * with ones (oneblob.h:225, triangle_wave.h:65). Values rounded to fp16. */
+ *  | padding], base_product_df.json order; the last nested encoding takes the
+ * alignment padding: TriangleWave writes ones (triangle_wave.h:65), OneBlob
+ * (theta) writes them at the wrong rows (below). Values rounded to fp16. */
 void go_df_encode(const go_df_config* c, const go_grid* g, int net, const float* params16,
                   const float* q, float theta_cond, float* out) {
   const int32_t k0 = go_df_input_width(c, net);
@@ -332,13 +333,22 @@ void go_df_encode(const go_df_config* c, const go_grid* g, int net, const float*
   o += g->c.n_levels * g->c.n_features_per_level;
   go_sh_encode(c->sh_degree, q + 3, tmp + o);
   o += c->sh_degree * c->sh_degree;
+  const int ob = o;
   go_oneblob_encode(c->oneblob_bins, q + 6, 3, tmp + o);
   o += 3 * c->oneblob_bins;
   if (net == 1) {
     go_triangle_wave_encode(c->tw_frequencies, theta_cond, tmp + o);
     o += c->tw_frequencies;
+    for (; o < k0; ++o) tmp[o] = 1.0;
+  } else {
+    /* OneBlob is the theta composite's last encoding and takes its alignment
+       padding; tcnn's OneBlob writes that padding (encodings/oneblob.h:223-226,
+       SoA layout) from n_dims_to_encode (3) rows into its own output: outputs
+       [3, 3 + pad) read 1 and the pad columns stay as allocated, 0. */
+    const int pad = k0 - o;
+    for (; o < k0; ++o) tmp[o] = 0.0;
+    for (int j = 3; j < 3 + pad; ++j) tmp[ob + j] = 1.0;
   }
-  for (; o < k0; ++o) tmp[o] = 1.0;
   for (int i = 0; i < k0; ++i) out[i] = go_store(tmp[i]);
 }
 
