@@ -296,11 +296,6 @@ void free_host_stage(Context& c) {
     if (e) cudaEventDestroy(e);
     e = nullptr;
   }
-  for (int i = 0; i < Context::kRingSlots; ++i) {
-    if (c.ring_feat_ev[i]) cudaEventDestroy(c.ring_feat_ev[i]);
-    if (c.ring_mlp_ev[i]) cudaEventDestroy(c.ring_mlp_ev[i]);
-    c.ring_feat_ev[i] = c.ring_mlp_ev[i] = nullptr;
-  }
 }
 
 void free_pw(gdf::PathWorkspace& w) {
@@ -549,78 +544,6 @@ static gdf_status grid_features(Context& c, const float* queries, const gdf_shad
   return GDF_OK;
 }
 
-// Inference of a large call as a pipeline of chunks of c.ring_chunk_tiles
-// tiles: stream pipe[0] gathers the grid features of every chunk in turn
-// into a ring of two feature buffers, stream pipe[1] runs the fused kernel
-// on each chunk as soon as its features are in, with two warpgroups per CTA
-// (c.ring_wgs), which leaves half of every SM's registers and shared memory
-// to the next chunk's gather blocks. The gathers (bound by L1-miss requests)
-// and the MLP / epilogue work (bound by instruction issue) then share the
-// SMs instead of taking turns, and a chunk's feature tiles are read back
-// while they are still in L2. Each chunk continues the Philox counter
-// (philox_row_base) and writes its own rows, so the results equal a single
-// launch's. Ordered after prior work on `user`; work issued on `user`
-// afterwards waits for both pipeline streams.
-static gdf_status infer_pipelined(Context& c, const gdf::DfKernelParams& base, const float* queries,
-                                  const gdf_shading* sh, const gdf_aabb& aabb, int64_t n, cudaStream_t user) {
-  const int64_t chunk_tiles = c.ring_chunk_tiles;
-  const int64_t chunk = chunk_tiles * 128;
-  if (!c.pipe[0]) {
-    for (cudaStream_t& ps : c.pipe) GDF_CUDA(cudaStreamCreateWithFlags(&ps, cudaStreamNonBlocking));
-    for (cudaEvent_t& e : c.pipe_ev) GDF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-  }
-  if (!c.ring_feat_ev[0]) {
-    for (int i = 0; i < Context::kRingSlots; ++i) {
-      GDF_CUDA(cudaEventCreateWithFlags(&c.ring_feat_ev[i], cudaEventDisableTiming));
-      GDF_CUDA(cudaEventCreateWithFlags(&c.ring_mlp_ev[i], cudaEventDisableTiming));
-    }
-  }
-  gdf_status s = ensure_features(c, Context::kRingSlots * chunk_tiles);
-  if (s) return s;
-  cudaStream_t fs = c.pipe[0], ms = c.pipe[1];
-  GDF_CUDA(cudaEventRecord(c.pipe_ev[2], user));
-  GDF_CUDA(cudaStreamWaitEvent(fs, c.pipe_ev[2], 0));
-  GDF_CUDA(cudaStreamWaitEvent(ms, c.pipe_ev[2], 0));
-  for (int64_t b = 0, k = 0; b < n; b += chunk, ++k) {
-    const int64_t m = std::min(chunk, n - b);
-    const int slot = static_cast<int>(k % Context::kRingSlots);
-    // the slot's previous chunk must have been read by its fused kernel
-    if (k >= Context::kRingSlots) GDF_CUDA(cudaStreamWaitEvent(fs, c.ring_mlp_ev[slot], 0));
-    gdf::DfKernelParams p = base;
-    gdf_shading shk{};
-    if (sh) {
-      shk.pos = sh->pos + b * 3;
-      shk.wo = sh->wo + b * 3;
-      shk.normal = sh->normal + b * 3;
-      shk.roughness = sh->roughness + b;
-      p.shading = shk;
-    }
-    p.queries = queries ? queries + b * 9 : nullptr;
-    p.guided = base.guided ? base.guided + b : nullptr;
-    p.uniforms = base.uniforms ? base.uniforms + b * 4 : nullptr;
-    p.wi = base.wi + b * 4;
-    p.dir_pdf = base.dir_pdf ? base.dir_pdf + b * 4 : nullptr;
-    p.n = m;
-    p.philox_row_base = base.philox_row_base + b;
-    if ((s = grid_features(c, p.queries, sh ? &shk : nullptr, aabb, m, p, fs, slot * chunk_tiles))) return s;
-    GDF_CUDA(cudaEventRecord(c.ring_feat_ev[slot], fs));
-    GDF_CUDA(cudaStreamWaitEvent(ms, c.ring_feat_ev[slot], 0));
-    cudaError_t e = gdf::launch_df_fused(df_shape(c), gdf::kModeInfer, p, c.num_sms, ms, c.ring_wgs);
-    if (e != cudaSuccess) return cuda_fail(e, "df_fused (pipelined)");
-    GDF_CUDA(cudaEventRecord(c.ring_mlp_ev[slot], ms));
-  }
-  GDF_CUDA(cudaEventRecord(c.pipe_ev[0], fs));
-  GDF_CUDA(cudaEventRecord(c.pipe_ev[1], ms));
-  GDF_CUDA(cudaStreamWaitEvent(user, c.pipe_ev[0], 0));
-  GDF_CUDA(cudaStreamWaitEvent(user, c.pipe_ev[1], 0));
-  return GDF_OK;
-}
-
-// Whether a call of n queries takes the pipelined path.
-static bool use_pipeline(const Context& c, int64_t n) {
-  return c.ring_chunk_tiles > 0 && n >= 2 * c.ring_chunk_tiles * 128;
-}
-
 extern "C" {
 
 gdf_status gdf_create(const gdf_config* cfg, gdf_ctx** out) {
@@ -842,8 +765,6 @@ gdf_status gdf_infer(gdf_ctx* ctx, const float* queries, const uint8_t* guided,
   p.n = n;
   p.philox_seed = philox_seed;
   p.philox_offset = philox_offset;
-  if (use_pipeline(ctx->c, n))
-    return infer_pipelined(ctx->c, p, queries, nullptr, gdf_aabb{}, n, static_cast<cudaStream_t>(stream));
   if ((s = grid_features(ctx->c, queries, nullptr, gdf_aabb{}, n, p, static_cast<cudaStream_t>(stream))))
     return s;
   cudaError_t e = gdf::launch_df_fused(df_shape(ctx->c), gdf::kModeInfer, p, ctx->c.num_sms,
@@ -887,24 +808,12 @@ gdf_status gdf_infer_ex(gdf_ctx* ctx, const gdf_infer_args* a, void* stream) {
   p.n = n;
   p.philox_seed = a->philox_seed;
   p.philox_offset = a->philox_offset;
-  if (use_pipeline(ctx->c, n))
-    return infer_pipelined(ctx->c, p, a->shading ? nullptr : a->queries_dev, a->shading, a->aabb, n,
-                           static_cast<cudaStream_t>(stream));
   if ((s = grid_features(ctx->c, a->queries_dev, a->shading, a->aabb, n, p,
                          static_cast<cudaStream_t>(stream))))
     return s;
   cudaError_t e = gdf::launch_df_fused(df_shape(ctx->c), gdf::kModeInfer, p, ctx->c.num_sms,
                                        static_cast<cudaStream_t>(stream));
   if (e != cudaSuccess) return cuda_fail(e, "df_fused (infer)");
-  return GDF_OK;
-}
-
-gdf_status gdf_set_infer_pipeline(gdf_ctx* ctx, int64_t chunk_tiles, int32_t warpgroups) {
-  if (!ctx) return fail(GDF_ERR_INVALID_ARG, "ctx is null");
-  if (chunk_tiles < 0 || (warpgroups != 2 && warpgroups != 4))
-    return fail(GDF_ERR_INVALID_ARG, "chunk_tiles must be >= 0 and warpgroups 2 or 4");
-  ctx->c.ring_chunk_tiles = chunk_tiles;
-  ctx->c.ring_wgs = warpgroups;
   return GDF_OK;
 }
 

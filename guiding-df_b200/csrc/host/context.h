@@ -112,14 +112,6 @@ struct Context {
   float* tool_uv = nullptr;      // [tool_cap x 2]
   float* tool_out = nullptr;     // [tool_cap x 4]
   cudaEvent_t pipe_ev[3] = {nullptr, nullptr, nullptr};
-  // Pipelined inference of large calls (gdf_infer, gdf_infer_ex): the grid
-  // features of chunk k+1 are gathered beside the fused kernel of chunk k,
-  // into a ring of kRingSlots feature buffers of ring_chunk_tiles tiles.
-  static constexpr int kRingSlots = 2;
-  int64_t ring_chunk_tiles = 1024;  // 0 = one grid-feature launch, then one fused launch
-  int ring_wgs = 2;                 // warpgroups per fused CTA in the pipelined path
-  cudaEvent_t ring_feat_ev[kRingSlots] = {nullptr, nullptr};
-  cudaEvent_t ring_mlp_ev[kRingSlots] = {nullptr, nullptr};
 };
 
 // Sets the thread-local message returned by gdf_last_error().

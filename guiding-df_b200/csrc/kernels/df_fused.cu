@@ -62,7 +62,7 @@ struct DfWidths {
 // FMT: MLP operand format of the inference forms, 0 fp16, 1 bf16, 2 FP8
 // (e4m3 hidden matrices, mlp_tail_f8).
 template <int L, int F, int NBT, int NBP, bool LINEAR, int MODE, int WGS, int FMT>
-__global__ void __launch_bounds__(128 * WGS, 4 / WGS) df_fused_kernel(const __grid_constant__ DfKernelParams p) {
+__global__ void __launch_bounds__(128 * WGS, 1) df_fused_kernel(const __grid_constant__ DfKernelParams p) {
   using Wd = DfWidths<L, F>;
   constexpr uint32_t LF = L * F;
   constexpr uint32_t KT = Wd::kTheta;            // theta input width
@@ -394,52 +394,29 @@ __global__ void __launch_bounds__(256) pack_fp8_kernel(const __grid_constant__ F
   }
 }
 
-template <int L, int F, int NBT, int NBP, bool LIN, int WGS>
-cudaError_t launch_wgs(int mode, const DfKernelParams& p, size_t smem, int num_sms, cudaStream_t st) {
+template <int L, int F, int NBT, int NBP, bool LIN>
+cudaError_t launch_t(int mode, const DfKernelParams& p, size_t smem, int num_sms, cudaStream_t st) {
   const int64_t n_tiles = (p.n + 127) / 128;
-  int64_t ctas = (n_tiles + WGS - 1) / WGS;
+  int64_t ctas = (n_tiles + kDfWarpgroups - 1) / kDfWarpgroups;
   if (ctas > num_sms) ctas = num_sms;
   if (ctas < 1) ctas = 1;
   const int fmt = (mode == kModeTrainFwd || mode == kModeTrainFeat) ? 0 : (p.fp8 ? 2 : (p.bf16 ? 1 : 0));
   auto pick = [&](auto k16, auto kb16, auto k8) { return fmt == 2 ? k8 : (fmt == 1 ? kb16 : k16); };
-  if constexpr (WGS != kDfWarpgroups) {
-    auto kern = pick(df_fused_kernel<L, F, NBT, NBP, LIN, kModeInfer, WGS, 0>,
-                     df_fused_kernel<L, F, NBT, NBP, LIN, kModeInfer, WGS, 1>,
-                     df_fused_kernel<L, F, NBT, NBP, LIN, kModeInfer, WGS, 2>);
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(smem));
-    if (e != cudaSuccess) return e;
-    kern<<<static_cast<unsigned>(ctas), 128 * WGS, smem, st>>>(p);
-    return cudaGetLastError();
-  }
   auto kern = mode == kModeInfer
-                  ? pick(df_fused_kernel<L, F, NBT, NBP, LIN, kModeInfer, WGS, 0>,
-                         df_fused_kernel<L, F, NBT, NBP, LIN, kModeInfer, WGS, 1>,
-                         df_fused_kernel<L, F, NBT, NBP, LIN, kModeInfer, WGS, 2>)
+                  ? pick(df_fused_kernel<L, F, NBT, NBP, LIN, kModeInfer, kDfWarpgroups, 0>,
+                         df_fused_kernel<L, F, NBT, NBP, LIN, kModeInfer, kDfWarpgroups, 1>,
+                         df_fused_kernel<L, F, NBT, NBP, LIN, kModeInfer, kDfWarpgroups, 2>)
               : mode == kModeEval
-                  ? pick(df_fused_kernel<L, F, NBT, NBP, LIN, kModeEval, WGS, 0>,
-                         df_fused_kernel<L, F, NBT, NBP, LIN, kModeEval, WGS, 1>,
-                         df_fused_kernel<L, F, NBT, NBP, LIN, kModeEval, WGS, 2>)
-              : mode == kModeTrainFeat ? df_fused_kernel<L, F, NBT, NBP, LIN, kModeTrainFeat, WGS, 0>
-                                       : df_fused_kernel<L, F, NBT, NBP, LIN, kModeTrainFwd, WGS, 0>;
+                  ? pick(df_fused_kernel<L, F, NBT, NBP, LIN, kModeEval, kDfWarpgroups, 0>,
+                         df_fused_kernel<L, F, NBT, NBP, LIN, kModeEval, kDfWarpgroups, 1>,
+                         df_fused_kernel<L, F, NBT, NBP, LIN, kModeEval, kDfWarpgroups, 2>)
+              : mode == kModeTrainFeat ? df_fused_kernel<L, F, NBT, NBP, LIN, kModeTrainFeat, kDfWarpgroups, 0>
+                                       : df_fused_kernel<L, F, NBT, NBP, LIN, kModeTrainFwd, kDfWarpgroups, 0>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
   if (e != cudaSuccess) return e;
-  kern<<<static_cast<unsigned>(ctas), 128 * WGS, smem, st>>>(p);
+  kern<<<static_cast<unsigned>(ctas), kDfThreads, smem, st>>>(p);
   return cudaGetLastError();
-}
-
-// Four warpgroups per CTA fill an SM's registers; two leave half of them
-// (and of the shared memory) to grid-feature blocks running beside the CTA
-// (the pipelined inference of large calls). The two-warpgroup form is built
-// for inference only.
-template <int L, int F, int NBT, int NBP, bool LIN>
-cudaError_t launch_t(int mode, const DfKernelParams& p, size_t smem, int num_sms, cudaStream_t st, int wgs) {
-  if (wgs == 2) {
-    if (mode != kModeInfer) return cudaErrorInvalidValue;
-    return launch_wgs<L, F, NBT, NBP, LIN, 2>(mode, p, smem, num_sms, st);
-  }
-  return launch_wgs<L, F, NBT, NBP, LIN, kDfWarpgroups>(mode, p, smem, num_sms, st);
 }
 
 }  // namespace
@@ -452,7 +429,7 @@ bool df_shape_supported(const DfShape& s) {
   return a || b || c;
 }
 
-size_t df_fused_smem_bytes(const DfShape& s, int mode, uint32_t bt, uint32_t bp, int wgs) {
+size_t df_fused_smem_bytes(const DfShape& s, int mode, uint32_t bt, uint32_t bp) {
   const uint32_t lf = static_cast<uint32_t>(s.levels * s.features);
   const uint32_t kt = static_cast<uint32_t>(pad16c(static_cast<int>(lf) + 28));
   const uint32_t kr = static_cast<uint32_t>(pad16c(static_cast<int>(lf) + 40)) - lf;
@@ -460,21 +437,20 @@ size_t df_fused_smem_bytes(const DfShape& s, int mode, uint32_t bt, uint32_t bp,
   const uint32_t ka = feat ? DfWidths<8, 2>::tile_a(kt - lf, kr) : DfWidths<8, 2>::tile_a(kt, kr);
   const size_t off_phi = (bt + 127u) & ~127u;
   const size_t off_tiles = (off_phi + bp + 127u) & ~size_t(127);
-  return off_tiles + static_cast<size_t>(wgs) * 128u * (ka + (feat ? 2u : 1u) * lf) * 2u +
-         8u * (2 * wgs + 1) + 16u;
+  return off_tiles + static_cast<size_t>(kDfWarpgroups) * 128u * (ka + (feat ? 2u : 1u) * lf) * 2u +
+         8u * (2 * kDfWarpgroups + 1) + 16u;
 }
 
 cudaError_t launch_df_fused(const DfShape& s, int mode, const DfKernelParams& p, int num_sms,
-                            cudaStream_t st, int wgs) {
+                            cudaStream_t st) {
   if (p.n <= 0) return cudaSuccess;
-  if (wgs != 2 && wgs != kDfWarpgroups) return cudaErrorInvalidValue;
-  const size_t smem = df_fused_smem_bytes(s, mode, p.blob_theta_bytes, p.blob_phi_bytes, wgs);
+  const size_t smem = df_fused_smem_bytes(s, mode, p.blob_theta_bytes, p.blob_phi_bytes);
   if (mode != kModeTrainFwd && (p.feat_theta == nullptr || p.feat_phi == nullptr))
     return cudaErrorInvalidValue;
 #define GDF_DISPATCH(L, F, NBT, NBP)                                                  \
   if (s.levels == L && s.features == F && s.bins_theta == NBT && s.bins_phi == NBP) { \
-    return s.linear ? launch_t<L, F, NBT, NBP, true>(mode, p, smem, num_sms, st, wgs) \
-                    : launch_t<L, F, NBT, NBP, false>(mode, p, smem, num_sms, st, wgs); \
+    return s.linear ? launch_t<L, F, NBT, NBP, true>(mode, p, smem, num_sms, st)      \
+                    : launch_t<L, F, NBT, NBP, false>(mode, p, smem, num_sms, st);    \
   }
   GDF_DISPATCH(8, 2, 32, 32)
   GDF_DISPATCH(16, 2, 64, 64)

@@ -87,12 +87,9 @@ struct DfShape {
 };
 
 // Returns cudaErrorNotSupported when no kernel is built for the shape.
-// wgs: warpgroups per CTA, 4, or 2 (inference only: leaves half of each SM
-// to grid-feature blocks of the pipelined inference).
 cudaError_t launch_df_fused(const DfShape& s, int mode, const DfKernelParams& p, int num_sms,
-                            cudaStream_t stream, int wgs = kDfWarpgroups);
-size_t df_fused_smem_bytes(const DfShape& s, int mode, uint32_t blob_theta_bytes, uint32_t blob_phi_bytes,
-                           int wgs = kDfWarpgroups);
+                            cudaStream_t stream);
+size_t df_fused_smem_bytes(const DfShape& s, int mode, uint32_t blob_theta_bytes, uint32_t blob_phi_bytes);
 bool df_shape_supported(const DfShape& s);
 
 // Both grids' features for inference / pdf evaluation.

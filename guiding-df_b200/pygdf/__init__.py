@@ -179,7 +179,6 @@ def lib() -> C.CDLL:
             "gdf_set_optimizer_state": [P, C.c_int32, P, P, P, C.c_int64, C.c_uint32],
             "gdf_train_loss_static": [P, P, P, P, C.c_int64, P, P, P],
             "gdf_infer_ex": [P, C.POINTER(InferArgs), P],
-            "gdf_set_infer_pipeline": [P, C.c_int64, C.c_int32],
             "gdf_infer_host": [P, P, P, P, C.c_uint64, C.c_uint64, P, P, C.c_int64, P],
             "gdf_pdf_image": [P, P, C.c_int32, C.c_int32, P, P],
             "gdf_group_create": [C.c_int32, C.POINTER(C.c_void_p)],
@@ -306,9 +305,6 @@ class Context:
         a = np.empty(self.n_params(net), dtype=np.float32)
         check(lib().gdf_get_inference_params(self.h, net, a.ctypes.data, a.size))
         return a
-
-    def set_infer_pipeline(self, chunk_tiles: int, warpgroups: int = 2):
-        check(lib().gdf_set_infer_pipeline(self.h, chunk_tiles, warpgroups))
 
     def save(self, prefix: str):
         check(lib().gdf_save_network(self.h, prefix.encode()))

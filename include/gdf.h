@@ -247,18 +247,6 @@ typedef struct gdf_infer_args {
 } gdf_infer_args;
 gdf_status gdf_infer_ex(gdf_ctx* ctx, const gdf_infer_args* args, void* stream);
 
-/* Pipelined inference of large calls (gdf_infer, gdf_infer_ex). A call of
- * at least 2 x chunk_tiles x 128 queries runs as chunks of chunk_tiles
- * 128-query tiles on two internal streams: the grid features of chunk k+1
- * are gathered while the fused network/sampling kernel works on chunk k,
- * with `warpgroups` (2 or 4) warpgroups per fused CTA -- 2 leaves half of
- * every SM to the gathers, 4 takes whole SMs. chunk_tiles = 0 turns the
- * pipeline off (one gather launch, then one fused launch). The default is
- * 1024 tiles and 2 warpgroups. Results are identical in every setting.
- * No counterpart in the reference, whose inference step is one sequence of
- * launches over the whole wavefront (learnedDistribution.cpp:167-206). */
-gdf_status gdf_set_infer_pipeline(gdf_ctx* ctx, int64_t chunk_tiles, int32_t warpgroups);
-
 /* gdf_infer on HOST buffers, for callers whose queries live in host memory:
  * the inputs are copied in, inferred and the guiding data copied back in
  * chunks of 524,288 queries pipelined over two internal streams, so the

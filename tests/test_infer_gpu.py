@@ -178,32 +178,3 @@ def test_sync_status_clean_after_runs():
     ctx, _, _ = make_ctx(pygdf.PRESET_SMALL)
     ctx.sync()
     ctx.close()
-
-
-@pytest.mark.parametrize("preset", [pygdf.PRESET_SMALL, pygdf.PRESET_FULL])
-@pytest.mark.parametrize("wgs", [2, 4])
-def test_pipelined_inference_equals_single_launch(preset, wgs):
-    """gdf_set_infer_pipeline: a call split into chunks (features of chunk
-    k+1 gathered beside the fused kernel of chunk k, two warpgroups per CTA
-    or four) gives bit for bit what one gather launch + one fused launch
-    gives: Philox counters continue across chunks, ragged last chunk."""
-    import torch
-    ctx, pt, pp = make_ctx(preset, seed=31)
-    n = 4 * 128 * 7 + 77
-    from pygdf import workload as W
-    q = dev(W.queries(n, 3))
-    wi0, guided = W.wi_init(n, 3, 0.8, 0.2)
-    g = dev(guided)
-    u = dev(W.uniforms(n, 3))
-    outs = []
-    for chunk in (0, 4):
-        ctx.set_infer_pipeline(chunk, wgs)
-        a, b = dev(wi0), dev(wi0)
-        ctx.infer(q, a, guided=g, seed=77, offset=5)
-        ctx.infer(q, b, guided=g, uniforms=u)
-        ctx.sync()
-        outs.append((a.cpu().numpy(), b.cpu().numpy()))
-    np.testing.assert_array_equal(outs[0][0], outs[1][0])
-    np.testing.assert_array_equal(outs[0][1], outs[1][1])
-    assert not np.array_equal(outs[0][0], wi0)
-    ctx.close()

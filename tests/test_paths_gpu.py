@@ -265,18 +265,6 @@ def test_infer_ex_shading_equals_prepared_queries():
     ctx.infer_ex(w_b, shading=sh, aabb=box, seed=9, offset=2)
     torch.cuda.synchronize()
     np.testing.assert_array_equal(_host(w_a), _host(w_b))
-    # the pipelined path (chunks of 32 tiles) takes the same shading points
-    # chunk by chunk, with the consumer view alongside
-    dp_a, dp_b = dev(np.zeros((n, 4), np.float32)), dev(np.zeros((n, 4), np.float32))
-    w_c, w_d = dev(wi0), dev(wi0)
-    ctx.set_infer_pipeline(0, 2)
-    ctx.infer_ex(w_c, shading=sh, aabb=box, seed=9, offset=2, dir_pdf=dp_a)
-    ctx.set_infer_pipeline(32, 2)
-    ctx.infer_ex(w_d, shading=sh, aabb=box, seed=9, offset=2, dir_pdf=dp_b)
-    torch.cuda.synchronize()
-    np.testing.assert_array_equal(_host(w_a), _host(w_c))
-    np.testing.assert_array_equal(_host(w_c), _host(w_d))
-    np.testing.assert_array_equal(_host(dp_a), _host(dp_b))
     ctx.close()
 
 
