@@ -257,6 +257,23 @@ def post_inference(d: DfCfg, lt, lp, uniforms, wi, guided=None, edge_gap=False):
     return (w, gap) if edge_gap else w
 
 
+def post_inference_tables(d: DfCfg, table_theta, table_phi, uniforms, wi, guided=None):
+    """thetaPostInference / phiPostInference (train.h:896-929) from given pdf
+    tables (softmax x N already applied): guided rows sample u_theta from
+    uniforms[:, 0:2] and u_phi from uniforms[:, 2:4]; every row's pdfs at its
+    directions multiply into wi[:, 2:4]."""
+    lin = d.pdf_interp == 0
+    w = f32(wi).copy()
+    u = f32(uniforms)
+    for i in range(w.shape[0]):
+        if guided is None or guided[i]:
+            w[i, 0] = sample_dir(table_theta[i], lin, float(u[i, 0]), float(u[i, 1]))[1]
+            w[i, 1] = sample_dir(table_phi[i], lin, float(u[i, 2]), float(u[i, 3]))[1]
+        w[i, 2] *= np.float32(sample_pdf(table_theta[i], float(w[i, 0]), lin))
+        w[i, 3] *= np.float32(sample_pdf(table_phi[i], float(w[i, 1]), lin))
+    return w
+
+
 def nrc_query(nc: NrcCfg, params, inp, n_threads=0):
     p = round_f16(params)
     x = f32(inp)

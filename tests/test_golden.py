@@ -1,0 +1,80 @@
+"""The FP64 oracle against golden vectors of the reference's own GPU path.
+
+tests/golden/reference_*.npz hold outputs of tiny-cuda-nn v1.6 and the
+reference DF kernels, rebuilt from the reference tree and run on a B200 by
+tests/golden/make_golden.py, for seeded inputs and weights that are
+regenerated here with numpy. On the CPU this checks that the oracle's
+encodings and MLPs reproduce the reference's pdf tables (within the
+reference's fp16 accumulation), that the oracle's epilogue turns the
+reference's own tables into the reference's sampled directions and pdfs,
+and that the oracle's divergence loss and MLP gradients match the
+reference's training step.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+import pygdf
+from gdf_testutil import gen_weights
+from pygdf import workload as W
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+FILES = sorted(glob.glob(os.path.join(HERE, "golden", "reference_*.npz")))
+
+pytestmark = pytest.mark.skipif(not FILES, reason="no golden vectors (tests/golden/make_golden.py)")
+
+
+def _load(path):
+    z = dict(np.load(path))
+    cfg = pygdf.default_config(int(z["preset"]))
+    d = O.df_cfg_from(cfg)
+    sw = int(z["seed_w"])
+    pt, pp = gen_weights(cfg, 0, sw, 1.2, 0.2), gen_weights(cfg, 1, sw + 1, 1.2, 0.2)
+    n, sq = int(z["n_queries"]), int(z["seed_q"])
+    q = W.queries(n, sq)
+    wi, guided = W.wi_init(n, sq, 0.8, 0.2)
+    u = W.uniforms(n, sq)
+    return z, cfg, d, pt, pp, q, wi, guided, u
+
+
+@pytest.mark.parametrize("path", FILES, ids=[os.path.basename(f) for f in FILES])
+def test_oracle_tables_reproduce_the_reference(path):
+    z, cfg, d, pt, pp, q, wi, guided, u = _load(path)
+    ref = z["wi"]
+    ot, op = O.pdf_tables(d, pt, pp, q, ref[:, 0])
+    for a, b in ((z["table_theta"], ot), (z["table_phi"], op)):
+        rel = np.abs(a.astype(np.float64) - b) / (np.abs(b) + 1e-3)
+        assert np.percentile(rel, 99) < 5e-3 and rel.max() < 2e-2, (np.percentile(rel, 99), rel.max())
+
+
+@pytest.mark.parametrize("path", FILES, ids=[os.path.basename(f) for f in FILES])
+def test_oracle_epilogue_on_reference_tables(path):
+    """The oracle's sampling and pdf interpolation on the reference's own
+    tables give the reference's guiding data: directions within 1e-6 except
+    where the GPU's contracted multiply-adds move a root (at most 2 % of the
+    rows, within 1e-4), pdfs within 1e-5 relative."""
+    z, cfg, d, pt, pp, q, wi, guided, u = _load(path)
+    ref = z["wi"]
+    w = O.post_inference_tables(d, z["table_theta"], z["table_phi"], u, wi, guided)
+    g = guided.astype(bool)
+    du = np.abs(w[g, :2] - ref[g, :2]).max(axis=1)
+    assert np.mean(du > 1e-6) < 0.02 and du.max() < 1e-4, (np.mean(du > 1e-6), du.max())
+    rel = np.abs(w[:, 2:] - ref[:, 2:]) / (np.abs(ref[:, 2:]) + 1e-6)
+    assert np.percentile(rel, 99) < 1e-5 and rel.max() < 1e-3
+
+
+@pytest.mark.parametrize("path", FILES, ids=[os.path.basename(f) for f in FILES])
+def test_oracle_training_matches_reference(path):
+    z, cfg, d, pt, pp, *_ = _load(path)
+    a, b, t = W.training_batch(int(z["n_train"]), int(z["seed_t"]), cfg.n_bins_theta, cfg.pdf_interp == 0)
+    r = O.df_train_grads(d, pt, pp, a, b, t, cfg.loss_scale)
+    lik = r["likelihood"].astype(np.float64)
+    assert abs(lik.mean() - float(z["loss"])) <= 2e-2 * abs(lik.mean())
+    np.testing.assert_allclose(lik, z["loss_per_record"], rtol=5e-2, atol=1e-3 * np.abs(lik).max())
+    for net, key in ((0, "grad_mlp_theta"), (1, "grad_mlp_phi")):
+        g16 = z[key].astype(np.float64)
+        g64 = (r["grad_theta"] if net == 0 else r["grad_phi"])[:g16.size]
+        assert np.linalg.norm(g16 - g64) / np.linalg.norm(g64) < 5e-2
