@@ -500,7 +500,7 @@ def time_reference_gpu(ctx, cfg, params, q, wi0, guided, nb, rank, dev, stream, 
     from pygdf import workload as W
     if not T.available(cfg.n_bins_theta, cfg.n_bins_phi):
         return {"unavailable": "reference GPU harness not built (oracle/build_ref_gpu.py)"}
-    R = T.DfRef(cfg)
+    R = T.DfRef(cfg, scrub=False)
     for net in (0, 1):
         R.set_params(net, params[net])
     n = q.shape[0]

@@ -56,6 +56,21 @@ constexpr uint32_t kReferenceSeed = 7272;
 
 thread_local std::string g_error;
 
+// Scrubbed-workspace mode (tref_set_scrub): the reference's theta network
+// reads four input columns that nothing writes -- tiny-cuda-nn v1.6's
+// OneBlob, the last encoding of the theta composite, writes its alignment
+// padding three rows into its own outputs instead of after them
+// (encodings/oneblob.h:223-226) -- so they hold whatever the stream's
+// workspace arena held before. On fresh memory that is 0. With scrubbing
+// on, each call first zeroes the start of its streams' arenas, so those
+// columns read 0 on every call, as on the reference's first call.
+bool g_scrub = false;
+
+void scrub_arena(cudaStream_t stream, size_t bytes) {
+  tcnn::GPUMemoryArena::Allocation a = tcnn::allocate_workspace(stream, bytes);
+  CUDA_CHECK_THROW(cudaMemsetAsync(a.data(), 0, bytes, stream));
+}  // freed here: the next allocations on `stream` start inside the zeroed range
+
 // LinearKernel (src/lib/src/core/device/cuda.h:79-92): one thread per
 // element, block size from the occupancy calculator.
 template <typename K, typename... Args>
@@ -215,6 +230,9 @@ extern "C" {
 
 const char* tref_last_error() { return g_error.c_str(); }
 
+// Turns the scrubbed-workspace mode on (nonzero) or off (the default).
+void tref_set_scrub(int32_t on) { g_scrub = on != 0; }
+
 // Bin counts this library was compiled with (N_DIM_OUTPUT, N_DIM_OUTPUT_PHI).
 void tref_bins(int32_t* theta, int32_t* phi) {
   *theta = (int32_t)N_DIM_OUTPUT;
@@ -319,6 +337,7 @@ int tref_df_infer(void* h, const float* queries_dev, const float* pos, const flo
     if (n <= 0) return;
     ensure_inference_capacity(s, n);
     const int64_t padded = tcnn::next_multiple<int64_t>(n, 128);
+    if (g_scrub) scrub_arena(stream, (64u << 20) + (size_t)padded * 1024u);
     // The queue holds n items; the padded rows of the batch are computed but
     // neither sampled nor written (train.h:425 returns for i >= size()).
     ScatterRayQueue q;
@@ -407,6 +426,11 @@ int tref_df_train_step(void* h, const float* in_theta_dev, const float* in_phi_d
     cudaStream_t stream_phi = s.stream_phi;
     if (n <= 0 || n % 128 != 0) throw std::runtime_error{"batch size must be a positive multiple of 128"};
     ensure_train_capacity(s, n);
+    if (g_scrub) {
+      scrub_arena(stream, (64u << 20) + (size_t)n * 4096u);
+      scrub_arena(stream_phi, (64u << 20) + (size_t)n * 4096u);
+      CUDA_CHECK_THROW(cudaDeviceSynchronize());
+    }
     GPUMatrix<float> inputs((float*)in_theta_dev, N_DIM_INPUT, n);
     GPUMatrix<float> inputs_phi((float*)in_phi_dev, N_DIM_INPUT_PHI, n);
     GPUMatrix<precision_t> outputs(s.train_out_theta.data(), N_DIM_PADDED_OUTPUT, n);

@@ -37,6 +37,8 @@ def lib(theta: int, phi: int) -> C.CDLL:
     L = C.CDLL(path, mode=os.RTLD_LOCAL | os.RTLD_NOW)
     vp, i64, i32, fp = C.c_void_p, C.c_int64, C.c_int32, C.POINTER(C.c_float)
     L.tref_last_error.restype = C.c_char_p
+    L.tref_set_scrub.argtypes = [i32]
+    L.tref_set_scrub.restype = None
     L.tref_bins.argtypes = [C.POINTER(i32), C.POINTER(i32)]
     L.tref_df_create.argtypes = [C.c_char_p, C.POINTER(vp)]
     L.tref_df_destroy.argtypes = [vp]
@@ -130,11 +132,18 @@ def _ptr(t) -> int | None:
 
 
 class DfRef:
-    """LearnedDistribution on tiny-cuda-nn (the reference GPU path)."""
+    """LearnedDistribution on tiny-cuda-nn (the reference GPU path).
 
-    def __init__(self, cfg):
+    scrub: zero the start of the workspace arenas before every call, so the
+    four theta-input columns the reference never writes (tiny-cuda-nn's
+    OneBlob misplaces its padding, encodings/oneblob.h:223-226) read 0, as
+    on the reference's first call, instead of stale workspace contents. The
+    parity tests scrub; the speed baseline does not."""
+
+    def __init__(self, cfg, scrub: bool = True):
         self.bins = (cfg.n_bins_theta, cfg.n_bins_phi)
         self.L = lib(*self.bins)
+        self.L.tref_set_scrub(int(scrub))
         h = C.c_void_p()
         _check(self.L, self.L.tref_df_create(json.dumps(df_nn_json(cfg)).encode(), C.byref(h)), "tref_df_create")
         self.h = h

