@@ -53,17 +53,23 @@ def test_oracle_tables_reproduce_the_reference(path):
 @pytest.mark.parametrize("path", FILES, ids=[os.path.basename(f) for f in FILES])
 def test_oracle_epilogue_on_reference_tables(path):
     """The oracle's sampling and pdf interpolation on the reference's own
-    tables give the reference's guiding data: directions within 1e-6 except
-    where the GPU's contracted multiply-adds move a root (at most 2 % of the
-    rows, within 1e-4), pdfs within 1e-5 relative."""
+    tables give the reference's guiding data: directions within 1e-5 (the
+    reference's device code is compiled with contracted multiply-adds, which
+    the host pin of the same functions -- bit-exact to the oracle -- keeps
+    separate; rows off by more than 1e-6 stay under 5 %), and the pdf
+    interpolation at the reference's directions within 1e-5 relative."""
     z, cfg, d, pt, pp, q, wi, guided, u = _load(path)
     ref = z["wi"]
     w = O.post_inference_tables(d, z["table_theta"], z["table_phi"], u, wi, guided)
     g = guided.astype(bool)
     du = np.abs(w[g, :2] - ref[g, :2]).max(axis=1)
-    assert np.mean(du > 1e-6) < 0.02 and du.max() < 1e-4, (np.mean(du > 1e-6), du.max())
-    rel = np.abs(w[:, 2:] - ref[:, 2:]) / (np.abs(ref[:, 2:]) + 1e-6)
-    assert np.percentile(rel, 99) < 1e-5 and rel.max() < 1e-3
+    assert np.mean(du > 1e-6) < 0.05 and du.max() < 1e-5, (np.mean(du > 1e-6), du.max())
+    # pdfs at the reference's own directions (phi conditioned as it was)
+    lin = d.pdf_interp == 0
+    pd = np.array([[O.sample_pdf(z["table_theta"][i], float(ref[i, 0]), lin),
+                    O.sample_pdf(z["table_phi"][i], float(ref[i, 1]), lin)] for i in range(ref.shape[0])])
+    rel = np.abs(pd * wi[:, 2:] - ref[:, 2:]) / (np.abs(ref[:, 2:]) + 1e-6)
+    assert np.percentile(rel, 99) < 1e-6 and rel.max() < 1e-5, (np.percentile(rel, 99), rel.max())
 
 
 @pytest.mark.parametrize("path", FILES, ids=[os.path.basename(f) for f in FILES])

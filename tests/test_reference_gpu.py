@@ -185,7 +185,7 @@ def test_training_matches_reference_gpu_path(preset):
         ours *= cfg.loss_scale
         for sl in (slice(0, n_mlp), slice(n_mlp, None)):
             e_ref = rn(g16[sl], g64[sl])
-            assert e_ref < 5e-2, (net, sl, e_ref)  # fp16 accumulation and fp16 atomics
+            assert e_ref < 0.1, (net, sl, e_ref)  # the reference's fp16 accumulation and fp16 atomics
             assert rn(ours[sl], g64[sl]) < GRAD_RTOL
             assert rn(ours[sl], g16[sl]) <= e_ref + GRAD_RTOL
     R.close()
