@@ -80,8 +80,18 @@ extern "C" gdf_status gdf_train_loss_static(gdf_ctx* ctx, const float* in_theta,
     return GDF_ERR_INVALID_ARG;
   }
   Context& c = ctx->c;
+  // The scratch address is looked up on the current device, the weights live
+  // on the context's: the two must be the same device.
+  int cur = -1;
+  cudaError_t e = cudaGetDevice(&cur);
+  if (e != cudaSuccess || cur != c.device) {
+    set_last_error(("gdf_train_loss_static: the current device (" + std::to_string(cur) +
+                    ") is not the context's device (" + std::to_string(c.device) + ")")
+                       .c_str());
+    return GDF_ERR_INVALID_ARG;
+  }
   void* base = nullptr;
-  cudaError_t e = scratch_address(&base);
+  e = scratch_address(&base);
   if (e != cudaSuccess) {
     set_last_error((std::string("cudaGetSymbolAddress(static scratch): ") + cudaGetErrorString(e)).c_str());
     return GDF_ERR_CUDA;

@@ -333,8 +333,10 @@ gdf_status gdf_set_optimizer_state(gdf_ctx* ctx, int32_t net, const float* m_hos
  *   - loss_out_dev: one double (mean loss), dropped_out_dev: one int64
  *     (records rejected by the validity filter), both device pointers;
  *   - the first call on a device looks up the array's device address
- *     (cudaGetSymbolAddress); make that first call before any stream
- *     capture;
+ *     (cudaGetSymbolAddress) and keeps it for the life of the process; make
+ *     that first call before any stream capture, and do not reset the
+ *     device (cudaDeviceReset) while the library is loaded;
+ *   - the current device must be the context's (else GDF_ERR_INVALID_ARG);
  *   - all calls share the one array: calls whose work overlaps on the GPU
  *     (other streams, other threads) race; order them on one stream. */
 gdf_status gdf_train_loss_static(gdf_ctx* ctx, const float* in_theta_dev, const float* in_phi_dev,

@@ -18,12 +18,13 @@ from pygdf import workload as W
 pytestmark = pytest.mark.gpu
 
 
-def _static_loss(ctx, a, b, t, n):
+def _static_loss(ctx, a, b, t, n, stream=None):
     import torch
     loss = torch.full((1,), float("nan"), dtype=torch.float64, device="cuda")
     dropped = torch.full((1,), -1, dtype=torch.int64, device="cuda")
+    sp = stream.cuda_stream if stream is not None else None
     pygdf.check(pygdf.lib().gdf_train_loss_static(ctx.h, a.data_ptr(), b.data_ptr(), t.data_ptr(), n,
-                                                  loss.data_ptr(), dropped.data_ptr(), None))
+                                                  loss.data_ptr(), dropped.data_ptr(), sp))
     torch.cuda.synchronize()
     return float(loss.item()), int(dropped.item())
 
@@ -61,4 +62,28 @@ def test_static_loss_rejects_batches_beyond_its_capacity():
     assert st == 1 and b"65536" in L.gdf_last_error()
     assert L.gdf_train_loss_static(ctx.h, x.data_ptr(), x.data_ptr(), x.data_ptr(), 0, out.data_ptr(),
                                    out.data_ptr(), None) == 1
+    ctx.close()
+
+
+def test_static_loss_at_full_capacity_on_a_side_stream():
+    """n = 65,536 fills the array exactly; two calls in a row on a stream
+    other than the default one (the counter reset and the kernels are
+    ordered on the caller's stream)."""
+    import torch
+    cfg = pygdf.default_config(pygdf.PRESET_SMALL)
+    ctx = pygdf.Context(cfg)
+    ctx.set_params(0, gen_weights(cfg, 0, 41))
+    ctx.set_params(1, gen_weights(cfg, 1, 42))
+    n = 65536
+    a, b, t = W.training_batch(n, 17, cfg.n_bins_theta)
+    t = t.copy()
+    t[[3, n - 1], 5] = 0.0  # two rejected records, one in the array's last slot
+    da, db, dt = dev(a), dev(b), dev(t)
+    side = torch.cuda.Stream()
+    for _ in range(2):
+        loss, dropped = _static_loss(ctx, da, db, dt, n, stream=side)
+        st = ctx.train_step(da, db, dt)
+        ctx.sync()
+        assert dropped == st.n_dropped == 2
+        assert abs(loss - st.loss) <= 1e-6 * abs(st.loss), (loss, st.loss)
     ctx.close()
