@@ -145,16 +145,35 @@ __device__ __forceinline__ float quartic_cdf(float x, float inv_radius) {
                                                           (1.0f / 5.0f) * u4) + 0.5f));
 }
 
+// The three wrapped kernel CDFs of one bin boundary, q(d) + q(d - 1) +
+// q(d + 1) summed left to right (oneblob.h:116-120), for d = boundary - x.
+// With 4 bins and x in [0, 1] (so d in [-1, 1]), |4 (d - 1)| >= 1.25 unless
+// d > 0.6875 and |4 (d + 1)| >= 1.25 unless d < -0.6875; the quartic is
+// monotone and already -0.023 / 1.023 at u = -1.25 / 1.25, so those terms
+// are exactly 0 and 1 after the clamp, and only one of the two wrapped
+// terms needs evaluating: the same float sum with 2 evaluations instead of 3.
+template <int NB>
+__device__ __forceinline__ float oneblob_boundary(float d, bool in_unit) {
+  const float nb = static_cast<float>(NB);
+  if (NB == 4 && in_unit) {
+    const float qw = quartic_cdf(d > 0.f ? d - 1.0f : d + 1.0f, nb);
+    const float t1 = d > 0.6875f ? qw : 0.0f;
+    const float t2 = d < -0.6875f ? qw : 1.0f;
+    return quartic_cdf(d, nb) + t1 + t2;
+  }
+  return quartic_cdf(d, nb) + quartic_cdf(d - 1.0f, nb) + quartic_cdf(d + 1.0f, nb);
+}
+
 // kernel_one_blob_soa (tcnn encodings/oneblob.h:99-127) for one input dim.
 template <int NB>
 __device__ __forceinline__ void oneblob_encode(float x, float* o) {
   const float nb = static_cast<float>(NB);
-  float left = quartic_cdf(-x, nb) + quartic_cdf(-x - 1.0f, nb) + quartic_cdf(-x + 1.0f, nb);
+  const bool in_unit = x >= 0.0f && x <= 1.0f;
+  float left = oneblob_boundary<NB>(-x, in_unit);
 #pragma unroll
   for (int k = 0; k < NB; ++k) {
     const float rb = static_cast<float>(k + 1) / nb;
-    const float right = quartic_cdf(rb - x, nb) + quartic_cdf(rb - x - 1.0f, nb) +
-                        quartic_cdf(rb - x + 1.0f, nb);
+    const float right = oneblob_boundary<NB>(rb - x, in_unit);
     o[k] = right - left;
     left = right;
   }

@@ -286,23 +286,51 @@ __device__ __forceinline__ void ones_to_tile(uint8_t* tile, uint32_t row, uint32
 // 12: OneBlob outputs [3, 3 + pad) read 1, and the pad columns keep what the
 // fresh buffer holds, 0. (The phi composite ends with TriangleWave, whose
 // kernel pads correctly: ones_to_tile.)
-__device__ __forceinline__ void theta_rest_to_tile(const float* q, uint8_t* tile, uint32_t row,
-                                                   uint32_t col, uint32_t K, bool bf16 = false) {
-  constexpr uint32_t kObFirst = 16, kObWidth = 12, kObDims = 3;
-  float v[28];
-  sh4_encode(q[3], q[4], q[5], v);
-  oneblob_encode<4>(q[6], v + 16);
-  oneblob_encode<4>(q[7], v + 20);
-  oneblob_encode<4>(q[8], v + 24);
+__device__ __forceinline__ void theta_rest_from_values(const float (&v)[28], uint8_t* tile, uint32_t row,
+                                                       uint32_t col, uint32_t K, bool bf16 = false) {
+  constexpr uint32_t kObFirst = 16, kObDims = 3;
   const uint32_t pad = K - col - 28;
 #pragma unroll
-  for (uint32_t j = kObDims; j < kObWidth; ++j)
-    if (j < kObDims + pad) v[kObFirst + j] = 1.f;
-  store_run(tile, row, col, K, v, 28, bf16);
+  for (uint32_t i = 0; i < 28; i += 2) {
+    const bool one0 = i >= kObFirst + kObDims && i < kObFirst + kObDims + pad;
+    const bool one1 = i + 1 >= kObFirst + kObDims && i + 1 < kObFirst + kObDims + pad;
+    store_h2(tile, row, col + i, K, one0 ? 1.f : v[i], one1 ? 1.f : v[i + 1], bf16);
+  }
   for (uint32_t c = col + 28; c < K; c += 2) {
     const uint32_t j = c - col - kObFirst;  // row within OneBlob's padded output
     store_h2(tile, row, c, K, j < kObDims + pad ? 1.f : 0.f, j + 1 < kObDims + pad ? 1.f : 0.f, bf16);
   }
+}
+
+// SH(16) of q[3..5] and OneBlob(4 bins) of q[6..8]: the 28 values both
+// networks' inputs carry after their grid features.
+__device__ __forceinline__ void sh_ob_values(const float* q, float (&v)[28]) {
+  sh4_encode(q[3], q[4], q[5], v);
+  oneblob_encode<4>(q[6], v + 16);
+  oneblob_encode<4>(q[7], v + 20);
+  oneblob_encode<4>(q[8], v + 24);
+}
+
+__device__ __forceinline__ void theta_rest_to_tile(const float* q, uint8_t* tile, uint32_t row,
+                                                   uint32_t col, uint32_t K, bool bf16 = false) {
+  float v[28];
+  sh_ob_values(q, v);
+  theta_rest_from_values(v, tile, row, col, K, bf16);
+}
+
+// n (even) values rounded to the operand format and packed in pairs, for a
+// later store_packed_run.
+template <int N>
+__device__ __forceinline__ void pack_run(const float (&v)[N], bool bf16, uint32_t (&w)[N / 2]) {
+#pragma unroll
+  for (int i = 0; i < N / 2; ++i) w[i] = pack2(v[2 * i], v[2 * i + 1], bf16);
+}
+
+template <int W>
+__device__ __forceinline__ void store_packed_run(uint8_t* t, uint32_t row, uint32_t col, uint32_t K,
+                                                 const uint32_t (&w)[W]) {
+#pragma unroll
+  for (int i = 0; i < W; ++i) *reinterpret_cast<uint32_t*>(t + elem_off(row, col + 2 * i, K)) = w[i];
 }
 
 // ------------------------------------------------------------- warpgroup

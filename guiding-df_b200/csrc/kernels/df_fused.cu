@@ -201,8 +201,15 @@ __global__ void __launch_bounds__(128 * WGS, 1) df_fused_kernel(const __grid_con
     }
 
     // ---- 1. theta input (grid features | SH | OneBlob | padding), layer 0
+    // Inference and pdf evaluation feed the phi network the same first nine
+    // inputs, so its SH / OneBlob values are computed here once and kept,
+    // packed, until its input tile is written (step 5).
+    uint32_t phi_shob[14];
     if constexpr (kFeat) {
-      tile::theta_rest_to_tile(q, c.tile_a, c.row, 0, KTR, c.bf16);
+      float shob[28];
+      tile::sh_ob_values(q, shob);
+      if constexpr (!kTrain) tile::pack_run<28>(shob, c.bf16, phi_shob);
+      tile::theta_rest_from_values(shob, c.tile_a, c.row, 0, KTR, c.bf16);
       mbar_wait(fbar, fphase, p.err, kErrMbarTimeout);
       fphase ^= 1u;
       tile::publish(c);
@@ -258,7 +265,8 @@ __global__ void __launch_bounds__(128 * WGS, 1) df_fused_kernel(const __grid_con
     }
 
     // ---- 5. phi input rest, layer 0 over tile P (grid) + tile A (rest)
-    tile::sh_ob_to_tile(qp, c.tile_a, c.row, 0, KR, c.bf16);
+    if constexpr (kFeat && !kTrain) tile::store_packed_run<14>(c.tile_a, c.row, 0, KR, phi_shob);
+    else tile::sh_ob_to_tile(qp, c.tile_a, c.row, 0, KR, c.bf16);
     {
       float tw[12];
       triangle_wave_encode<12>(cond, tw);

@@ -216,8 +216,15 @@ __global__ void __launch_bounds__(128 * WGS, 1) group_fused_kernel(const __grid_
     float q[9];
 #pragma unroll
     for (int i = 0; i < 9; ++i) q[i] = valid ? __ldg(J.queries + row * 9 + i) : 0.5f;
-    // theta input (grid features | SH | OneBlob | padding), layer 0
-    tile::theta_rest_to_tile(q, c.tile_a, c.row, 0, KTR, BF16);
+    // theta input (grid features | SH | OneBlob | padding), layer 0; the phi
+    // network's SH / OneBlob values are the same, kept packed until its input
+    uint32_t phi_shob[14];
+    {
+      float shob[28];
+      tile::sh_ob_values(q, shob);
+      tile::pack_run<28>(shob, BF16, phi_shob);
+      tile::theta_rest_from_values(shob, c.tile_a, c.row, 0, KTR, BF16);
+    }
     mbar_wait(fbar, fphase, g.err, kErrMbarTimeout);
     fphase ^= 1u;
     tile::publish(c);
@@ -249,7 +256,7 @@ __global__ void __launch_bounds__(128 * WGS, 1) group_fused_kernel(const __grid_
     const tile::RowResult rt = epilogue_bins<LINEAR>(J.bins_theta, c.tmem + c.lane_base, guided, wi.x, u[0], u[1]);
     const float cond = condition_bins<LINEAR>(J.bins_theta, rt.u);
     // phi input rest (SH | OneBlob | TriangleWave(u_theta) | 1-pad), layer 0
-    tile::sh_ob_to_tile(q, c.tile_a, c.row, 0, KR, BF16);
+    tile::store_packed_run<14>(c.tile_a, c.row, 0, KR, phi_shob);
     {
       float tw[12];
       triangle_wave_encode<12>(cond, tw);
