@@ -474,12 +474,14 @@ def time_grouped(W, rank, dev, stream, flush, args):
         out[name] = statistics.mean(times)
     group.sync(stream)
     wgs, fb, tune_ms = group.tuning()
+    small = time_grouped_small(W, rank, dev, stream, flush, args)
     total = jobs_n * sum(sizes)
     res = {"metric": "guided queries/s, 8 jobs x 6 bounces in grouped launches",
            "value": total / (out["grouped"] * 1e-3), "unit": "queries/s", "ms_per_frame": out["grouped"],
            "separate_calls_ms_per_frame": out["separate"], "speedup_vs_separate": out["separate"] / out["grouped"],
            "queries_per_frame": total, "wavefronts": sizes, "bins": "4 jobs x 64, 4 jobs x 32",
-           "launches_per_frame": 2 * bounces, "tuned": {"warpgroups": wgs, "feature_block": fb}}
+           "launches_per_frame": 2 * bounces, "tuned": {"warpgroups": wgs, "feature_block": fb},
+           "small_jobs": small}
     group.close()
     for c in ctxs:
         c.close()
@@ -540,6 +542,66 @@ def time_reference_gpu(ctx, cfg, params, q, wi0, guided, nb, rank, dev, stream, 
             "train_ms": ms_ref_train, "train_records_s": nb / (ms_ref_train * 1e-3),
             "ratio_train": ms_ref_train / ms_ours_train if ms_ours_train else None,
             "batch": nb, "queries": n}
+
+
+def time_grouped_small(W, rank, dev, stream, flush, args):
+    """Many small, uneven jobs -- the case grouping is for: 64 render jobs
+    with their own networks (config-1 sizes, 32 or 64 bins) and wavefronts
+    log-uniform in 2^10..2^16 queries, one grouped call against 64 separate
+    gdf_infer calls."""
+    import torch
+    import pygdf
+    n_jobs = 64
+    rng = np.random.default_rng(700 + rank)
+    sizes = [int(np.exp(rng.uniform(np.log(1 << 10), np.log(1 << 16)))) for _ in range(n_jobs)]
+    ctxs, qs, wis, wi0s, gs = [], [], [], [], []
+    for k in range(n_jobs):
+        cfg = pygdf.default_config(pygdf.PRESET_FULL)
+        cfg.n_bins_theta = cfg.n_bins_phi = 64 if k % 2 == 0 else 32
+        cfg.max_queries = 1 << 16
+        ctxs.append(pygdf.Context(cfg))
+        qs.append(torch.from_numpy(W.queries(sizes[k], 900 + 7 * rank + k)).to(dev))
+        wi_h, g_h = W.wi_init(sizes[k], 900 + k, guided_frac=0.7, one_sided_frac=0.1)
+        wi0s.append(torch.from_numpy(wi_h).to(dev))
+        wis.append(torch.from_numpy(wi_h).to(dev))
+        gs.append(torch.from_numpy(g_h).to(dev))
+    group = pygdf.Group(max_jobs=n_jobs)
+
+    def run(grouped, f):
+        for k in range(n_jobs):
+            wis[k].copy_(wi0s[k])
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        if grouped:
+            group.infer([{"ctx": ctxs[k], "queries": qs[k], "wi": wis[k], "guided": gs[k], "n": sizes[k],
+                          "seed": 9, "offset": f} for k in range(n_jobs)], stream=stream)
+        else:
+            for k in range(n_jobs):
+                ctxs[k].infer(qs[k], wis[k], guided=gs[k], seed=9, offset=f, n=sizes[k], stream=stream)
+        e.record(stream)
+        e.synchronize()
+        return s.elapsed_time(e)
+
+    out = {}
+    for name, grouped in (("grouped", True), ("separate", False)):
+        for f in range(max(args.warmup, 1)):
+            run(grouped, f)
+        ts = []
+        for f in range(args.steps):
+            flush.zero_()
+            ts.append(run(grouped, 1000 + f))
+        out[name] = statistics.mean(ts)
+    group.sync(stream)
+    wgs, fb, _ = group.tuning()
+    group.close()
+    for c in ctxs:
+        c.close()
+    total = sum(sizes)
+    return {"jobs": n_jobs, "queries": total, "sizes": "log-uniform 2^10..2^16 (seeded)",
+            "ms_grouped": out["grouped"], "ms_separate": out["separate"],
+            "speedup_vs_separate": out["separate"] / out["grouped"],
+            "value": total / (out["grouped"] * 1e-3), "unit": "queries/s",
+            "tuned": {"warpgroups": wgs, "feature_block": fb}}
 
 
 SERVE_SLOTS, SERVE_TRAIN_SLOTS = 8, 2

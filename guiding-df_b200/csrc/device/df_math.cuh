@@ -423,7 +423,18 @@ struct SampleResult {
 // instead, so the same latched pair serves the pdf interpolation of every
 // row; a guided sample whose rounding puts it outside its segment falls back
 // to indexed reads.
-template <int N, bool LINEAR>
+// Neumaier's compensated summation step (Neumaier 1974, the improved Kahan
+// sum): s + c carries the running sum with the rounding error of each
+// addition kept in c.
+__device__ __forceinline__ void neumaier_add(float& s, float& c, float x) {
+  const float t = s + x;
+  c += fabsf(s) >= fabsf(x) ? (s - t) + x : (x - t) + s;
+  s = t;
+}
+
+// COMP: the CDF boundaries accumulate with neumaier_add (the BF16 / FP8
+// inference forms); without it they follow the reference's plain float sum.
+template <int N, bool LINEAR, bool COMP = false>
 __device__ __forceinline__ SampleResult sample_and_pdf(const float (&pdf)[N], bool guided, float u_given,
                                                        float u, float u2) {
   const float nf = static_cast<float>(N);
@@ -433,14 +444,20 @@ __device__ __forceinline__ SampleResult sample_and_pdf(const float (&pdf)[N], bo
     int seg = 0;
     float cm1 = 0.f, lo = pdf[0], hi = pdf[0];
     float b = pdf[0] * 0.5f / nf;  // b_0: end of the leading half-bin
+    float bc = 0.f;                 // its compensation (COMP)
     const float b0 = b;
 #pragma unroll
     for (int i = 0; i < N; ++i) {
-      if (i > 0) b = b + (pdf[i - 1] + pdf[i]) / static_cast<float>(2 * N);
-      const bool cond = guided ? (b <= u) : (i <= f_given);
+      if (i > 0) {
+        const float term = (pdf[i - 1] + pdf[i]) / static_cast<float>(2 * N);
+        if constexpr (COMP) neumaier_add(b, bc, term);
+        else b = b + term;
+      }
+      const float bv = COMP ? b + bc : b;
+      const bool cond = guided ? (bv <= u) : (i <= f_given);
       if (cond) {
         seg = i + 1;
-        cm1 = b;
+        cm1 = bv;
         lo = pdf[i];
         hi = pdf[i + 1 < N ? i + 1 : N - 1];
       }
@@ -466,14 +483,16 @@ __device__ __forceinline__ SampleResult sample_and_pdf(const float (&pdf)[N], bo
     const int f_given = safe_floor<N>(u_given * nf);
     int seg = 0;
     float cm1 = 0.f, cur = pdf[0];
-    float c = 0.f;
+    float c = 0.f, cc = 0.f;
 #pragma unroll
     for (int i = 0; i < N; ++i) {
-      c = c + pdf[i] / nf;
-      const bool cond = guided ? (c <= u) : (i < f_given);
+      if constexpr (COMP) neumaier_add(c, cc, pdf[i] / nf);
+      else c = c + pdf[i] / nf;
+      const float cv = COMP ? c + cc : c;
+      const bool cond = guided ? (cv <= u) : (i < f_given);
       if (cond) {
         seg = i + 1;
-        cm1 = c;
+        cm1 = cv;
         cur = pdf[i + 1 < N ? i + 1 : N - 1];
       }
     }

@@ -680,7 +680,9 @@ struct RowResult {
 // registers: softmax2 x N, inversion sampling when `guided` (else u is the
 // given coordinate), pdf interpolation at u. Out of line so the theta and
 // phi networks share one copy of the code.
-template <int NB, bool LINEAR>
+// COMP (the BF16 / FP8 inference forms): the softmax sum and the CDF use
+// Neumaier's compensated summation.
+template <int NB, bool LINEAR, bool COMP = false>
 __device__ __noinline__ RowResult row_epilogue(uint32_t taddr, bool guided, float u_given, float u_main,
                                                float u_fallback) {
   float v[NB];
@@ -707,16 +709,17 @@ __device__ __noinline__ RowResult row_epilogue(uint32_t taddr, bool guided, floa
   for (int i = 0; i < NB; ++i) m = fmaxf(m, v[i]);
   constexpr float kLog2e = 1.4426950408889634074f;
   const float ml = m * kLog2e;
-  float s = 0.0f;
+  float s = 0.0f, sc = 0.0f;
 #pragma unroll
   for (int i = 0; i < NB; ++i) {
     v[i] = ex2_approx(fmaf(v[i], kLog2e, -ml));
-    s += v[i];
+    if constexpr (COMP) neumaier_add(s, sc, v[i]);
+    else s += v[i];
   }
-  const float k = static_cast<float>(NB) / s;
+  const float k = static_cast<float>(NB) / (COMP ? s + sc : s);
 #pragma unroll
   for (int i = 0; i < NB; ++i) v[i] *= k;
-  const SampleResult sr = sample_and_pdf<NB, LINEAR>(v, guided, u_given, u_main, u_fallback);
+  const SampleResult sr = sample_and_pdf<NB, LINEAR, COMP>(v, guided, u_given, u_main, u_fallback);
   RowResult r;
   r.u = sr.u;
   r.pdf = sr.pdf;
@@ -728,7 +731,7 @@ __device__ __noinline__ RowResult row_epilogue(uint32_t taddr, bool guided, floa
 // TMEM, sums them in double and max-merges |1 - sum p_i / N| per warp into
 // *norm_err as the bits of a non-negative double (NaN sorts above all).
 // Called by every lane of the warp, right after row_epilogue.
-template <int NB>
+template <int NB, bool COMP = false>
 __device__ __noinline__ void row_norm_check(uint32_t taddr, unsigned long long* norm_err) {
   float v[NB];
   if constexpr (NB == 16) {
@@ -751,13 +754,14 @@ __device__ __noinline__ void row_norm_check(uint32_t taddr, unsigned long long* 
   for (int i = 0; i < NB; ++i) m = fmaxf(m, v[i]);
   constexpr float kLog2e = 1.4426950408889634074f;
   const float ml = m * kLog2e;
-  float s = 0.0f;
+  float s = 0.0f, sc = 0.0f;
 #pragma unroll
   for (int i = 0; i < NB; ++i) {
     v[i] = ex2_approx(fmaf(v[i], kLog2e, -ml));
-    s += v[i];
+    if constexpr (COMP) neumaier_add(s, sc, v[i]);
+    else s += v[i];
   }
-  const float k = static_cast<float>(NB) / s;
+  const float k = static_cast<float>(NB) / (COMP ? s + sc : s);
   double sum = 0.0;
 #pragma unroll
   for (int i = 0; i < NB; ++i) sum += static_cast<double>(v[i] * k);

@@ -256,9 +256,9 @@ __global__ void __launch_bounds__(128 * WGS, 1) df_fused_kernel(const __grid_con
       cond = qp[9];
     } else {
       const float u_theta_given = MODE == kModeInfer ? wi.x : (valid ? __ldg(p.u_eval + row * 2) : 0.5f);
-      const tile::RowResult rt = tile::row_epilogue<NBT, LINEAR>(
+      const tile::RowResult rt = tile::row_epilogue<NBT, LINEAR, (FMT != 0)>(
           c.tmem + c.lane_base, MODE == kModeInfer && guided, u_theta_given, u[0], u[1]);
-      if (p.norm_err != nullptr) tile::row_norm_check<NBT>(c.tmem + c.lane_base, p.norm_err);
+      if (p.norm_err != nullptr) tile::row_norm_check<NBT, (FMT != 0)>(c.tmem + c.lane_base, p.norm_err);
       u_theta = rt.u;
       pdf_theta = rt.pdf;
       cond = theta_condition<NBT, LINEAR>(u_theta);
@@ -306,9 +306,9 @@ __global__ void __launch_bounds__(128 * WGS, 1) df_fused_kernel(const __grid_con
       continue;
     }
     const float u_phi_given = MODE == kModeInfer ? wi.y : (valid ? __ldg(p.u_eval + row * 2 + 1) : 0.5f);
-    const tile::RowResult rp = tile::row_epilogue<NBP, LINEAR>(
+    const tile::RowResult rp = tile::row_epilogue<NBP, LINEAR, (FMT != 0)>(
         c.tmem + c.lane_base, MODE == kModeInfer && guided, u_phi_given, u[2], u[3]);
-    if (p.norm_err != nullptr) tile::row_norm_check<NBP>(c.tmem + c.lane_base, p.norm_err);
+    if (p.norm_err != nullptr) tile::row_norm_check<NBP, (FMT != 0)>(c.tmem + c.lane_base, p.norm_err);
     if constexpr (MODE == kModeInfer) {
       const float4 o = make_float4(u_theta, rp.u, wi.z * pdf_theta, wi.w * rp.pdf);
       if (valid) *reinterpret_cast<float4*>(p.wi + row * 4) = o;

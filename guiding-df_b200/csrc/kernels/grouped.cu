@@ -46,12 +46,12 @@ __device__ __forceinline__ int find_job(const GroupJobDev* jobs, int n, int64_t 
   return lo;
 }
 
-template <bool LINEAR>
+template <bool LINEAR, bool COMP>
 __device__ __forceinline__ tile::RowResult epilogue_bins(int nb, uint32_t taddr, bool guided, float u_given,
                                                          float u0, float u1) {
-  if (nb == 16) return tile::row_epilogue<16, LINEAR>(taddr, guided, u_given, u0, u1);
-  if (nb == 32) return tile::row_epilogue<32, LINEAR>(taddr, guided, u_given, u0, u1);
-  return tile::row_epilogue<64, LINEAR>(taddr, guided, u_given, u0, u1);
+  if (nb == 16) return tile::row_epilogue<16, LINEAR, COMP>(taddr, guided, u_given, u0, u1);
+  if (nb == 32) return tile::row_epilogue<32, LINEAR, COMP>(taddr, guided, u_given, u0, u1);
+  return tile::row_epilogue<64, LINEAR, COMP>(taddr, guided, u_given, u0, u1);
 }
 
 template <bool LINEAR>
@@ -253,7 +253,7 @@ __global__ void __launch_bounds__(128 * WGS, 1) group_fused_kernel(const __grid_
         for (int k = 0; k < 4; ++k) u[k] = u32_to_uniform(r[k]);
       }
     }
-    const tile::RowResult rt = epilogue_bins<LINEAR>(J.bins_theta, c.tmem + c.lane_base, guided, wi.x, u[0], u[1]);
+    const tile::RowResult rt = epilogue_bins<LINEAR, BF16>(J.bins_theta, c.tmem + c.lane_base, guided, wi.x, u[0], u[1]);
     const float cond = condition_bins<LINEAR>(J.bins_theta, rt.u);
     // phi input rest (SH | OneBlob | TriangleWave(u_theta) | 1-pad), layer 0
     tile::store_packed_run<14>(c.tile_a, c.row, 0, KR, phi_shob);
@@ -271,7 +271,7 @@ __global__ void __launch_bounds__(128 * WGS, 1) group_fused_kernel(const __grid_
     }
     tile::mlp_tail(c, w_phi_hidden, J.hidden_phi, static_cast<uint32_t>(J.bins_phi));
     fetch_features(s + gridDim.x);  // both feature tiles have been read
-    const tile::RowResult rp = epilogue_bins<LINEAR>(J.bins_phi, c.tmem + c.lane_base, guided, wi.y, u[2], u[3]);
+    const tile::RowResult rp = epilogue_bins<LINEAR, BF16>(J.bins_phi, c.tmem + c.lane_base, guided, wi.y, u[2], u[3]);
     if (valid)
       *reinterpret_cast<float4*>(J.wi + row * 4) = make_float4(rt.u, rp.u, wi.z * rt.pdf, wi.w * rp.pdf);
   }

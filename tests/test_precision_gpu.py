@@ -132,3 +132,27 @@ def test_errors_against_unrounded_oracle():
     assert e["fp16"]["pdf"][1] < e["bf16"]["pdf"][1] < e["fp8"]["pdf"][1]
     assert e["fp16"]["loss"] < 1e-3 and e["bf16"]["loss"] < 5e-3 and e["fp8"]["loss"] < 0.05
     assert e["fp16"]["dir"][1] < e["bf16"]["dir"][1] < e["fp8"]["dir"][1] < 1e-2
+
+
+@pytest.mark.parametrize("form", FORMS, ids=["bf16", "fp8"])
+def test_form_compensated_scans(form):
+    """The BF16 / FP8 forms keep softmax, CDF and interpolation in fp32 with
+    Neumaier-compensated sums: the FP64 normalisation check of their pdfs
+    (|1 - sum p_i / N| per row and network) stays at the few roundings left
+    after the compensated sum -- below the plain FP16 form's bound of a
+    64-term fp32 sum -- and their sampled directions still invert their
+    own CDFs (parity with the oracle of the same form is checked above)."""
+    import torch
+    prec, storage = form
+    ctx, pt, pp = make_ctx(pygdf.PRESET_FULL, seed=4, precision=prec)
+    n = 6000
+    q = dev(W.queries(n, 2))
+    wi0, guided = W.wi_init(n, 2, 0.8, 0.2)
+    wi = dev(wi0)
+    err = torch.zeros(1, dtype=torch.float64, device="cuda")
+    ctx.infer_ex(wi, queries=q, guided=dev(guided), seed=3, offset=9, norm_err=err)
+    ctx.sync()
+    e = float(err.cpu().item())
+    print(storage, "max |1 - sum p / N| with compensated sums:", e)
+    assert 0.0 <= e <= 4 * 2.0 ** -24, e
+    ctx.close()
