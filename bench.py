@@ -236,6 +236,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="CPU-baseline sample length; 0 skips it (profiling runs)")
     ap.add_argument("--skip-e2e", action="store_true", help="profiling runs: kernel timing only")
+    ap.add_argument("--queries", type=int, default=0,
+                    help="profiling runs: a smaller bounce of this many queries (0: the workload's)")
     ap.add_argument("--stages", default="infer,train,refgpu,records,forms,grouped,serve",
                     help="comma list of infer, train, records (profiling runs select one)")
     args = ap.parse_args()
@@ -244,7 +246,7 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
-    n = N_QUERIES[args.workload]
+    n = args.queries if args.queries > 0 else N_QUERIES[args.workload]
     workload_name = ("DF guided inference, 1920x1080 wavefront: hash grid 16 levels x 2 features, "
                      "2^19 entries/level, theta/phi MLP 64x4, 64 bins, linear interpolation"
                      if args.workload == "full" else
