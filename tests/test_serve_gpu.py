@@ -101,12 +101,19 @@ def test_results_same_alone_and_in_the_mix():
                 assert abs(st.loss - losses[(k, s)]) <= 1e-4 * abs(st.loss), (st.loss, losses[(k, s)])
     alone_params = [alone[2 + k].get_params(n) for k in range(2) for n in (0, 1)]
     lr = cfg.adam_df.learning_rate
-    for x, y in zip(mix_params, alone_params):
-        close = np.isclose(x, y, rtol=1e-5, atol=1e-7)
-        # measured on a B200: 98.0 % and 99.85 % of the weights in two runs
-        # (the grid gradient is a float-atomic sum whose order changes from
-        # run to run); weights of the wrong instance would agree on ~none
-        assert close.mean() >= 0.9, close.mean()
+    import oracle as O
+    d = O.df_cfg_from(cfg)
+    for i, (x, y) in enumerate(zip(mix_params, alone_params)):
+        n_mlp = O.df_mlp_params(d, i % 2)
+        # MLP matrices: fixed-order gradient reductions; they differ only
+        # through the grid weights the steps after the first saw
+        mlp = np.isclose(x[:n_mlp], y[:n_mlp], rtol=1e-5, atol=1e-7)
+        assert mlp.mean() >= 0.99, mlp.mean()
+        # grid tables: the grid gradient is a float-atomic sum whose order
+        # changes from run to run; measured on a B200: 98.0 % and 99.85 % of
+        # the entries in two runs (weights of the wrong instance agree on ~none)
+        grid = np.isclose(x[n_mlp:], y[n_mlp:], rtol=1e-5, atol=1e-7)
+        assert grid.mean() >= 0.97, grid.mean()
         # the rest: near-zero gradients whose float-atomic sum changed sign,
         # each Adam step moving the weight by at most about lr
         assert np.abs(x - y).max() <= 2 * 3 * lr, np.abs(x - y).max()
