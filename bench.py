@@ -236,6 +236,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="CPU-baseline sample length; 0 skips it (profiling runs)")
     ap.add_argument("--skip-e2e", action="store_true", help="profiling runs: kernel timing only")
+    ap.add_argument("--serve-reserve", type=int, default=0,
+                    help="serving stage: SMs training leaves to inference (gdf_server_config.train_sm_reserve)")
     ap.add_argument("--queries", type=int, default=0,
                     help="profiling runs: a smaller bounce of this many queries (0: the workload's)")
     ap.add_argument("--stages", default="infer,train,refgpu,records,forms,grouped,serve",
@@ -625,7 +627,8 @@ def time_serving(W, rank, dev, args):
         cfg.max_queries = n_max
         insts.append(pygdf.Context(cfg))
     budget = 120 * (1 << 30)
-    srv = pygdf.Server(budget, slots=SERVE_SLOTS, max_batch=32, max_train_slots=SERVE_TRAIN_SLOTS)
+    srv = pygdf.Server(budget, slots=SERVE_SLOTS, max_batch=32, max_train_slots=SERVE_TRAIN_SLOTS,
+                       train_sm_reserve=args.serve_reserve)
     for c in insts:
         srv.add_instance(c)
     q = torch.from_numpy(W.queries(n_max, 800 + rank)).to(dev)
@@ -705,7 +708,7 @@ def time_serving(W, rank, dev, args):
            "offered_load": "80 % of the batched peak", "requests": st.requests,
            "resident_gb": peak.resident_bytes / 2 ** 30, "budget_gb": budget / 2 ** 30,
            "sizes": "log-uniform 2^10..2^21 queries (training batches capped at 2^20)",
-           "mix": "1 training : 3 inference"}
+           "mix": "1 training : 3 inference", "train_sm_reserve": args.serve_reserve}
     srv.close()
     for c in insts:
         c.close()

@@ -1022,7 +1022,7 @@ static gdf::AdamParams adam_params(Context& c, int id, const gdf_adam_config& a,
   p.n = n.n_params;
   p.n_mlp = n.n_mlp;
   p.partials = c.ws.partial[id];
-  p.n_partials = c.num_sms;
+  p.n_partials = gdf::train_ctas(c);
   p.grid_grad = n.grad;
   p.master = n.master;
   p.w16 = n.w16;
@@ -1111,7 +1111,7 @@ gdf_status gdf_train_step(gdf_ctx* ctx, const float* in_theta, const float* in_p
   tf.feat_phi = c.ws.feat[1];
   cudaError_t e = gdf::launch_train_features(shape, tf, st);
   if (e != cudaSuccess) return cuda_fail(e, "train_features");
-  e = gdf::launch_df_fused(shape, gdf::kModeTrainFeat, p, c.num_sms, st);
+  e = gdf::launch_df_fused(shape, gdf::kModeTrainFeat, p, gdf::train_ctas(c), st);
   if (e != cudaSuccess) return cuda_fail(e, "df_fused (train forward)");
 
   // 2. backward of each network
@@ -1136,7 +1136,7 @@ gdf_status gdf_train_step(gdf_ctx* ctx, const float* in_theta, const float* in_p
     b.hidden = nt.hidden;
     b.err = c.d_err;
     b.gl = nt.gl;
-    e = gdf::launch_df_train_bwd(shape, id == 1, b, c.num_sms, st);
+    e = gdf::launch_df_train_bwd(shape, id == 1, b, gdf::train_ctas(c), st);
     if (e != cudaSuccess) return cuda_fail(e, "df_train_bwd");
     gdf::GridScatterParams g;
     g.in = b.in;
@@ -1252,7 +1252,7 @@ gdf_status gdf_nrc_train_step(gdf_ctx* ctx, const float* in, const float* target
   p.loss_out = c.ws.fwd;
   p.n_dropped = c.ws.dropped;
   p.err = c.d_err;
-  cudaError_t e = gdf::launch_nrc_train_bwd(p, c.num_sms, st);
+  cudaError_t e = gdf::launch_nrc_train_bwd(p, gdf::train_ctas(c), st);
   if (e != cudaSuccess) return cuda_fail(e, "nrc_train_bwd");
   gdf::AdamParams a = adam_params(c, 2, c.cfg.adam_nrc, c.cfg.nrc_loss_scale, c.ws.sq + 2 * gdf::kAdamBlocks);
   a.grid_grad = nullptr;

@@ -86,6 +86,9 @@ struct Context {
   gdf_config cfg{};
   int device = 0;
   int num_sms = 148;
+  // CTAs of the training step's persistent kernels (0: one per SM). A server
+  // that keeps SMs free for inference while training runs lowers it.
+  int train_ctas = 0;
   Net net[3];  // theta, phi, nrc
   uint32_t* d_err = nullptr;  // device error word of bounded waits
   TrainWorkspace ws;
@@ -113,6 +116,14 @@ struct Context {
   float* tool_out = nullptr;     // [tool_cap x 4]
   cudaEvent_t pipe_ev[3] = {nullptr, nullptr, nullptr};
 };
+
+// CTAs of the training step's persistent kernels (and weight-gradient partials).
+inline int train_ctas(const Context& c) {
+  return c.train_ctas > 0 && c.train_ctas < c.num_sms ? c.train_ctas : c.num_sms;
+}
+
+// The group's device error flag (set by its kernels' bounded waits).
+uint32_t* group_err_flag(gdf_group* g);
 
 // Sets the thread-local message returned by gdf_last_error().
 void set_last_error(const char* msg);

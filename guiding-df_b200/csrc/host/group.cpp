@@ -2,6 +2,7 @@
 // grid-feature launch and one persistent fused launch for all jobs,
 // replayed from a CUDA graph, with the warpgroups per CTA and the feature
 // kernel's block size chosen by timing the candidates on the job set.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -42,6 +43,10 @@ struct Plan {
   // the feature launch, whose grid follows the call's row count
   cudaGraphNode_t feat_node = nullptr;
   cudaKernelNodeParams feat_params{};
+  // the fused launch, whose grid follows the group's SM cap
+  cudaGraphNode_t fused_node = nullptr;
+  cudaKernelNodeParams fused_params{};
+  unsigned fused_grid = 0;  // as captured: one CTA per SM
 };
 
 }  // namespace
@@ -49,6 +54,7 @@ struct Plan {
 struct gdf_group {
   int device = 0;
   int num_sms = 148;
+  int sm_cap = 0;  // CTAs of the fused launch (0: one per SM)
   int32_t max_jobs = 0;
   gdf::GroupHeader* d_hdr = nullptr;
   gdf::GroupJobDev* d_jobs = nullptr;
@@ -242,6 +248,15 @@ gdf_status get_plan(gdf_group* g, const JobSet& js, int wgs, int fblock, size_t*
   cudaError_t e4 = cudaGraphGetRootNodes(graph, &p.feat_node, &n_roots);
   if (e4 == cudaSuccess && n_roots != 1) e4 = cudaErrorInvalidValue;
   if (e4 == cudaSuccess) e4 = cudaGraphKernelNodeGetParams(p.feat_node, &p.feat_params);
+  if (e4 == cudaSuccess) {
+    cudaGraphNode_t nodes[2];
+    size_t n_nodes = 2;
+    e4 = cudaGraphGetNodes(graph, nodes, &n_nodes);
+    if (e4 == cudaSuccess && n_nodes != 2) e4 = cudaErrorInvalidValue;
+    if (e4 == cudaSuccess) p.fused_node = nodes[0] == p.feat_node ? nodes[1] : nodes[0];
+    if (e4 == cudaSuccess) e4 = cudaGraphKernelNodeGetParams(p.fused_node, &p.fused_params);
+    p.fused_grid = p.fused_params.gridDim.x;
+  }
   if (e4 == cudaSuccess) e4 = cudaGraphInstantiate(&p.exec, graph, 0);
   if (e4 != cudaSuccess) {
     cudaGraphDestroy(graph);
@@ -267,6 +282,11 @@ gdf_status launch_plan(gdf_group* g, size_t plan, const JobSet& js, cudaStream_t
   Plan& p = g->plans[plan];
   p.feat_params.gridDim = dim3(static_cast<unsigned>(feature_blocks(js, p.fblock)));
   GDF_GCUDA(cudaGraphExecKernelNodeSetParams(p.exec, p.feat_node, &p.feat_params));
+  const unsigned grid = g->sm_cap > 0 ? std::min(p.fused_grid, static_cast<unsigned>(g->sm_cap)) : p.fused_grid;
+  if (p.fused_params.gridDim.x != grid) {
+    p.fused_params.gridDim = dim3(grid);
+    GDF_GCUDA(cudaGraphExecKernelNodeSetParams(p.exec, p.fused_node, &p.fused_params));
+  }
   GDF_GCUDA(cudaGraphLaunch(p.exec, st));
   GDF_GCUDA(cudaEventRecord(g->last_launch, st));
   g->launched = true;
@@ -290,6 +310,13 @@ gdf_status autotune(gdf_group* g, const gdf_job* jobs, int32_t n, const JobSet& 
     }
     g->tune_cap = total;
   }
+  // candidates are timed on the whole device, whatever the launch cap
+  struct Uncap {
+    gdf_group* g;
+    int cap;
+    ~Uncap() { g->sm_cap = cap; }
+  } uncap{g, g->sm_cap};
+  g->sm_cap = 0;
   const std::pair<int, int> cand[4] = {{4, 256}, {4, 128}, {2, 256}, {2, 128}};
   cudaEvent_t a, b;
   GDF_GCUDA(cudaEventCreate(&a));
@@ -432,6 +459,13 @@ gdf_status gdf_group_tuning(const gdf_group* g, int32_t* warpgroups, int32_t* fe
   return GDF_OK;
 }
 
+gdf_status gdf_group_set_sm_cap(gdf_group* g, int32_t ctas) {
+  if (!g) return gfail(GDF_ERR_INVALID_ARG, "null group");
+  if (ctas < 0) return gfail(GDF_ERR_INVALID_ARG, "ctas must be >= 0");
+  g->sm_cap = ctas;
+  return GDF_OK;
+}
+
 gdf_status gdf_group_sync_status(gdf_group* g, void* stream) {
   if (!g) return gfail(GDF_ERR_INVALID_ARG, "null group");
   GDF_GCUDA(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
@@ -445,3 +479,9 @@ gdf_status gdf_group_sync_status(gdf_group* g, void* stream) {
 }
 
 }  // extern "C"
+
+namespace gdf {
+
+uint32_t* group_err_flag(gdf_group* g) { return g->d_err; }
+
+}  // namespace gdf

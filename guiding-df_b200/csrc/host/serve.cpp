@@ -48,18 +48,21 @@ struct Request {
   int slot = -1;
   int64_t transient = 0;
   gdf_status status = GDF_OK;
+  std::string msg;  // what failed, when status is not GDF_OK
   gdf_train_stats stats{};
 };
 
-struct TrainOut {  // pinned: loss sum, squared gradient norm, dropped records
+struct SlotOut {  // pinned: a training request's loss sum, squared gradient
+                  // norm and dropped records; the slot's device error flag
   double stats[2];
   unsigned long long dropped;
+  uint32_t dev_err;
 };
 
 struct Slot {
   cudaStream_t stream = nullptr;
   cudaEvent_t done = nullptr;
-  TrainOut* out = nullptr;     // statistics of a training request on this slot
+  SlotOut* out = nullptr;      // read back when the slot's work ends
   gdf_group* group = nullptr;  // grouped inference launches on this slot
   std::vector<Request*> reqs;  // requests whose work ends at `done`
   bool busy = false;
@@ -94,6 +97,12 @@ int64_t transient_bytes(const gdf_request& r) {
   // grouped feature tiles for inference (2 networks x 64 B per query at the
   // full configuration); the training step uses its context's workspace
   return r.kind == GDF_REQ_INFER ? (r.n + 127) / 128 * 128 * 128 : 0;
+}
+
+// Copies a device error flag to pinned memory and clears it, in stream order.
+void read_and_clear(uint32_t* d_flag, uint32_t* h_flag, cudaStream_t st) {
+  cudaMemcpyAsync(h_flag, d_flag, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+  cudaMemsetAsync(d_flag, 0, sizeof(uint32_t), st);
 }
 
 // Issues one round of admitted work. Holds the lock.
@@ -139,11 +148,17 @@ void admit(gdf_server* s) {
     Slot& sl = s->slots[free_slots[used_slots++]];
     q->slot = static_cast<int>(&sl - s->slots.data());
     gdf_ctx* inst = q->r.instance;
+    // training's persistent kernels leave train_sm_reserve SMs to inference
+    inst->c.train_ctas = s->cfg.train_sm_reserve > 0 ? inst->c.num_sms - s->cfg.train_sm_reserve : 0;
     q->status = gdf_train_step(inst, q->r.in_theta_dev, q->r.in_phi_dev, q->r.target_dev, q->r.n, nullptr, sl.stream);
-    // the step's FP64 statistics, read back without blocking the scheduler
+    inst->c.train_ctas = 0;
+    if (q->status) q->msg = gdf_last_error();
+    // the step's FP64 statistics and the instance's device error flag, read
+    // back without blocking the scheduler
     cudaMemcpyAsync(sl.out->stats, inst->c.ws.stats, sizeof(sl.out->stats), cudaMemcpyDeviceToHost, sl.stream);
     cudaMemcpyAsync(&sl.out->dropped, inst->c.ws.dropped, sizeof(sl.out->dropped), cudaMemcpyDeviceToHost,
                     sl.stream);
+    read_and_clear(inst->c.d_err, &sl.out->dev_err, sl.stream);
     sl.reqs.assign(1, q);
     sl.busy = true;
     s->train_busy += 1;
@@ -157,8 +172,17 @@ void admit(gdf_server* s) {
       jobs[k] = gdf_job{r.instance, r.queries_dev, r.guided_dev, r.uniforms_dev, r.philox_seed,
                         r.philox_offset, r.wi_dev, r.n};
     }
+    // while training runs, inference takes the SMs training leaves free;
+    // a grouped launch keeps its CTA count to the end, so later requests get
+    // the whole device again once training is done
+    gdf_group_set_sm_cap(sl.group, s->cfg.train_sm_reserve > 0 && s->train_busy > 0 ? s->cfg.train_sm_reserve : 0);
     const gdf_status st = gdf_group_infer(sl.group, jobs.data(), static_cast<int32_t>(jobs.size()), sl.stream);
-    for (Request* q : infer) q->status = st;
+    const std::string msg = st ? gdf_last_error() : "";
+    for (Request* q : infer) {
+      q->status = st;
+      q->msg = msg;
+    }
+    read_and_clear(gdf::group_err_flag(sl.group), &sl.out->dev_err, sl.stream);
     sl.reqs = infer;
     sl.busy = true;
     cudaEventRecord(sl.done, sl.stream);
@@ -174,7 +198,13 @@ bool complete(gdf_server* s) {
     if (e == cudaErrorNotReady) continue;
     const Clock::time_point now = Clock::now();
     for (Request* q : sl.reqs) {
-      if (e != cudaSuccess && q->status == GDF_OK) q->status = GDF_ERR_CUDA;
+      if (e != cudaSuccess && q->status == GDF_OK) {
+        q->status = GDF_ERR_CUDA;
+        q->msg = cudaGetErrorString(e);
+      } else if (sl.out->dev_err != 0u && q->status == GDF_OK) {
+        q->status = GDF_ERR_TIMEOUT;
+        q->msg = "a bounded device wait gave up (code " + std::to_string(sl.out->dev_err) + ")";
+      }
       if (q->r.kind == GDF_REQ_TRAIN) {
         s->train_busy -= 1;
         q->stats.loss = sl.out->stats[0] / static_cast<double>(q->r.n);
@@ -219,9 +249,10 @@ extern "C" {
 gdf_status gdf_server_create(const gdf_server_config* cfg, gdf_server** out) {
   if (!cfg || !out) return sfail(GDF_ERR_INVALID_ARG, "null config / output");
   if (cfg->slots < 1 || cfg->slots > 64 || cfg->max_batch < 1 || cfg->max_batch > 4096 ||
-      cfg->max_train_slots < 0 || cfg->hbm_budget_bytes <= 0)
+      cfg->max_train_slots < 0 || cfg->hbm_budget_bytes <= 0 || cfg->train_sm_reserve < 0)
     return sfail(GDF_ERR_INVALID_ARG,
-                 "slots in [1, 64], max_batch in [1, 4096], max_train_slots >= 0, positive budget");
+                 "slots in [1, 64], max_batch in [1, 4096], max_train_slots >= 0, positive budget, "
+                 "train_sm_reserve >= 0");
   *out = nullptr;
   gdf_server* s = new (std::nothrow) gdf_server();
   if (!s) return sfail(GDF_ERR_OOM_BUDGET, "host allocation failed");
@@ -232,12 +263,18 @@ gdf_status gdf_server_create(const gdf_server_config* cfg, gdf_server** out) {
     delete s;
     return sfail(GDF_ERR_CUDA, "cudaSetDevice");
   }
+  int n_sms = 0;
+  cudaDeviceGetAttribute(&n_sms, cudaDevAttrMultiProcessorCount, cfg->device);
+  if (cfg->train_sm_reserve >= n_sms) {
+    delete s;
+    return sfail(GDF_ERR_INVALID_ARG, "train_sm_reserve must leave training at least one SM");
+  }
   s->slots.resize(static_cast<size_t>(cfg->slots));
   for (Slot& sl : s->slots) {
     gdf_status st;
     if (cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) != cudaSuccess ||
-        cudaMallocHost(&sl.out, sizeof(TrainOut)) != cudaSuccess) {
+        cudaMallocHost(&sl.out, sizeof(SlotOut)) != cudaSuccess) {
       gdf_server_destroy(s);
       return sfail(GDF_ERR_CUDA, "server streams");
     }
@@ -328,9 +365,10 @@ gdf_status gdf_server_wait(gdf_server* s, uint64_t ticket, gdf_train_stats* stat
   if (stats) *stats = q->stats;
   if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(q->t_done - q->t_submit).count();
   const gdf_status st = q->status;
+  const std::string msg = q->msg;
   s->all.erase(it);
   delete q;
-  if (st) return sfail(st, "request failed on the device");
+  if (st) return sfail(st, "request failed: " + msg);
   return GDF_OK;
 }
 

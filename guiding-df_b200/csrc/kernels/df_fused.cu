@@ -27,6 +27,7 @@
 #include "../device/records.cuh"
 #include "../device/sm100.cuh"
 #include "df_kernels.h"
+#include "launch_util.h"
 
 namespace gdf {
 namespace {
@@ -420,8 +421,7 @@ cudaError_t launch_t(int mode, const DfKernelParams& p, size_t smem, int num_sms
                          df_fused_kernel<L, F, NBT, NBP, LIN, kModeEval, kDfWarpgroups, 2>)
               : mode == kModeTrainFeat ? df_fused_kernel<L, F, NBT, NBP, LIN, kModeTrainFeat, kDfWarpgroups, 0>
                                        : df_fused_kernel<L, F, NBT, NBP, LIN, kModeTrainFwd, kDfWarpgroups, 0>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(smem));
+  cudaError_t e = allow_dynamic_smem(kern);
   if (e != cudaSuccess) return e;
   kern<<<static_cast<unsigned>(ctas), kDfThreads, smem, st>>>(p);
   return cudaGetLastError();

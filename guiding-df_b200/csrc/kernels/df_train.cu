@@ -33,6 +33,7 @@
 #include "../device/train_tile.cuh"
 #include "df_kernels.h"
 #include "train_kernels.h"
+#include "launch_util.h"
 
 namespace gdf {
 namespace {
@@ -412,7 +413,7 @@ cudaError_t launch_bwd_t(const DfBwdParams& p, int ctas, cudaStream_t st) {
   const size_t smem = ((p.blob_bytes + 127u) & ~127u) + 128u * K0 * 2u +
                       static_cast<size_t>(p.hidden + 1) * 128u * 64u * 2u + 64u;
   auto k = df_train_bwd_kernel<L, F, NB, LIN, PHI>;
-  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  cudaError_t e = allow_dynamic_smem(k);
   if (e != cudaSuccess) return e;
   k<<<ctas, 128, smem, st>>>(p);
   return cudaGetLastError();
@@ -754,8 +755,7 @@ cudaError_t launch_adam_lr_table(float lr, float beta1, float beta2, float* tabl
 
 cudaError_t launch_adam_ema(const AdamParams& p, cudaStream_t st) {
   if (p.n <= 0) return cudaSuccess;
-  cudaError_t e = cudaFuncSetAttribute(adam_ema_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(kAdamSmem));
+  cudaError_t e = allow_dynamic_smem(adam_ema_kernel);
   if (e != cudaSuccess) return e;
   adam_ema_kernel<<<p.n_blocks, 256, kAdamSmem, st>>>(p);
   return cudaGetLastError();

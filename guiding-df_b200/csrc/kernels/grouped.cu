@@ -22,6 +22,7 @@
 #include "../device/df_tile.cuh"
 #include "../device/sm100.cuh"
 #include "group_kernels.h"
+#include "launch_util.h"
 
 namespace gdf {
 namespace {
@@ -292,7 +293,7 @@ cudaError_t features_l(const GroupShape& s, const GroupParams& p, int blocks, in
 template <int L, int F, bool LIN, int WGS>
 cudaError_t fused_l(bool bf16, const GroupParams& p, size_t smem, int ctas, cudaStream_t st) {
   auto kern = bf16 ? group_fused_kernel<L, F, LIN, WGS, true> : group_fused_kernel<L, F, LIN, WGS, false>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  cudaError_t e = allow_dynamic_smem(kern);
   if (e != cudaSuccess) return e;
   kern<<<ctas, 128 * WGS, smem, st>>>(p);
   return cudaGetLastError();

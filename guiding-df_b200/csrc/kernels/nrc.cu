@@ -20,6 +20,7 @@
 #include "../device/sm100.cuh"
 #include "../device/train_tile.cuh"
 #include "nrc_kernels.h"
+#include "launch_util.h"
 
 namespace gdf {
 namespace {
@@ -315,8 +316,7 @@ __global__ void __launch_bounds__(128, 1) nrc_train_bwd_kernel(const __grid_cons
 cudaError_t launch_nrc_query(const NrcParams& p, int num_sms, cudaStream_t st) {
   if (p.n <= 0) return cudaSuccess;
   const size_t smem = ((p.blob_bytes + 127u) & ~127u) + kNrcWgs * 128u * kNrcK0 * 2u + 8u * (kNrcWgs + 1) + 16u;
-  cudaError_t e = cudaFuncSetAttribute(nrc_query_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(smem));
+  cudaError_t e = allow_dynamic_smem(nrc_query_kernel);
   if (e != cudaSuccess) return e;
   const int64_t tiles = (p.n + 127) / 128;
   int64_t ctas = (tiles + kNrcWgs - 1) / kNrcWgs;
@@ -329,8 +329,7 @@ cudaError_t launch_nrc_train_bwd(const NrcTrainParams& p, int ctas, cudaStream_t
   if (p.n <= 0) return cudaSuccess;
   const size_t smem = ((p.blob_bytes + 127u) & ~127u) + 128u * kNrcK0 * 2u +
                       static_cast<size_t>(p.hidden + 1) * 128u * 64u * 2u + 64u;
-  cudaError_t e = cudaFuncSetAttribute(nrc_train_bwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(smem));
+  cudaError_t e = allow_dynamic_smem(nrc_train_bwd_kernel);
   if (e != cudaSuccess) return e;
   nrc_train_bwd_kernel<<<ctas, 128, smem, st>>>(p);
   return cudaGetLastError();

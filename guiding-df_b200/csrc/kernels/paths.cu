@@ -13,6 +13,7 @@
 
 #include "../device/records.cuh"
 #include "paths_kernels.h"
+#include "launch_util.h"
 
 namespace gdf {
 namespace {
@@ -459,8 +460,7 @@ cudaError_t produce(const ProduceParams& p, cudaStream_t st) {
   produce_mask_kernel<KIND><<<static_cast<unsigned>(nb), kProduceBlock, 0, st>>>(p);
   scan_blocks_kernel<<<1, kScanThreads, 0, st>>>(p.block_counts, p.block_offsets, p.totals, nb);
   constexpr size_t smem = emit_smem_bytes<KIND>();
-  cudaError_t e = cudaFuncSetAttribute(produce_emit_kernel<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(smem));
+  cudaError_t e = allow_dynamic_smem(produce_emit_kernel<KIND>);
   if (e != cudaSuccess) return e;
   produce_emit_kernel<KIND><<<static_cast<unsigned>(nb), kProduceBlock, smem, st>>>(p);
   return cudaGetLastError();

@@ -127,7 +127,8 @@ class Request(C.Structure):
 
 class ServerConfig(C.Structure):
     _fields_ = [("device", C.c_int32), ("slots", C.c_int32), ("max_batch", C.c_int32),
-                ("max_train_slots", C.c_int32), ("hbm_budget_bytes", C.c_int64)]
+                ("max_train_slots", C.c_int32), ("hbm_budget_bytes", C.c_int64),
+                ("train_sm_reserve", C.c_int32)]
 
 
 class ServerStats(C.Structure):
@@ -187,6 +188,7 @@ def lib() -> C.CDLL:
             "gdf_group_tuning": [P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), P],
             "gdf_group_sync_status": [P, P],
             "gdf_group_set_shape": [P, C.c_int32, C.c_int32],
+            "gdf_group_set_sm_cap": [P, C.c_int32],
             "gdf_ctx_bytes": [P, C.POINTER(C.c_int64)],
             "gdf_server_create": [C.POINTER(ServerConfig), C.POINTER(C.c_void_p)],
             "gdf_server_destroy": [P],
@@ -470,6 +472,12 @@ class Group:
             a.n = j.get("n", j["queries"].shape[0])
         check(lib().gdf_group_infer(self.h, arr, len(jobs), _stream(stream)))
 
+    def set_shape(self, warpgroups: int, feature_block: int):
+        check(lib().gdf_group_set_shape(self.h, warpgroups, feature_block))
+
+    def set_sm_cap(self, ctas: int):
+        check(lib().gdf_group_set_sm_cap(self.h, ctas))
+
     def tuning(self):
         import numpy as np
         w, b = C.c_int32(), C.c_int32()
@@ -505,8 +513,8 @@ class Server:
     """gdf_server: resident instances, continuous admission and batching."""
 
     def __init__(self, budget_bytes: int, slots: int = 4, max_batch: int = 16, device: int = 0,
-                 max_train_slots: int = 0):
-        cfg = ServerConfig(device, slots, max_batch, max_train_slots, budget_bytes)
+                 max_train_slots: int = 0, train_sm_reserve: int = 0):
+        cfg = ServerConfig(device, slots, max_batch, max_train_slots, budget_bytes, train_sm_reserve)
         h = C.c_void_p()
         check(lib().gdf_server_create(C.byref(cfg), C.byref(h)))
         self.h = h

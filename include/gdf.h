@@ -390,6 +390,11 @@ gdf_status gdf_group_tuning(const gdf_group* g, int32_t* warpgroups, int32_t* fe
  * and skips tuning; warpgroups = 0 returns to tuning. */
 gdf_status gdf_group_set_shape(gdf_group* g, int32_t warpgroups, int32_t feature_block);
 
+/* Caps the CTAs of the group's persistent fused launches at `ctas` (0: one
+ * per SM, the default), so that later calls leave the other SMs to work on
+ * other streams; results do not depend on the cap. */
+gdf_status gdf_group_set_sm_cap(gdf_group* g, int32_t ctas);
+
 /* gdf_sync_status for the group's kernels. */
 gdf_status gdf_group_sync_status(gdf_group* g, void* stream);
 
@@ -425,6 +430,9 @@ typedef struct gdf_server_config {
   int32_t max_batch;          /* inference requests per grouped launch        */
   int32_t max_train_slots;    /* slots training may hold at once (0: slots-1) */
   int64_t hbm_budget_bytes;   /* resident instances + in-flight requests      */
+  int32_t train_sm_reserve;   /* SMs training's persistent kernels leave free,
+                                 and the CTAs inference launches get while
+                                 training runs (0: none reserved)            */
 } gdf_server_config;
 
 typedef struct gdf_server_stats {

@@ -69,3 +69,31 @@ def test_group_equals_separate_calls():
     g.close()
     for c in ctxs:
         c.close()
+
+
+def test_sm_cap_keeps_results_across_plans():
+    """A capped fused launch gives the same rows. The cap is applied to each
+    captured graph when it is replayed; the plan with 64-bin jobs (the most
+    shared memory) is replayed capped after a plan of 32-bin jobs only was
+    captured, which must not invalidate its launch."""
+    ctxs = _contexts()
+    g = pygdf.Group(max_jobs=16)
+    g.set_shape(4, 256)
+    big = _jobs(ctxs, [9000, 7000, 5000, 3000, 2000, 1000], seed=70)
+    g.infer(big)
+    small = _jobs(ctxs[1::2], [4000, 3000, 2000], seed=80)  # 32-bin jobs only
+    g.infer(small)
+    g.sync()
+    _check(big)
+    _check(small)
+    for cap in (20, 1, 0):
+        g.set_sm_cap(cap)
+        again = _jobs(ctxs, [9000, 7000, 5000, 3000, 2000, 1000], seed=90 + cap)
+        g.infer(again)
+        g.sync()
+        _check(again)
+    with pytest.raises(pygdf.GdfError):
+        g.set_sm_cap(-1)
+    g.close()
+    for c in ctxs:
+        c.close()
