@@ -137,7 +137,7 @@ gdf_status dalloc(T** p, size_t n) {
 void free_net(Net& n) {
   cudaFree(n.master); cudaFree(n.w16); cudaFree(n.ema16); cudaFree(n.adam_m);
   cudaFree(n.adam_v); cudaFree(n.adam_step); cudaFree(n.grad); cudaFree(n.blob_ema);
-  cudaFree(n.blob_w16); cudaFree(n.blob_f8);
+  cudaFree(n.blob_w16); cudaFree(n.blob_f8); cudaFree(n.opt);
   n = Net{};
 }
 
@@ -195,7 +195,7 @@ gdf_status alloc_net(Net& n) {
   const size_t np = static_cast<size_t>(n.n_params);
   if ((s = dalloc(&n.master, np)) || (s = dalloc(&n.w16, np)) || (s = dalloc(&n.ema16, np)) ||
       (s = dalloc(&n.adam_m, np)) || (s = dalloc(&n.adam_v, np)) ||
-      (s = dalloc(&n.adam_step, np)) || (s = dalloc(&n.grad, np)) ||
+      (s = dalloc(&n.adam_step, np)) || (s = dalloc(&n.grad, np)) || (s = dalloc(&n.opt, 1)) ||
       (s = dalloc(&n.blob_ema, static_cast<size_t>(n.n_mlp))) ||
       (s = dalloc(&n.blob_w16, static_cast<size_t>(n.n_mlp))))
     return s;
@@ -252,7 +252,7 @@ gdf_status init_params(Net& n, uint32_t seed, uint32_t stream_id) {
   GDF_CUDA(cudaMemset(n.adam_v, 0, h.size() * 4));
   GDF_CUDA(cudaMemset(n.adam_step, 0, h.size() * 4));
   GDF_CUDA(cudaMemset(n.grad, 0, h.size() * 4));
-  n.opt_step = 0;
+  GDF_CUDA(cudaMemset(n.opt, 0, sizeof(gdf::OptState)));
   return upload_params(n, h);
 }
 
@@ -313,6 +313,10 @@ void free_pw(gdf::PathWorkspace& w) {
   cudaFree(w.nrc_out);
   cudaFree(w.nrc_train_in);
   cudaFree(w.nrc_train_target);
+  cudaFree(w.plan);
+  cudaFree(w.loss_acc);
+  cudaFree(w.frame_loss);
+  cudaFree(w.frame_n);
   w = gdf::PathWorkspace{};
 }
 
@@ -1015,7 +1019,7 @@ gdf_status gdf_post_inference(gdf_ctx* ctx, const float* lt, const float* lp, co
 }
 
 static gdf::AdamParams adam_params(Context& c, int id, const gdf_adam_config& a, float loss_scale,
-                                    double* sq) {
+                                    double* sq, const int64_t* n_dev = nullptr) {
   Net& n = c.net[id];
   gdf::AdamParams p;
   std::memset(&p, 0, sizeof(p));
@@ -1039,9 +1043,9 @@ static gdf::AdamParams adam_params(Context& c, int id, const gdf_adam_config& a,
     p.layer_cols[l] = n.cols[l];
     off += static_cast<int64_t>(n.rows[l]) * n.cols[l];
   }
-  // AdamOptimizer::step increments its step before use (adam.h:150-152);
-  // EmaOptimizer::step debiases with that step (ema.h:102-110).
-  const uint32_t step = ++n.opt_step;
+  // the step counter lives on the device; the optimizer kernel advances it
+  p.opt = n.opt;
+  p.n_dev = n_dev;
   p.loss_scale = loss_scale;
   p.lr = a.learning_rate;
   p.beta1 = a.beta1;
@@ -1049,8 +1053,6 @@ static gdf::AdamParams adam_params(Context& c, int id, const gdf_adam_config& a,
   p.eps = a.epsilon;
   p.l2_reg = a.l2_reg;
   p.ema_decay = a.ema_decay;
-  p.debias_old = 1.0f - static_cast<float>(std::pow(static_cast<double>(a.ema_decay), static_cast<double>(step - 1)));
-  p.debias_new = 1.0f / (1.0f - static_cast<float>(std::pow(static_cast<double>(a.ema_decay), static_cast<double>(step))));
   p.sq_partial = sq;
   p.n_blocks = gdf::kAdamBlocks;
   if (id < 2) {
@@ -1065,17 +1067,17 @@ static gdf::AdamParams adam_params(Context& c, int id, const gdf_adam_config& a,
   return p;
 }
 
-gdf_status gdf_train_step(gdf_ctx* ctx, const float* in_theta, const float* in_phi,
-                          const float* target, int64_t n, gdf_train_stats* stats, void* stream) {
-  if (!ctx) return fail(GDF_ERR_INVALID_ARG, "ctx is null");
-  Context& c = ctx->c;
-  if (n <= 0) return fail(GDF_ERR_INVALID_ARG, "n must be positive");
-  if (n > c.ws.capacity) return fail(GDF_ERR_INVALID_ARG, "n exceeds max_train_batch");
-  gdf_status s;
-  if ((s = check_ptr(in_theta, "in_theta")) || (s = check_ptr(in_phi, "in_phi")) ||
-      (s = check_ptr(target, "target")))
-    return s;
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
+}  // extern "C"
+
+namespace {
+
+// One DF training step (learnedDistribution.cpp:247-288), stream-ordered.
+// With n_dev set the batch holds min(*n_dev, n) records, read on the device
+// (n bounds the launches), and an empty batch leaves every weight and the
+// optimizer step counter untouched; loss_acc (nullable) gets the batch's
+// mean loss added on the device.
+gdf_status train_step_dev(Context& c, const float* in_theta, const float* in_phi, const float* target,
+                          int64_t n, const int64_t* n_dev, double* loss_acc, cudaStream_t st) {
   const gdf::DfShape shape = df_shape(c);
   GDF_CUDA(cudaMemsetAsync(c.ws.dropped, 0, sizeof(unsigned long long), st));
 
@@ -1096,12 +1098,16 @@ gdf_status gdf_train_step(gdf_ctx* ctx, const float* in_theta, const float* in_p
   p.train_out = c.ws.fwd;
   p.n_dropped = c.ws.dropped;
   p.loss_scale_per_record = c.cfg.loss_scale / static_cast<float>(n);
+  p.loss_scale = c.cfg.loss_scale;
+  p.n_dev = n_dev;
   p.n = n;
   gdf::TrainFeatParams tf;
+  std::memset(&tf, 0, sizeof(tf));
   tf.in_theta = in_theta;
   tf.in_phi = in_phi;
   tf.target = target;
   tf.n = n;
+  tf.n_dev = n_dev;
   tf.n_tiles = (n + 127) / 128;
   tf.grid_theta = p.grid_theta;
   tf.grid_phi = p.grid_phi;
@@ -1124,6 +1130,7 @@ gdf_status gdf_train_step(gdf_ctx* ctx, const float* in_theta, const float* in_p
     b.target = target;
     b.fwd = c.ws.fwd;
     b.n = n;
+    b.n_dev = n_dev;
     b.blob = nt.blob_w16;
     b.blob_bytes = nt.blob_bytes;
     b.grid = nt.w16 + nt.n_mlp;
@@ -1139,10 +1146,12 @@ gdf_status gdf_train_step(gdf_ctx* ctx, const float* in_theta, const float* in_p
     e = gdf::launch_df_train_bwd(shape, id == 1, b, gdf::train_ctas(c), st);
     if (e != cudaSuccess) return cuda_fail(e, "df_train_bwd");
     gdf::GridScatterParams g;
+    std::memset(&g, 0, sizeof(g));
     g.in = b.in;
     g.in_stride = b.in_stride;
     g.fwd = c.ws.fwd;
     g.n = n;
+    g.n_dev = n_dev;
     g.dx = c.ws.dx;
     g.dx_rows = c.ws.capacity;
     g.grid_grad = b.grid_grad;
@@ -1153,7 +1162,7 @@ gdf_status gdf_train_step(gdf_ctx* ctx, const float* in_theta, const float* in_p
   // 3. Adam + EMA, re-layout of the weights
   for (int id = 0; id < 2; ++id) {
     gdf::AdamParams a = adam_params(c, id, c.cfg.adam_df, c.cfg.loss_scale,
-                                    c.ws.sq + static_cast<size_t>(id) * gdf::kAdamBlocks);
+                                    c.ws.sq + static_cast<size_t>(id) * gdf::kAdamBlocks, n_dev);
     a.grid_grad = c.net[id].grad + c.net[id].n_mlp;
     e = gdf::launch_adam_ema(a, st);
     if (e != cudaSuccess) return cuda_fail(e, "adam_ema");
@@ -1161,8 +1170,28 @@ gdf_status gdf_train_step(gdf_ctx* ctx, const float* in_theta, const float* in_p
       return cuda_fail(e, "pack fp8");
   }
   // 4. FP64 loss and gradient-norm reductions
-  e = gdf::launch_train_stats_mb(c.ws.fwd, n, c.ws.sq, 2 * gdf::kAdamBlocks, c.ws.stat_part, c.ws.stats, st);
+  e = gdf::launch_train_stats_mb(c.ws.fwd, n, n_dev, c.ws.sq, 2 * gdf::kAdamBlocks, c.ws.stat_part, c.ws.stats,
+                                 loss_acc, st);
   if (e != cudaSuccess) return cuda_fail(e, "train_stats");
+  return GDF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+gdf_status gdf_train_step(gdf_ctx* ctx, const float* in_theta, const float* in_phi,
+                          const float* target, int64_t n, gdf_train_stats* stats, void* stream) {
+  if (!ctx) return fail(GDF_ERR_INVALID_ARG, "ctx is null");
+  Context& c = ctx->c;
+  if (n <= 0) return fail(GDF_ERR_INVALID_ARG, "n must be positive");
+  if (n > c.ws.capacity) return fail(GDF_ERR_INVALID_ARG, "n exceeds max_train_batch");
+  gdf_status s;
+  if ((s = check_ptr(in_theta, "in_theta")) || (s = check_ptr(in_phi, "in_phi")) ||
+      (s = check_ptr(target, "target")))
+    return s;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if ((s = train_step_dev(c, in_theta, in_phi, target, n, nullptr, nullptr, st))) return s;
   if (stats) {
     double h[2];
     unsigned long long dropped = 0;
@@ -1186,7 +1215,11 @@ gdf_status gdf_get_optimizer_state(const gdf_ctx* ctx, int32_t net, float* m, fl
   if (m) GDF_CUDA(cudaMemcpy(m, nt->adam_m, static_cast<size_t>(n) * 4, cudaMemcpyDeviceToHost));
   if (v) GDF_CUDA(cudaMemcpy(v, nt->adam_v, static_cast<size_t>(n) * 4, cudaMemcpyDeviceToHost));
   if (steps) GDF_CUDA(cudaMemcpy(steps, nt->adam_step, static_cast<size_t>(n) * 4, cudaMemcpyDeviceToHost));
-  if (opt_step) *opt_step = nt->opt_step;
+  if (opt_step) {
+    gdf::OptState o;
+    GDF_CUDA(cudaMemcpy(&o, nt->opt, sizeof(o), cudaMemcpyDeviceToHost));
+    *opt_step = o.step;
+  }
   return GDF_OK;
 }
 
@@ -1198,7 +1231,7 @@ gdf_status gdf_set_optimizer_state(gdf_ctx* ctx, int32_t net, const float* m, co
   if (m) GDF_CUDA(cudaMemcpy(nt->adam_m, m, static_cast<size_t>(n) * 4, cudaMemcpyHostToDevice));
   if (v) GDF_CUDA(cudaMemcpy(nt->adam_v, v, static_cast<size_t>(n) * 4, cudaMemcpyHostToDevice));
   if (steps) GDF_CUDA(cudaMemcpy(nt->adam_step, steps, static_cast<size_t>(n) * 4, cudaMemcpyHostToDevice));
-  nt->opt_step = opt_step;
+  GDF_CUDA(cudaMemcpy(&nt->opt->step, &opt_step, sizeof(opt_step), cudaMemcpyHostToDevice));
   GDF_CUDA(cudaDeviceSynchronize());
   return GDF_OK;
 }
@@ -1258,8 +1291,8 @@ gdf_status gdf_nrc_train_step(gdf_ctx* ctx, const float* in, const float* target
   a.grid_grad = nullptr;
   e = gdf::launch_adam_ema(a, st);
   if (e != cudaSuccess) return cuda_fail(e, "adam_ema (nrc)");
-  e = gdf::launch_train_stats_mb(c.ws.fwd, m, c.ws.sq + 2 * gdf::kAdamBlocks, gdf::kAdamBlocks, c.ws.stat_part,
-                                 c.ws.stats, st);
+  e = gdf::launch_train_stats_mb(c.ws.fwd, m, nullptr, c.ws.sq + 2 * gdf::kAdamBlocks, gdf::kAdamBlocks,
+                                 c.ws.stat_part, c.ws.stats, nullptr, st);
   if (e != cudaSuccess) return cuda_fail(e, "train_stats (nrc)");
   if (stats) {
     double h[2];
@@ -1341,6 +1374,21 @@ gdf_status ensure_df_records(Context& c, int64_t cap) {
   return GDF_OK;
 }
 
+gdf_status ensure_plan(Context& c, int32_t batches) {
+  gdf::PathWorkspace& w = c.pw;
+  gdf_status s;
+  if (!w.loss_acc && ((s = dalloc(&w.loss_acc, 1)) || (s = dalloc(&w.frame_loss, 1)) ||
+                      (s = dalloc(&w.frame_n, 1))))
+    return s;
+  if (batches <= w.plan_len && w.plan) return GDF_OK;
+  cudaFree(w.plan);
+  w.plan = nullptr;
+  w.plan_len = 0;
+  if ((s = dalloc(&w.plan, static_cast<size_t>(batches) + 1))) return s;
+  w.plan_len = batches;
+  return GDF_OK;
+}
+
 gdf_status ensure_nrc_rows(Context& c, int64_t cap) {
   gdf::PathWorkspace& w = c.pw;
   if (cap <= w.nrc_cap) return GDF_OK;
@@ -1365,9 +1413,9 @@ gdf_status ensure_nrc_rows(Context& c, int64_t cap) {
 }
 
 // One producer pass; counts[] receive the full list sizes (synchronises).
-gdf_status produce(Context& c, const gdf_path_state& st, const gdf_aabb& aabb,
-                   const gdf_train_pixels& px, int kind, gdf::ProduceParams p,
-                   int64_t counts[2], cudaStream_t s) {
+// Launches the record producer; the counts stay on the device (c.pw.totals).
+gdf_status produce_dev(Context& c, const gdf_path_state& st, const gdf_aabb& aabb,
+                       const gdf_train_pixels& px, int kind, gdf::ProduceParams p, cudaStream_t s) {
   const int64_t n = train_pixels(px);
   gdf_status rc = ensure_scratch(c, n);
   if (rc) return rc;
@@ -1384,6 +1432,15 @@ gdf_status produce(Context& c, const gdf_path_state& st, const gdf_aabb& aabb,
   p.totals = c.pw.totals;
   cudaError_t e = gdf::launch_produce(p, kind, s);
   if (e != cudaSuccess) return cuda_fail(e, "record producer");
+  return GDF_OK;
+}
+
+// The record producer with its counts read back to the host.
+gdf_status produce(Context& c, const gdf_path_state& st, const gdf_aabb& aabb,
+                   const gdf_train_pixels& px, int kind, gdf::ProduceParams p,
+                   int64_t counts[2], cudaStream_t s) {
+  gdf_status rc = produce_dev(c, st, aabb, px, kind, p, s);
+  if (rc) return rc;
   GDF_CUDA(cudaMemcpyAsync(c.pw.totals_host, c.pw.totals, 2 * sizeof(int64_t),
                            cudaMemcpyDeviceToHost, s));
   GDF_CUDA(cudaStreamSynchronize(s));
@@ -1582,42 +1639,61 @@ gdf_status gdf_nrc_substitute_paths(gdf_ctx* ctx, gdf_path_state* state, const g
   return GDF_OK;
 }
 
-gdf_status gdf_train_paths(gdf_ctx* ctx, const gdf_path_state* state, const gdf_aabb* aabb,
-                           const gdf_train_pixels* px, float* loss_host, int64_t* n_samples_host,
-                           void* stream) {
+gdf_status gdf_train_paths_async(gdf_ctx* ctx, const gdf_path_state* state, const gdf_aabb* aabb,
+                                 const gdf_train_pixels* px, float* loss_dev, int64_t* n_samples_dev,
+                                 void* stream) {
   if (!ctx) return fail(GDF_ERR_INVALID_ARG, "ctx is null");
   Context& c = ctx->c;
   gdf_status s;
   if ((s = check_px(state, aabb, px))) return s;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const int64_t cap = train_pixels(*px) * GDF_MAX_TRAIN_DEPTH;
-  if ((s = ensure_df_records(c, cap))) return s;
+  const int32_t per_frame = c.cfg.df_batches_per_frame;
+  if ((s = ensure_df_records(c, cap)) || (s = ensure_plan(c, std::max<int32_t>(per_frame, 1)))) return s;
   gdf::ProduceParams p;
   std::memset(&p, 0, sizeof(p));
   p.out_a0 = c.pw.df_in;
   p.out_a1 = c.pw.df_in_phi;
   p.out_a2 = c.pw.df_target;
   p.cap_a = c.pw.df_cap;
-  int64_t counts[2];
-  if ((s = produce(c, *state, *aabb, *px, gdf::kRecordsDf, p, counts, st))) return s;
-  const int64_t n = counts[0];
-  if (n_samples_host) *n_samples_host = n;
-  // LearnedDistribution::trainStep batch loop (learnedDistribution.cpp:227-290).
+  if ((s = produce_dev(c, *state, *aabb, *px, gdf::kRecordsDf, p, st))) return s;
+  // LearnedDistribution::trainStep batch loop (learnedDistribution.cpp:226-290)
+  // with the record count on the device: every batch the loop can reach is
+  // launched, sized by the plan, and one past the count trains nothing.
   const int64_t bs = c.cfg.df_batch_size;
-  const int64_t batches = std::min<int64_t>(n / bs + 1, c.cfg.df_batches_per_frame);
-  double loss = 0.0;
-  for (int64_t it = 0; it < batches; ++it) {
-    int64_t local = std::min<int64_t>(n - it * bs, bs);
-    local -= local % 128;
-    if (local < c.cfg.min_train_batch) break;
-    gdf_train_stats ts;
+  cudaError_t e = gdf::launch_df_batch_plan(c.pw.totals, bs, per_frame, c.cfg.min_train_batch, c.pw.plan,
+                                            c.pw.loss_acc, st);
+  if (e != cudaSuccess) return cuda_fail(e, "batch plan");
+  for (int32_t it = 0; it < per_frame; ++it) {
     const int64_t o = it * bs;
-    if ((s = gdf_train_step(ctx, c.pw.df_in + o * 9, c.pw.df_in_phi + o * 10, c.pw.df_target + o * 9,
-                            local, &ts, stream)))
+    if (o >= c.pw.df_cap) break;  // the count never exceeds the record capacity
+    const int64_t bound = std::min<int64_t>(bs, c.pw.df_cap - o);
+    if ((s = train_step_dev(c, c.pw.df_in + o * 9, c.pw.df_in_phi + o * 10, c.pw.df_target + o * 9, bound,
+                            c.pw.plan + 1 + it, c.pw.loss_acc, st)))
       return s;
-    loss += ts.loss;
   }
-  if (loss_host) *loss_host = batches > 0 ? static_cast<float>(loss / static_cast<double>(batches)) : 0.f;
+  e = gdf::launch_df_frame_finish(c.pw.plan, c.pw.loss_acc, c.pw.totals, loss_dev, n_samples_dev, st);
+  if (e != cudaSuccess) return cuda_fail(e, "frame finish");
+  return GDF_OK;
+}
+
+gdf_status gdf_train_paths(gdf_ctx* ctx, const gdf_path_state* state, const gdf_aabb* aabb,
+                           const gdf_train_pixels* px, float* loss_host, int64_t* n_samples_host,
+                           void* stream) {
+  if (!ctx) return fail(GDF_ERR_INVALID_ARG, "ctx is null");
+  Context& c = ctx->c;
+  gdf_status s;
+  if ((s = check_px(state, aabb, px)) || (s = ensure_plan(c, std::max<int32_t>(c.cfg.df_batches_per_frame, 1))))
+    return s;
+  if ((s = gdf_train_paths_async(ctx, state, aabb, px, c.pw.frame_loss, c.pw.frame_n, stream))) return s;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  float loss = 0.f;
+  int64_t n = 0;
+  GDF_CUDA(cudaMemcpyAsync(&loss, c.pw.frame_loss, sizeof(loss), cudaMemcpyDeviceToHost, st));
+  GDF_CUDA(cudaMemcpyAsync(&n, c.pw.frame_n, sizeof(n), cudaMemcpyDeviceToHost, st));
+  GDF_CUDA(cudaStreamSynchronize(st));
+  if (loss_host) *loss_host = loss;
+  if (n_samples_host) *n_samples_host = n;
   return GDF_OK;
 }
 

@@ -11,6 +11,7 @@
 #include "../../../include/gdf.h"
 #include "../device/grid_levels.h"
 #include "../kernels/df_kernels.h"
+#include "../kernels/train_kernels.h"
 
 namespace gdf {
 
@@ -42,7 +43,7 @@ struct Net {
   uint8_t* blob_f8 = nullptr;
   uint32_t f8_bytes = 0;
   Fp8PackParams f8_pack{};
-  uint32_t opt_step = 0;       // optimizer step counter (Adam m_current_step)
+  OptState* opt = nullptr;     // optimizer step counter (device; the optimizer kernel advances it)
 };
 
 // Device workspace of the training step, sized by max_train_batch.
@@ -80,6 +81,12 @@ struct PathWorkspace {
   float* nrc_train_in = nullptr;    // [nrc_cap x 15]
   float* nrc_train_target = nullptr;// [nrc_cap x 3]
   int64_t nrc_rows = 0;             // query rows of the last NRC build
+  // frame-level DF training with the record count on the device
+  int32_t plan_len = 0;             // batches the plan holds
+  int64_t* plan = nullptr;          // [1 + plan_len]: batches, records per batch
+  double* loss_acc = nullptr;       // [1] sum of the batches' mean losses
+  float* frame_loss = nullptr;      // [1] device results of gdf_train_paths
+  int64_t* frame_n = nullptr;       // [1]
 };
 
 struct Context {

@@ -142,7 +142,12 @@ __global__ void __launch_bounds__(128 * WGS, 1) df_fused_kernel(const __grid_con
   const float* ds_phi = reinterpret_cast<const float*>(
       smem + off_phi + 64u * (LF + KR) * 2u + static_cast<uint32_t>(p.hidden_phi - 1) * 4096u + NBP * 128u);
 
-  const int64_t n_tiles = (p.n + 127) / 128;
+  // training modes with a device-side record count: min(*n_dev, n) rows
+  const int64_t n_rows = (kTrain && p.n_dev) ? min(*p.n_dev, p.n) : p.n;
+  const float loss_scale_per_record = (kTrain && p.n_dev)
+                                          ? (n_rows > 0 ? p.loss_scale / static_cast<float>(n_rows) : 0.f)
+                                          : p.loss_scale_per_record;
+  const int64_t n_tiles = (n_rows + 127) / 128;
   // Both feature tiles of tile t, one bulk copy each, completing on fbar.
   auto fetch_features = [&](int64_t t) {
     if (!c.leader) return;
@@ -157,7 +162,7 @@ __global__ void __launch_bounds__(128 * WGS, 1) df_fused_kernel(const __grid_con
   for (int64_t t = static_cast<int64_t>(blockIdx.x) * WGS + wg; t < n_tiles;
        t += static_cast<int64_t>(gridDim.x) * WGS) {
     const int64_t row = t * 128 + c.row;
-    const bool valid = row < p.n;
+    const bool valid = row < n_rows;
     float q[9], qp[10];
     if (MODE == kModeInfer && p.shading.pos != nullptr) {
       // generate_inference_data_AR (train.cu:344-361) in registers
@@ -296,7 +301,7 @@ __global__ void __launch_bounds__(128 * WGS, 1) df_fused_kernel(const __grid_con
       const float li = (tg[2] + tg[3] + tg[4]) / 3.0f;
       const float wi_pdf = tg[5] + kEps;
       const float gpdf = fabsf(pdf_theta) * fabsf(pdf_phi) * kInv4Pi * (1.f / kInv4Pi) + kEps;
-      const float prefix = -li / wi_pdf / gpdf * p.loss_scale_per_record;
+      const float prefix = -li / wi_pdf / gpdf * loss_scale_per_record;
       const float lik = -li / wi_pdf * logf(gpdf);
       if (valid) {
         const float4 o = record_ok ? make_float4(pdf_theta, pdf_phi, prefix, lik)

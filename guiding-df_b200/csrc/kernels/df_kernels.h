@@ -42,6 +42,10 @@ struct DfKernelParams {
   float* train_out;                  // n x 4: pdf_theta, pdf_phi, prefix, likelihood
   unsigned long long* n_dropped;     // records rejected by the validity filter
   float loss_scale_per_record;       // TRAIN_LOSS_SCALE / n
+  // training modes: when set, the batch has min(*n_dev, n) records (n is
+  // then the launch's bound) and the per-record scale is loss_scale / that
+  const int64_t* n_dev;
+  float loss_scale;
   GridLevels gl_theta, gl_phi;
   // grid features of both networks, precomputed by launch_grid_features
   // (inference and pdf evaluation): 128-row tiles, canonical layout
@@ -62,6 +66,7 @@ struct TrainFeatParams {
   const float* in_phi;       // n x 10 GuidedInputPhi
   const float* target;       // n x 9 GuidedOutput (the validity filter reads it)
   int64_t n, n_tiles;
+  const int64_t* n_dev;      // nullable: min(*n_dev, n) records (n, n_tiles: the launch's bound)
   const __half* grid_theta;  // fp16 training tables
   const __half* grid_phi;
   GridLevels gl_theta, gl_phi;

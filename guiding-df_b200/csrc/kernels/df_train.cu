@@ -159,6 +159,7 @@ __global__ void __launch_bounds__(256) grid_scatter_kernel(const __grid_constant
   if (gid >= p.n * L) return;
   const int l = static_cast<int>(gid / p.n);
   const int64_t row = gid - static_cast<int64_t>(l) * p.n;
+  if (p.n_dev && row >= *p.n_dev) return;  // beyond this batch's records
   if (__ldg(p.fwd + row * 4 + 2) == 0.f) return;
   float pos[3], dl[F];
 #pragma unroll
@@ -196,7 +197,8 @@ __global__ void __launch_bounds__(128, 1) df_train_bwd_kernel(const __grid_const
   // [0] weights, [1] MMA completion, [2] feature tile
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + off_bar);
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + off_bar + 32);
-  const int64_t n_tiles = (p.n + 127) / 128;
+  const int64_t n_rows = p.n_dev ? min(*p.n_dev, p.n) : p.n;
+  const int64_t n_tiles = (n_rows + 127) / 128;
   auto fetch_features = [&](int64_t t) {
     mbar_arrive_expect_tx(&bars[2], kXF);
     bulk_g2s(smem + off_xf, p.feat + t * (128 * LF), kXF, &bars[2]);
@@ -263,7 +265,7 @@ __global__ void __launch_bounds__(128, 1) df_train_bwd_kernel(const __grid_const
   bool first = true;
   for (int64_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
     const int64_t row = t * 128 + c.row;
-    const bool valid = row < p.n;
+    const bool valid = row < n_rows;
     float q[10];
 #pragma unroll
     for (int i = 0; i < 10; ++i) q[i] = 0.5f;
@@ -425,7 +427,7 @@ cudaError_t launch_bwd_t(const DfBwdParams& p, int ctas, cudaStream_t st) {
 // parameter whose own step counter is k, lr sqrt(1 - beta2^k) / (1 - beta1^k),
 // comes from a table filled by adam_lr_table_kernel with the same float
 // expression; past the table's end the value is lr exactly.
-__device__ __forceinline__ void adam_param(const AdamParams& p, bool matrix, float graw, float& wf,
+__device__ __forceinline__ void adam_param(const AdamParams& p, const float2 debias, bool matrix, float graw, float& wf,
                                            float& m1, float& m2, uint32_t& step, __half& w16h,
                                            __half& emah, double& sq) {
   float g = graw / p.loss_scale;
@@ -444,8 +446,8 @@ __device__ __forceinline__ void adam_param(const AdamParams& p, bool matrix, flo
   } else {
     w16 = __half2float(w16h);
   }
-  emah = __float2half_rn((__half2float(emah) * p.ema_decay * p.debias_old + w16 * (1 - p.ema_decay)) *
-                         p.debias_new);
+  emah = __float2half_rn((__half2float(emah) * p.ema_decay * debias.x + w16 * (1 - p.ema_decay)) *
+                         debias.y);
 }
 
 __global__ void adam_lr_table_kernel(float lr, float beta1, float beta2, float* table, int32_t n) {
@@ -473,6 +475,21 @@ __device__ __forceinline__ void write_il(const AdamParams& p, int64_t j, uint2 e
 }
 
 __global__ void __launch_bounds__(256) adam_ema_kernel(const __grid_constant__ AdamParams p) {
+  if (p.n_dev && *p.n_dev <= 0) return;  // empty batch: no optimizer step
+  // AdamOptimizer::step increments its counter before use (adam.h:150-152);
+  // EmaOptimizer::step debiases with it (ema.h:102-110). Every block reads
+  // the counter here; the last block to finish stores the new value.
+  __shared__ float2 debias_s;
+  __shared__ uint32_t opt_step_s;
+  if (threadIdx.x == 0) {
+    const uint32_t opt_step = p.opt->step + 1;
+    const double d = static_cast<double>(p.ema_decay);
+    debias_s = make_float2(1.0f - static_cast<float>(pow(d, static_cast<double>(opt_step - 1))),
+                           1.0f / (1.0f - static_cast<float>(pow(d, static_cast<double>(opt_step)))));
+    opt_step_s = opt_step;
+  }
+  __syncthreads();
+  const float2 debias = debias_s;
   double local_sq = 0.0;
   const int64_t tid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   const int64_t nth = static_cast<int64_t>(gridDim.x) * blockDim.x;
@@ -484,7 +501,7 @@ __global__ void __launch_bounds__(256) adam_ema_kernel(const __grid_constant__ A
     float wf = p.master[i], m1 = p.m[i], m2 = p.v[i];
     uint32_t step = p.step[i];
     __half w16h = p.w16[i], emah = p.ema16[i];
-    adam_param(p, true, graw, wf, m1, m2, step, w16h, emah, local_sq);
+    adam_param(p, debias, true, graw, wf, m1, m2, step, w16h, emah, local_sq);
     p.master[i] = wf;
     p.m[i] = m1;
     p.v[i] = m2;
@@ -561,7 +578,7 @@ __global__ void __launch_bounds__(256) adam_ema_kernel(const __grid_constant__ A
     __half* ee = reinterpret_cast<__half*>(&e4);
     const float gg[4] = {g4.x, g4.y, g4.z, g4.w};
 #pragma unroll
-    for (int k = 0; k < 4; ++k) adam_param(p, false, gg[k], (&w4.x)[k], (&m4.x)[k], (&v4.x)[k], (&s4.x)[k], hh[k], ee[k], local_sq);
+    for (int k = 0; k < 4; ++k) adam_param(p, debias, false, gg[k], (&w4.x)[k], (&m4.x)[k], (&v4.x)[k], (&s4.x)[k], hh[k], ee[k], local_sq);
     reinterpret_cast<float4*>(b + 4 * kAdamTile)[t] = w4;
     reinterpret_cast<float4*>(b + 8 * kAdamTile)[t] = m4;
     reinterpret_cast<float4*>(b + 12 * kAdamTile)[t] = v4;
@@ -606,7 +623,7 @@ __global__ void __launch_bounds__(256) adam_ema_kernel(const __grid_constant__ A
     __half* ee = reinterpret_cast<__half*>(&e4);
     const float gg[4] = {g4.x, g4.y, g4.z, g4.w};
 #pragma unroll
-    for (int k = 0; k < 4; ++k) adam_param(p, false, gg[k], (&w4.x)[k], (&m4.x)[k], (&v4.x)[k], (&s4.x)[k], hh[k], ee[k], local_sq);
+    for (int k = 0; k < 4; ++k) adam_param(p, debias, false, gg[k], (&w4.x)[k], (&m4.x)[k], (&v4.x)[k], (&s4.x)[k], hh[k], ee[k], local_sq);
     *reinterpret_cast<float4*>(p.master + i) = w4;
     *reinterpret_cast<float4*>(p.m + i) = m4;
     *reinterpret_cast<float4*>(p.v + i) = v4;
@@ -622,7 +639,7 @@ __global__ void __launch_bounds__(256) adam_ema_kernel(const __grid_constant__ A
     float wf = p.master[i], m1 = p.m[i], m2 = p.v[i];
     uint32_t step = p.step[i];
     __half w16h = p.w16[i], emah = p.ema16[i];
-    adam_param(p, false, graw, wf, m1, m2, step, w16h, emah, local_sq);
+    adam_param(p, debias, false, graw, wf, m1, m2, step, w16h, emah, local_sq);
     p.master[i] = wf;
     p.m[i] = m1;
     p.v[i] = m2;
@@ -642,7 +659,16 @@ __global__ void __launch_bounds__(256) adam_ema_kernel(const __grid_constant__ A
     if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
     __syncthreads();
   }
-  if (threadIdx.x == 0) p.sq_partial[blockIdx.x] = red[0];
+  if (threadIdx.x == 0) {
+    p.sq_partial[blockIdx.x] = red[0];
+    // this block read the step counter at its start; the last block done
+    // stores the advanced counter and resets the count for the next launch
+    __threadfence();
+    if (atomicAdd(&p.opt->blocks_done, 1u) == gridDim.x - 1) {
+      p.opt->step = opt_step_s;
+      p.opt->blocks_done = 0u;
+    }
+  }
 }
 
 // Deterministic FP64 reductions: loss = sum(likelihood) (column 3 of the
@@ -674,8 +700,9 @@ __global__ void train_stats_kernel(const float* __restrict__ fwd, int64_t n, con
 // The same two FP64 sums over many blocks: each block sums the likelihood
 // column over one contiguous range of records (fixed order) ...
 __global__ void __launch_bounds__(512) loss_partials_kernel(const float* __restrict__ fwd, int64_t n,
-                                                            double* __restrict__ part) {
+                                                            const int64_t* n_dev, double* __restrict__ part) {
   __shared__ double red[512];
+  if (n_dev) n = min(*n_dev, n);
   const int64_t per = (n + gridDim.x - 1) / gridDim.x;
   const int64_t b = static_cast<int64_t>(blockIdx.x) * per;
   const int64_t e = min(n, b + per);
@@ -693,7 +720,8 @@ __global__ void __launch_bounds__(512) loss_partials_kernel(const float* __restr
 // ... and one block adds the block sums and the optimizer's partials.
 __global__ void __launch_bounds__(256) stats_final_kernel(const double* __restrict__ part, int n_part,
                                                           const double* __restrict__ sq, int n_sq,
-                                                          double* out) {
+                                                          double* out, int64_t n, const int64_t* n_dev,
+                                                          double* loss_acc) {
   __shared__ double red[256];
   for (int k = 0; k < 2; ++k) {
     const double* v = k == 0 ? part : sq;
@@ -708,6 +736,10 @@ __global__ void __launch_bounds__(256) stats_final_kernel(const double* __restri
     }
     if (threadIdx.x == 0) out[k] = red[0];
     __syncthreads();
+  }
+  if (threadIdx.x == 0 && loss_acc) {
+    const int64_t rows = n_dev ? min(*n_dev, n) : n;
+    if (rows > 0) *loss_acc += out[0] / static_cast<double>(rows);
   }
 }
 
@@ -767,10 +799,10 @@ cudaError_t launch_train_stats(const float* fwd, int64_t n, const double* sq, in
   return cudaGetLastError();
 }
 
-cudaError_t launch_train_stats_mb(const float* fwd, int64_t n, const double* sq, int n_sq, double* part,
-                                  double* out, cudaStream_t st) {
-  loss_partials_kernel<<<kStatBlocks, 512, 0, st>>>(fwd, n, part);
-  stats_final_kernel<<<1, 256, 0, st>>>(part, kStatBlocks, sq, n_sq, out);
+cudaError_t launch_train_stats_mb(const float* fwd, int64_t n, const int64_t* n_dev, const double* sq, int n_sq,
+                                  double* part, double* out, double* loss_acc, cudaStream_t st) {
+  loss_partials_kernel<<<kStatBlocks, 512, 0, st>>>(fwd, n, n_dev, part);
+  stats_final_kernel<<<1, 256, 0, st>>>(part, kStatBlocks, sq, n_sq, out, n, n_dev, loss_acc);
   return cudaGetLastError();
 }
 

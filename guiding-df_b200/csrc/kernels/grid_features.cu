@@ -81,8 +81,10 @@ __global__ void __launch_bounds__(256, 4) train_features_kernel(const __grid_con
   if (gid >= rows * NCH) return;
   const int64_t row = gid % rows;
   const int chunk = static_cast<int>(gid / rows);
+  const int64_t n = p.n_dev ? min(*p.n_dev, p.n) : p.n;
+  if (row >= (n + 127) / 128 * 128) return;  // tiles beyond this batch's records
   float pt[3] = {0.5f, 0.5f, 0.5f}, pp[3] = {0.5f, 0.5f, 0.5f};
-  if (row < p.n) {
+  if (row < n) {
     bool ok = true;
     float a[3], b[3];
 #pragma unroll

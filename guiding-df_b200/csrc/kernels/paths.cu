@@ -477,6 +477,47 @@ cudaError_t launch_produce(const ProduceParams& p, int kind, cudaStream_t st) {
   }
 }
 
+namespace {
+
+__global__ void df_batch_plan_kernel(const int64_t* count, int64_t bs, int32_t per_frame, int64_t min_batch,
+                                     int64_t* plan, double* loss_acc) {
+  const int64_t n = *count;
+  const int64_t batches = min(n / bs + 1, static_cast<int64_t>(per_frame));
+  plan[0] = batches;
+  bool stop = false;
+  for (int32_t i = 0; i < per_frame; ++i) {
+    int64_t local = i < batches ? min(n - i * bs, bs) : 0;
+    local -= local % 128;
+    if (stop || local < min_batch) {
+      stop = true;
+      local = 0;
+    }
+    plan[1 + i] = local;
+  }
+  *loss_acc = 0.0;
+}
+
+__global__ void df_frame_finish_kernel(const int64_t* plan, const double* loss_acc, const int64_t* count,
+                                       float* loss_out, int64_t* n_out) {
+  const int64_t batches = plan[0];
+  if (loss_out) *loss_out = batches > 0 ? static_cast<float>(*loss_acc / static_cast<double>(batches)) : 0.f;
+  if (n_out) *n_out = *count;
+}
+
+}  // namespace
+
+cudaError_t launch_df_batch_plan(const int64_t* count, int64_t bs, int32_t per_frame, int64_t min_batch,
+                                 int64_t* plan, double* loss_acc, cudaStream_t st) {
+  df_batch_plan_kernel<<<1, 1, 0, st>>>(count, bs, per_frame, min_batch, plan, loss_acc);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_df_frame_finish(const int64_t* plan, const double* loss_acc, const int64_t* count,
+                                   float* loss_out, int64_t* n_out, cudaStream_t st) {
+  df_frame_finish_kernel<<<1, 1, 0, st>>>(plan, loss_acc, count, loss_out, n_out);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_prepare_queries(const gdf_shading& s, const gdf_aabb& aabb, float* queries,
                                    int64_t n, cudaStream_t st) {
   if (n == 0) return cudaSuccess;

@@ -51,6 +51,17 @@ inline int64_t produce_blocks(int64_t n_train) {
 // mask -> block scan -> emit; totals[] hold the full counts afterwards.
 cudaError_t launch_produce(const ProduceParams& p, int kind, cudaStream_t st);
 
+// The frame-level batch plan of LearnedDistribution::trainStep
+// (learnedDistribution.cpp:226-236) from the record count on the device:
+// plan[0] = batches = min(count / bs + 1, per_frame); plan[1 + i] = the
+// records of batch i (min(count - i bs, bs) rounded down to 128), or 0 from
+// the first batch below min_batch on (the loop's break). Zeroes loss_acc.
+cudaError_t launch_df_batch_plan(const int64_t* count, int64_t bs, int32_t per_frame, int64_t min_batch,
+                                 int64_t* plan, double* loss_acc, cudaStream_t st);
+// loss_out = loss_acc / batches (0 without batches), n_out = count.
+cudaError_t launch_df_frame_finish(const int64_t* plan, const double* loss_acc, const int64_t* count,
+                                   float* loss_out, int64_t* n_out, cudaStream_t st);
+
 // generate_inference_data_AR (train.cu:334-362) alone.
 cudaError_t launch_prepare_queries(const gdf_shading& s, const gdf_aabb& aabb, float* queries,
                                    int64_t n, cudaStream_t st);

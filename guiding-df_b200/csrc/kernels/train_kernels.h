@@ -17,6 +17,7 @@ struct DfBwdParams {
   const float* target;      // n x 9 GuidedOutput
   const float* fwd;         // n x 4 from the training forward: pdf_theta, pdf_phi, prefix, likelihood
   int64_t n;
+  const int64_t* n_dev;     // nullable: min(*n_dev, n) records (n: the launch's bound)
   const __half* blob;       // fp16 training weights, canonical layout
   uint32_t blob_bytes;
   const __half* grid;       // fp16 training grid tables
@@ -37,10 +38,20 @@ struct GridScatterParams {
   int32_t in_stride;
   const float* fwd;         // n x 4 from the training forward (prefix 0: rejected record)
   int64_t n;
+  const int64_t* n_dev;     // nullable: min(*n_dev, n) records (n: the launch's bound)
   const float* dx;          // [L][dx_rows][F]
   int64_t dx_rows;
   float* grid_grad;
   GridLevels gl;
+};
+
+// A network's optimizer step counter (Adam m_current_step, adam.h:150-152),
+// in device memory so that a step can be skipped on the device (an empty
+// batch). The optimizer kernel's blocks all read it; the last block to
+// finish advances it (blocks_done counts them and is reset to 0).
+struct OptState {
+  uint32_t step;
+  uint32_t blocks_done;
 };
 
 // Adam + EMA over one network (tcnn optimizers/adam.h, ema.h).
@@ -60,7 +71,9 @@ struct AdamParams {
   int64_t layer_off[12];
   int32_t layer_cols[12];
   int32_t n_layers;
-  float loss_scale, lr, beta1, beta2, eps, l2_reg, ema_decay, debias_old, debias_new;
+  float loss_scale, lr, beta1, beta2, eps, l2_reg, ema_decay;
+  OptState* opt;            // the step counter, advanced by this launch
+  const int64_t* n_dev;     // nullable: the step is skipped when *n_dev == 0
   double* sq_partial;       // [n_blocks]
   int32_t n_blocks;
   // interleaved inference copy of the EMA grid ([entries][theta F | phi F]),
@@ -85,8 +98,9 @@ cudaError_t launch_adam_lr_table(float lr, float beta1, float beta2, float* tabl
 // The same two sums with the loss over kStatBlocks blocks; part holds
 // kStatBlocks doubles of scratch.
 constexpr int kStatBlocks = 148;
-cudaError_t launch_train_stats_mb(const float* fwd, int64_t n, const double* sq, int n_sq, double* part,
-                                  double* out, cudaStream_t stream);
+// n_dev (nullable): min(*n_dev, n) records; loss_acc (nullable): += out[0] / records, if any.
+cudaError_t launch_train_stats_mb(const float* fwd, int64_t n, const int64_t* n_dev, const double* sq, int n_sq,
+                                  double* part, double* out, double* loss_acc, cudaStream_t stream);
 cudaError_t launch_train_stats(const float* fwd, int64_t n, const double* sq, int n_sq, double* out,
                                cudaStream_t st);
 

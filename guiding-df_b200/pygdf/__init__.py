@@ -208,6 +208,8 @@ def lib() -> C.CDLL:
                                     C.POINTER(C.c_float), C.POINTER(C.c_int64), P],
             "gdf_nrc_substitute_paths": [P, C.POINTER(PathState), C.POINTER(Aabb),
                                          C.POINTER(TrainPixels), C.c_int32, P],
+            "gdf_train_paths_async": [P, C.POINTER(PathState), C.POINTER(Aabb), C.POINTER(TrainPixels),
+                                      P, P, P],
             "gdf_train_paths": [P, C.POINTER(PathState), C.POINTER(Aabb), C.POINTER(TrainPixels),
                                 C.POINTER(C.c_float), C.POINTER(C.c_int64), P],
         }
@@ -425,6 +427,13 @@ class Context:
         check(lib().gdf_train_paths(self.h, C.byref(st), C.byref(aabb), C.byref(px),
                                     C.byref(loss), C.byref(n), _stream(stream)))
         return loss.value, n.value
+
+    def train_paths_async(self, st: PathState, aabb: Aabb, px: TrainPixels, loss_dev=None, n_dev=None,
+                          stream=None):
+        """Stream-ordered frame training; results land in device tensors
+        (float32 loss, int64 record count)."""
+        check(lib().gdf_train_paths_async(self.h, C.byref(st), C.byref(aabb), C.byref(px), _ptr(loss_dev),
+                                          _ptr(n_dev), _stream(stream)))
 
     def get_optimizer_state(self, net: int):
         import numpy as np

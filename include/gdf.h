@@ -575,10 +575,25 @@ gdf_status gdf_nrc_substitute_paths(gdf_ctx* ctx, gdf_path_state* state, const g
 /* LearnedDistribution::trainStep (learnedDistribution.cpp:208-293): builds
  * the records (gdf_build_train_records) into library buffers and runs the
  * batch loop of gdf_train_step. *loss_host = sum of batch losses / batch
- * count; *n_samples_host = records built. Synchronises. */
+ * count; *n_samples_host = records built. Synchronises once, at the end, to
+ * read the two results (gdf_train_paths_async without the read-back). */
 gdf_status gdf_train_paths(gdf_ctx* ctx, const gdf_path_state* state, const gdf_aabb* aabb,
                            const gdf_train_pixels* px, float* loss_host, int64_t* n_samples_host,
                            void* stream);
+
+/* gdf_train_paths, stream-ordered: the record count stays on the device,
+ * every batch the loop can reach (df_batches_per_frame) is launched with
+ * its size read on the device, and a batch past the count, or below
+ * min_train_batch, trains nothing (no optimizer step). No host
+ * synchronisation and no allocation once the buffers for this pixel count
+ * exist (a first call allocates them), so the call can be captured in a
+ * CUDA graph. loss_dev (float) and n_samples_dev (int64), device pointers,
+ * receive the two results; either may be null. The reference reads the
+ * count back (learnedDistribution.cpp:225-226); this entry point has no
+ * counterpart there. */
+gdf_status gdf_train_paths_async(gdf_ctx* ctx, const gdf_path_state* state, const gdf_aabb* aabb,
+                                 const gdf_train_pixels* px, float* loss_dev, int64_t* n_samples_dev,
+                                 void* stream);
 
 /* ----------------------------------------------------------------- errors */
 

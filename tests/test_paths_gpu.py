@@ -247,6 +247,59 @@ def test_train_paths_batch_loop():
     ctx2.close()
 
 
+def test_train_paths_async_captures_into_a_graph():
+    """gdf_train_paths_async keeps the record count on the device, so the
+    frame's producer and batch loop capture into one CUDA graph. Each replay
+    trains a frame: its loss and record count equal gdf_train_paths' on a
+    context with the same weights (batches after the first see grid weights
+    whose gradients were summed by float atomics: 1e-5 relative), and only
+    the batches the loop reaches take an optimizer step."""
+    fields, depth = W.path_state(60000, 16)
+    cfg, ctx = _ctx()
+    _, ctx2 = _ctx()
+    _, _, st = _state_dev(fields, depth)
+    box, px = pygdf.Aabb.of(*AABB), _px(60000)
+    init = [ctx.get_params(k) for k in (0, 1)]
+    loss_d = torch.zeros(1, dtype=torch.float32, device="cuda")
+    n_d = torch.zeros(1, dtype=torch.int64, device="cuda")
+    ctx.train_paths_async(st, box, px, loss_d, n_d)  # allocates the frame buffers
+    torch.cuda.synchronize()
+    for k in (0, 1):  # back to the initial weights and optimizer state
+        ctx.set_params(k, init[k])
+        z = np.zeros(init[k].size, np.float32)
+        ctx.set_optimizer_state(k, z, z, np.zeros(init[k].size, np.uint32), 0)
+    g = torch.cuda.CUDAGraph()
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        with torch.cuda.graph(g, stream=s, capture_error_mode="relaxed"):
+            ctx.train_paths_async(st, box, px, loss_d, n_d, stream=s)
+    torch.cuda.synchronize()
+    loss_ref, n_ref = ctx2.train_paths(st, box, px)
+    bs = cfg.df_batch_size
+    batches = min(n_ref // bs + 1, cfg.df_batches_per_frame)
+    used = 0
+    for it in range(batches):
+        local = min(n_ref - it * bs, bs)
+        if local - local % 128 < cfg.min_train_batch:
+            break
+        used += 1
+    assert 2 <= used < cfg.df_batches_per_frame  # launched batches that train nothing are covered
+    for frame in (1, 2):
+        g.replay()
+        torch.cuda.synchronize()
+        assert int(n_d.item()) == n_ref
+        for k in (0, 1):
+            assert ctx.get_optimizer_state(k)[3] == frame * used
+        if frame == 1:
+            loss = float(loss_d.item())
+            assert abs(loss - loss_ref) <= 1e-5 * abs(loss_ref), (loss, loss_ref)
+            assert ctx2.get_optimizer_state(0)[3] == used
+    del g
+    ctx.close()
+    ctx2.close()
+
+
 def test_infer_ex_shading_equals_prepared_queries():
     cfg, ctx = _ctx(pygdf.PRESET_FULL)
     rng = np.random.default_rng(3)
