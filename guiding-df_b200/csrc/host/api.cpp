@@ -854,25 +854,34 @@ gdf_status gdf_infer_host(gdf_ctx* ctx, const float* queries_h, const uint8_t* g
   }
   if ((s = ensure_features(c, (n + 127) / 128))) return s;
   cudaStream_t user = static_cast<cudaStream_t>(stream);
-  GDF_CUDA(cudaEventRecord(c.pipe_ev[2], user));
-  for (cudaStream_t ps : c.pipe) GDF_CUDA(cudaStreamWaitEvent(ps, c.pipe_ev[2], 0));
-  // Chunks of 4096 tiles alternate between two streams, so the copy engines
-  // move chunk k+1 in and chunk k-1 out while chunk k computes. Smaller
-  // chunks cost more per chunk than they save in pipeline fill (a 1080p
-  // bounce: 2.86 ms with 1024-tile chunks, 2.60 ms with 4096).
-  constexpr int64_t kChunk = 4096 * 128;
-  for (int64_t b = 0, k = 0; b < n; b += kChunk, ++k) {
-    const int64_t m = std::min(kChunk, n - b);
-    cudaStream_t ps = c.pipe[k & 1];
+  GDF_CUDA(cudaEventRecord(c.pipe_ev[3], user));
+  for (cudaStream_t ps : c.pipe) GDF_CUDA(cudaStreamWaitEvent(ps, c.pipe_ev[3], 0));
+  // Three streams: input copies, kernels, output copies. Each chunk has its
+  // own device rows, so the input copies run back to back at the link's
+  // rate (they bound the call: the kernels outrun PCIe), a chunk's kernels
+  // start when its rows are in, and its output copy when they are done.
+  // What remains after the last input copy is the last chunk's kernels and
+  // output copy, so chunks are at most 4096 tiles and at most half of what
+  // remains, down to 256 tiles.
+  cudaStream_t s_in = c.pipe[0], s_run = c.pipe[1], s_out = c.pipe[2];
+  constexpr int64_t kChunk = 4096 * 128, kMinChunk = 256 * 128;
+  int64_t m = 0;
+  for (int64_t b = 0; b < n; b += m) {
+    const int64_t rest = n - b;
+    m = std::min(kChunk, (rest / 2 + 127) / 128 * 128);
+    if (m < kMinChunk) m = std::min(rest, kMinChunk);
     GDF_CUDA(cudaMemcpyAsync(c.host_q + b * 9, queries_h + b * 9, static_cast<size_t>(m) * 36,
-                             cudaMemcpyHostToDevice, ps));
+                             cudaMemcpyHostToDevice, s_in));
     GDF_CUDA(cudaMemcpyAsync(c.host_wi + b * 4, wi_in_h + b * 4, static_cast<size_t>(m) * 16,
-                             cudaMemcpyHostToDevice, ps));
+                             cudaMemcpyHostToDevice, s_in));
     if (guided_h)
-      GDF_CUDA(cudaMemcpyAsync(c.host_g + b, guided_h + b, static_cast<size_t>(m), cudaMemcpyHostToDevice, ps));
+      GDF_CUDA(cudaMemcpyAsync(c.host_g + b, guided_h + b, static_cast<size_t>(m), cudaMemcpyHostToDevice, s_in));
     if (uniforms_h)
       GDF_CUDA(cudaMemcpyAsync(c.host_u + b * 4, uniforms_h + b * 4, static_cast<size_t>(m) * 16,
-                               cudaMemcpyHostToDevice, ps));
+                               cudaMemcpyHostToDevice, s_in));
+    // one event object per hand-over: each wait takes the record before it
+    GDF_CUDA(cudaEventRecord(c.pipe_ev[4], s_in));
+    GDF_CUDA(cudaStreamWaitEvent(s_run, c.pipe_ev[4], 0));
     gdf::DfKernelParams p = df_params(c);
     p.queries = c.host_q + b * 9;
     p.guided = guided_h ? c.host_g + b : nullptr;
@@ -882,13 +891,15 @@ gdf_status gdf_infer_host(gdf_ctx* ctx, const float* queries_h, const uint8_t* g
     p.philox_seed = philox_seed;
     p.philox_offset = philox_offset;
     p.philox_row_base = b;
-    if ((s = grid_features(c, p.queries, nullptr, gdf_aabb{}, m, p, ps, b / 128))) return s;
-    cudaError_t e = gdf::launch_df_fused(df_shape(c), gdf::kModeInfer, p, c.num_sms, ps);
+    if ((s = grid_features(c, p.queries, nullptr, gdf_aabb{}, m, p, s_run, b / 128))) return s;
+    cudaError_t e = gdf::launch_df_fused(df_shape(c), gdf::kModeInfer, p, c.num_sms, s_run);
     if (e != cudaSuccess) return cuda_fail(e, "df_fused (infer_host)");
+    GDF_CUDA(cudaEventRecord(c.pipe_ev[5], s_run));
+    GDF_CUDA(cudaStreamWaitEvent(s_out, c.pipe_ev[5], 0));
     GDF_CUDA(cudaMemcpyAsync(wi_out_h + b * 4, c.host_wi + b * 4, static_cast<size_t>(m) * 16,
-                             cudaMemcpyDeviceToHost, ps));
+                             cudaMemcpyDeviceToHost, s_out));
   }
-  for (int i = 0; i < 2; ++i) {
+  for (int i = 0; i < 3; ++i) {
     GDF_CUDA(cudaEventRecord(c.pipe_ev[i], c.pipe[i]));
     GDF_CUDA(cudaStreamWaitEvent(user, c.pipe_ev[i], 0));
   }

@@ -112,7 +112,8 @@ struct Context {
   uint8_t* host_g = nullptr;     // [host_cap]
   float* host_u = nullptr;       // [host_cap x 4]
   float* host_wi = nullptr;      // [host_cap x 4]
-  cudaStream_t pipe[2] = {nullptr, nullptr};
+  // gdf_infer_host's streams: [0] input copies, [1] kernels, [2] output copies
+  cudaStream_t pipe[3] = {nullptr, nullptr, nullptr};
   // Adam step sizes by per-parameter step counter: [0] DF optimizer, [1] NRC
   float* lr_table[2] = {nullptr, nullptr};
   int32_t lr_table_n[2] = {0, 0};
@@ -121,7 +122,9 @@ struct Context {
   float* tool_q = nullptr;       // [tool_cap x 9]
   float* tool_uv = nullptr;      // [tool_cap x 2]
   float* tool_out = nullptr;     // [tool_cap x 4]
-  cudaEvent_t pipe_ev[3] = {nullptr, nullptr, nullptr};
+  // [0..2]: each pipe stream's end; [3]: the call's start; [4]: a chunk's
+  // input copies done; [5]: a chunk's kernels done
+  cudaEvent_t pipe_ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
 };
 
 // CTAs of the training step's persistent kernels (and weight-gradient partials).
