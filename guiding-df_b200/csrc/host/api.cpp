@@ -264,7 +264,8 @@ void free_ws(gdf::TrainWorkspace& w) {
   cudaFree(w.dropped);
   cudaFree(w.feat[0]);
   cudaFree(w.feat[1]);
-  cudaFree(w.dx);
+  cudaFree(w.dx[0]);
+  cudaFree(w.dx[1]);
   cudaFree(w.stat_part);
   w = gdf::TrainWorkspace{};
 }
@@ -291,6 +292,14 @@ void free_host_stage(Context& c) {
   for (cudaStream_t& s : c.pipe) {
     if (s) cudaStreamDestroy(s);
     s = nullptr;
+  }
+  for (cudaStream_t& s : c.train_aux) {
+    if (s) cudaStreamDestroy(s);
+    s = nullptr;
+  }
+  for (cudaEvent_t& e : c.train_ev) {
+    if (e) cudaEventDestroy(e);
+    e = nullptr;
   }
   for (cudaEvent_t& e : c.pipe_ev) {
     if (e) cudaEventDestroy(e);
@@ -335,11 +344,18 @@ gdf_status alloc_ws(Context& c) {
     return s;
   const size_t feat = static_cast<size_t>((cap + 127) / 128 * 128) * static_cast<size_t>(c.net[0].levels) *
                       static_cast<size_t>(c.net[0].features);
-  if ((s = dalloc(&w.feat[0], feat)) || (s = dalloc(&w.feat[1], feat)) ||
-      (s = dalloc(&w.dx, static_cast<size_t>(cap) * static_cast<size_t>(c.net[0].levels) *
-                             static_cast<size_t>(c.net[0].features))) ||
-      (s = dalloc(&w.stat_part, gdf::kStatBlocks)))
+  const size_t dx = static_cast<size_t>(cap) * static_cast<size_t>(c.net[0].levels) *
+                    static_cast<size_t>(c.net[0].features);
+  if ((s = dalloc(&w.feat[0], feat)) || (s = dalloc(&w.feat[1], feat)) || (s = dalloc(&w.dx[0], dx)) ||
+      (s = dalloc(&w.dx[1], dx)) || (s = dalloc(&w.stat_part, gdf::kStatBlocks)))
     return s;
+  if (!c.train_aux[0]) {
+    int least = 0, greatest = 0;
+    GDF_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    GDF_CUDA(cudaStreamCreateWithPriority(&c.train_aux[0], cudaStreamNonBlocking, greatest));
+    GDF_CUDA(cudaStreamCreateWithPriority(&c.train_aux[1], cudaStreamNonBlocking, least));
+    for (cudaEvent_t& e : c.train_ev) GDF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
   return GDF_OK;
 }
 
@@ -646,7 +662,7 @@ gdf_status gdf_ctx_bytes(const gdf_ctx* ctx, int64_t* bytes) {
   b += c.feat_tiles * 128 * lf * 2 * 2;                       // inference feature tiles
   b += c.ws.capacity * 16 + 3 * static_cast<int64_t>(c.num_sms) * (c.net[0].n_mlp + c.net[1].n_mlp) +
        3 * gdf::kAdamBlocks * 8 + 64 + (c.ws.capacity + 127) / 128 * 128 * lf * 2 * 2 +
-       c.ws.capacity * lf * 4 + gdf::kStatBlocks * 8;          // training workspace
+       2 * c.ws.capacity * lf * 4 + gdf::kStatBlocks * 8;      // training workspace
   b += (c.lr_table_n[0] + c.lr_table_n[1]) * 4;
   b += c.host_cap * (9 * 4 + 1 + 4 * 4 + 4 * 4) + c.tool_cap * (9 + 2 + 4) * 4;
   b += c.pw.pixels * 2 + c.pw.df_cap * 28 * 4 + c.pw.nrc_cap * (15 + 1 + 1 + 3 + 15 + 3) * 4;
@@ -1131,8 +1147,14 @@ gdf_status train_step_dev(Context& c, const float* in_theta, const float* in_phi
   e = gdf::launch_df_fused(shape, gdf::kModeTrainFeat, p, gdf::train_ctas(c), st);
   if (e != cudaSuccess) return cuda_fail(e, "df_fused (train forward)");
 
-  // 2. backward of each network
-  for (int id = 0; id < 2; ++id) {
+  // 2.-3. backward of each network, then its optimizer step. The theta
+  // backward runs first; then the phi backward (one CTA per SM: its weight
+  // gradients fill the TMEM) on a high-priority stream, so its CTAs are
+  // placed first, beside the theta grid backward (fp32 atomics) on a second
+  // stream, which then runs the theta optimizer beside the phi grid
+  // backward. Each network has its own dL/dfeatures buffer; both streams
+  // join the caller's stream before the statistics.
+  auto backward = [&](int id, cudaStream_t sb) -> gdf_status {
     Net& nt = c.net[id];
     gdf::DfBwdParams b;
     std::memset(&b, 0, sizeof(b));
@@ -1146,7 +1168,7 @@ gdf_status train_step_dev(Context& c, const float* in_theta, const float* in_phi
     b.blob_bytes = nt.blob_bytes;
     b.grid = nt.w16 + nt.n_mlp;
     b.feat = c.ws.feat[id];
-    b.dx = c.ws.dx;
+    b.dx = c.ws.dx[id];
     b.dx_rows = c.ws.capacity;
     b.grid_grad = nt.grad + nt.n_mlp;
     b.wgrad_partial = c.ws.partial[id];
@@ -1154,32 +1176,45 @@ gdf_status train_step_dev(Context& c, const float* in_theta, const float* in_phi
     b.hidden = nt.hidden;
     b.err = c.d_err;
     b.gl = nt.gl;
-    e = gdf::launch_df_train_bwd(shape, id == 1, b, gdf::train_ctas(c), st);
-    if (e != cudaSuccess) return cuda_fail(e, "df_train_bwd");
+    const cudaError_t eb = gdf::launch_df_train_bwd(shape, id == 1, b, gdf::train_ctas(c), sb);
+    if (eb != cudaSuccess) return cuda_fail(eb, "df_train_bwd");
+    return GDF_OK;
+  };
+  auto grid_and_optimizer = [&](int id, cudaStream_t sb) -> gdf_status {
+    Net& nt = c.net[id];
     gdf::GridScatterParams g;
     std::memset(&g, 0, sizeof(g));
-    g.in = b.in;
-    g.in_stride = b.in_stride;
+    g.in = id == 0 ? in_theta : in_phi;
+    g.in_stride = id == 0 ? 9 : 10;
     g.fwd = c.ws.fwd;
     g.n = n;
     g.n_dev = n_dev;
-    g.dx = c.ws.dx;
+    g.dx = c.ws.dx[id];
     g.dx_rows = c.ws.capacity;
-    g.grid_grad = b.grid_grad;
+    g.grid_grad = nt.grad + nt.n_mlp;
     g.gl = nt.gl;
-    e = gdf::launch_grid_scatter(nt.levels, nt.features, g, st);
-    if (e != cudaSuccess) return cuda_fail(e, "grid_scatter");
-  }
-  // 3. Adam + EMA, re-layout of the weights
-  for (int id = 0; id < 2; ++id) {
+    cudaError_t eg = gdf::launch_grid_scatter(nt.levels, nt.features, g, sb);
+    if (eg != cudaSuccess) return cuda_fail(eg, "grid_scatter");
     gdf::AdamParams a = adam_params(c, id, c.cfg.adam_df, c.cfg.loss_scale,
                                     c.ws.sq + static_cast<size_t>(id) * gdf::kAdamBlocks, n_dev);
-    a.grid_grad = c.net[id].grad + c.net[id].n_mlp;
-    e = gdf::launch_adam_ema(a, st);
-    if (e != cudaSuccess) return cuda_fail(e, "adam_ema");
-    if (c.net[id].infer_f8 && (e = gdf::launch_pack_fp8(c.net[id].f8_pack, st)) != cudaSuccess)
-      return cuda_fail(e, "pack fp8");
-  }
+    a.grid_grad = nt.grad + nt.n_mlp;
+    eg = gdf::launch_adam_ema(a, sb);
+    if (eg != cudaSuccess) return cuda_fail(eg, "adam_ema");
+    if (nt.infer_f8 && (eg = gdf::launch_pack_fp8(nt.f8_pack, sb)) != cudaSuccess) return cuda_fail(eg, "pack fp8");
+    return GDF_OK;
+  };
+  gdf_status sg;
+  if ((sg = backward(0, st))) return sg;
+  cudaStream_t s_phi = c.train_aux[0], s_theta = c.train_aux[1];
+  GDF_CUDA(cudaEventRecord(c.train_ev[0], st));
+  GDF_CUDA(cudaStreamWaitEvent(s_phi, c.train_ev[0], 0));
+  GDF_CUDA(cudaStreamWaitEvent(s_theta, c.train_ev[0], 0));
+  if ((sg = backward(1, s_phi)) || (sg = grid_and_optimizer(0, s_theta)) || (sg = grid_and_optimizer(1, s_phi)))
+    return sg;
+  GDF_CUDA(cudaEventRecord(c.train_ev[1], s_phi));
+  GDF_CUDA(cudaEventRecord(c.train_ev[2], s_theta));
+  GDF_CUDA(cudaStreamWaitEvent(st, c.train_ev[1], 0));
+  GDF_CUDA(cudaStreamWaitEvent(st, c.train_ev[2], 0));
   // 4. FP64 loss and gradient-norm reductions
   e = gdf::launch_train_stats_mb(c.ws.fwd, n, n_dev, c.ws.sq, 2 * gdf::kAdamBlocks, c.ws.stat_part, c.ws.stats,
                                  loss_acc, st);

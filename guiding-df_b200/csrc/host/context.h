@@ -55,7 +55,7 @@ struct TrainWorkspace {
   double* stats = nullptr;                // [2]: loss sum, squared gradient norm
   unsigned long long* dropped = nullptr;  // [1]
   __half* feat[2] = {nullptr, nullptr};   // [capacity rounded to 128 x L*F] per DF network
-  float* dx = nullptr;                    // [L][capacity][F] dL/dgrid-features of one network
+  float* dx[2] = {nullptr, nullptr};      // [L][capacity][F] dL/dgrid-features per DF network
   double* stat_part = nullptr;            // [kStatBlocks] per-block loss sums
 };
 
@@ -112,6 +112,11 @@ struct Context {
   uint8_t* host_g = nullptr;     // [host_cap]
   float* host_u = nullptr;       // [host_cap x 4]
   float* host_wi = nullptr;      // [host_cap x 4]
+  // the training step's second half: [0] the phi backward, grid backward and
+  // optimizer (high priority), [1] the theta grid backward and optimizer;
+  // events [0] fork, [1], [2] joins
+  cudaStream_t train_aux[2] = {nullptr, nullptr};
+  cudaEvent_t train_ev[3] = {nullptr, nullptr, nullptr};
   // gdf_infer_host's streams: [0] input copies, [1] kernels, [2] output copies
   cudaStream_t pipe[3] = {nullptr, nullptr, nullptr};
   // Adam step sizes by per-parameter step counter: [0] DF optimizer, [1] NRC
