@@ -113,7 +113,7 @@ struct Context {
   float* host_u = nullptr;       // [host_cap x 4]
   float* host_wi = nullptr;      // [host_cap x 4]
   // the training step's second half: [0] the phi backward, grid backward and
-  // optimizer (high priority), [1] the theta grid backward and optimizer;
+  // optimizer, [1] the theta grid backward and optimizer;
   // events [0] fork, [1], [2] joins
   cudaStream_t train_aux[2] = {nullptr, nullptr};
   cudaEvent_t train_ev[3] = {nullptr, nullptr, nullptr};
