@@ -54,6 +54,13 @@ TRAIN_BATCH = {"full": 262144, "small": 65536}
 # forward + data gradient + weight gradient of both networks (the backward's
 # forward recomputation is an implementation cost, not counted)
 TRAIN_FLOP_PER_RECORD = {k: 3 * v for k, v in FLOP_PER_QUERY.items()}
+# MLP parameters of the theta + phi networks (tcnn pads input widths to 16);
+# the rest of a network's parameters are its grid tables
+MLP_PARAMS = {"full": (64 * 64 + 3 * 64 * 64 + 64 * 64) + (80 * 64 + 3 * 64 * 64 + 64 * 64),
+              "small": (48 * 64 + 2 * 64 * 64 + 64 * 32) + (64 * 64 + 2 * 64 * 64 + 64 * 32)}
+# grid-feature kernel, per query: the 3 position floats read, both networks'
+# fp16 features written (2 x levels x features x 2 B); plus the fp16 tables once
+FEATURE_BYTES_PER_QUERY = {"full": 12 + 2 * 16 * 2 * 2, "small": 12 + 2 * 8 * 2 * 2}
 METRIC = "guided queries/s"
 
 
@@ -304,8 +311,9 @@ def main():
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream()
 
-    def step(offset):
-        ctx.infer(q, wi, guided=guided, seed=7, offset=offset, n=n, stream=stream)
+    def step(offset, stages=None):
+        ctx.infer_ex(wi, n=n, queries=q, guided=guided, seed=7, offset=offset, stream=stream,
+                     stage_events=stages)
 
     for i in range(args.warmup):
         wi.copy_(wi0)
@@ -317,7 +325,7 @@ def main():
     clocks = ClockSampler(local_rank)
     clocks.start()
     time.sleep(0.3)
-    times = []
+    times, stage_ms = [], []
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -325,11 +333,16 @@ def main():
         wi.copy_(wi0)
         flush.zero_()
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        # the call re-records these after its grid-feature and fused launches
+        mid = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        for m_ in mid:
+            m_.record(stream)
         s.record(stream)
-        step(1000 + i)
+        step(1000 + i, mid)
         e.record(stream)
         e.synchronize()
         times.append(s.elapsed_time(e))
+        stage_ms.append((s.elapsed_time(mid[0]), mid[0].elapsed_time(mid[1])))
     torch.cuda.synchronize()
     ctx.sync(stream)
     if dist:
@@ -417,9 +430,11 @@ def main():
         serving = time_serving(W, rank, dev, args)
     clk = clocks.stop()
     ctx.sync(stream)
+    kern = {"stage_ms": stage_ms,
+            "grid_bytes": 2 * (ctx.n_params(0) + ctx.n_params(1) - MLP_PARAMS[args.workload])}
     _report(args, rank, world, dist, dev, n, cfg, params, times, e2e_times, train_times, rec_times,
             last, n_rec, rec_bytes, clk, nb, workload_name, threads, q_h, wi_h, guided_h, form_times,
-            grouped, serving, pcie, refgpu)
+            grouped, serving, pcie, refgpu, kern)
     ctx.close()
     if dist:
         dist.destroy_process_group()
@@ -811,13 +826,16 @@ def job_rate(units_per_rank, world, ms):
 
 def _report(args, rank, world, dist, dev, n, cfg, params, times, e2e_times, train_times, rec_times,
             last, n_rec, rec_bytes, clk, nb, workload_name, threads, q_h, wi_h, guided_h, form_times,
-            grouped, serving, pcie=None, refgpu=None):
+            grouped, serving, pcie=None, refgpu=None, kern=None):
     import torch
     ms = statistics.mean(times)
+    ms_feat = statistics.mean(t[0] for t in kern["stage_ms"])
+    ms_fused = statistics.mean(t[1] for t in kern["stage_ms"])
     ms_e2e = statistics.mean(e2e_times) if e2e_times else float("nan")
     ms_train = statistics.mean(train_times) if train_times else float("nan")
     ms_rec = statistics.mean(rec_times) if rec_times else float("nan")
-    ms, ms_e2e, ms_train, ms_rec = max_over_ranks([ms, ms_e2e, ms_train, ms_rec], dist, dev)
+    ms, ms_e2e, ms_train, ms_rec, ms_feat, ms_fused = max_over_ranks(
+        [ms, ms_e2e, ms_train, ms_rec, ms_feat, ms_fused], dist, dev)
     value = job_rate(n, world, ms)
     e2e_value = job_rate(n, world, ms_e2e)
     h2d = q_h.nbytes + wi_h.nbytes + guided_h.nbytes
@@ -827,10 +845,28 @@ def _report(args, rank, world, dist, dev, n, cfg, params, times, e2e_times, trai
         peaks = load_peaks()
         flops = FLOP_PER_QUERY[args.workload] * n
         achieved = flops / (ms * 1e-3) / 1e12  # average launch duration
-        traffic = None
+        traffic, k_traffic = None, {}
         prof = os.path.join(ROOT, "profiles", f"infer_step_{args.workload}.json")
         if os.path.exists(prof):
-            traffic = json.load(open(prof)).get("dram_bytes_per_step")
+            pj = json.load(open(prof))
+            traffic = pj.get("dram_bytes_per_step")
+            k_traffic = pj.get("dram_bytes", {})
+        # per kernel, each against its own CUDA-event duration in this run
+        fused_tf = flops / (ms_fused * 1e-3) / 1e12
+        feat_bytes = FEATURE_BYTES_PER_QUERY[args.workload] * n + kern["grid_bytes"]
+        feat_gbs = feat_bytes / (ms_feat * 1e-3) / 1e9
+        kernels = [
+            {"kernel": "df_fused_kernel", "bound": "tensor", "achieved": fused_tf, "peak": peaks["bf16_tflops"],
+             "unit": "TFLOP/s", "frac": fused_tf / peaks["bf16_tflops"], "traffic": k_traffic.get("df_fused_kernel"),
+             "ms": ms_fused, "algorithmic": f"{FLOP_PER_QUERY[args.workload]} flop per query (theta + phi MLPs)"},
+            {"kernel": "grid_features_kernel", "bound": "hbm", "achieved": feat_gbs, "peak": peaks["hbm_gbs"],
+             "unit": "GB/s", "frac": feat_gbs / peaks["hbm_gbs"], "traffic": k_traffic.get("grid_features_kernel"),
+             "ms": ms_feat,
+             "algorithmic": f"{FEATURE_BYTES_PER_QUERY[args.workload]} B per query (positions read, both "
+                            f"networks' fp16 features written) + {kern['grid_bytes']} B of fp16 tables; its "
+                            f"measured bound is the L1-to-L2 request rate of the random gathers, not HBM"},
+        ]
+        dominant = max(kernels, key=lambda k: k["ms"])
         if args.cpu_seconds > 0:
             cpu_v, cpu_n, cpu_s = cpu_sample(cfg, params, args.cpu_seconds, threads)
         else:
@@ -843,10 +879,14 @@ def _report(args, rank, world, dist, dev, n, cfg, params, times, e2e_times, trai
                        "parallelism": f"replicas x{world}"},
             "e2e": {"value": e2e_value, "unit": "queries/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e},
-            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peaks["bf16_tflops"],
-                         "unit": "TFLOP/s", "frac": achieved / peaks["bf16_tflops"], "traffic": traffic,
-                         "peak_source": peaks["source"], "kernel": "gdf_infer: grid_features_kernel + df_fused_kernel",
-                         "flop_per_query": FLOP_PER_QUERY[args.workload]},
+            "roofline": {**{k: dominant[k] for k in ("bound", "achieved", "peak", "unit", "frac", "traffic",
+                                                      "kernel", "ms")},
+                         "peak_source": peaks["source"],
+                         "dominant": "the longer of the step's two kernels in this run",
+                         "kernels": kernels,
+                         "step": {"kernels": "grid_features_kernel + df_fused_kernel", "achieved": achieved,
+                                  "unit": "TFLOP/s", "frac": achieved / peaks["bf16_tflops"],
+                                  "traffic": traffic}},
             "cpu_baseline": {"value": cpu_v, "unit": "queries/s", "cores": threads, "kind": "reference",
                              "sample": f"{cpu_n} queries ({cpu_s:.1f} s): the bounce's first 131,072 queries "
                                        f"repeated; reference epilogue (train.h) compiled for the host after a "

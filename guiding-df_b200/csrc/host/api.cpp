@@ -828,9 +828,13 @@ gdf_status gdf_infer_ex(gdf_ctx* ctx, const gdf_infer_args* a, void* stream) {
   if ((s = grid_features(ctx->c, a->queries_dev, a->shading, a->aabb, n, p,
                          static_cast<cudaStream_t>(stream))))
     return s;
+  if (a->stage_events)
+    GDF_CUDA(cudaEventRecord(static_cast<cudaEvent_t>(a->stage_events[0]), static_cast<cudaStream_t>(stream)));
   cudaError_t e = gdf::launch_df_fused(df_shape(ctx->c), gdf::kModeInfer, p, ctx->c.num_sms,
                                        static_cast<cudaStream_t>(stream));
   if (e != cudaSuccess) return cuda_fail(e, "df_fused (infer)");
+  if (a->stage_events)
+    GDF_CUDA(cudaEventRecord(static_cast<cudaEvent_t>(a->stage_events[1]), static_cast<cudaStream_t>(stream)));
   return GDF_OK;
 }
 

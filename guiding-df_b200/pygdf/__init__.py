@@ -95,7 +95,7 @@ class InferArgs(C.Structure):
                 ("guided_dev", C.c_void_p), ("uniforms_dev", C.c_void_p),
                 ("philox_seed", C.c_uint64), ("philox_offset", C.c_uint64),
                 ("wi_dev", C.c_void_p), ("dir_pdf_dev", C.c_void_p), ("n", C.c_int64),
-                ("cdf_norm_err_dev", C.c_void_p)]
+                ("cdf_norm_err_dev", C.c_void_p), ("stage_events", C.c_void_p)]
 
 
 def path_state(fields: dict, cur_depth) -> PathState:
@@ -366,7 +366,10 @@ class Context:
         return st
 
     def infer_ex(self, wi, n=None, queries=None, shading: "Shading | None" = None, aabb=None,
-                 guided=None, uniforms=None, seed=0, offset=0, dir_pdf=None, norm_err=None, stream=None):
+                 guided=None, uniforms=None, seed=0, offset=0, dir_pdf=None, norm_err=None, stream=None,
+                 stage_events=None):
+        """stage_events: two recorded torch.cuda.Event objects (timing) that
+        the call re-records after the grid-feature and the fused launch."""
         n = wi.shape[0] if n is None else n
         a = InferArgs()
         a.queries_dev = _ptr(queries)
@@ -382,6 +385,10 @@ class Context:
         a.dir_pdf_dev = _ptr(dir_pdf)
         a.n = n
         a.cdf_norm_err_dev = _ptr(norm_err)
+        if stage_events is not None:
+            evs = (C.c_void_p * 2)(*[e.cuda_event for e in stage_events])
+            a.stage_events = C.cast(evs, C.c_void_p)
+            a._keep_events = evs
         check(lib().gdf_infer_ex(self.h, C.byref(a), _stream(stream)))
 
     def build_train_records(self, st: PathState, aabb: Aabb, px: TrainPixels, in_theta, in_phi,

@@ -244,13 +244,18 @@ typedef struct gdf_infer_args {
   float* dir_pdf_dev;
   int64_t n;
   double* cdf_norm_err_dev;
+  /* nullable: two cudaEvent_t that the call records on `stream`, after the
+   * grid-feature launch and after the fused launch, so that a caller can
+   * time each kernel (no counterpart in the reference) */
+  void* const* stage_events;
 } gdf_infer_args;
 gdf_status gdf_infer_ex(gdf_ctx* ctx, const gdf_infer_args* args, void* stream);
 
 /* gdf_infer on HOST buffers, for callers whose queries live in host memory:
  * the inputs are copied in, inferred and the guiding data copied back in
- * chunks of 524,288 queries pipelined over two internal streams, so the
- * transfers overlap the kernels. Results are identical to gdf_infer on the
+ * chunks of at most 524,288 queries pipelined over three internal streams
+ * (input copies, kernels, output copies), so the transfers overlap the
+ * kernels. Results are identical to gdf_infer on the
  * same data (the in-kernel Philox counter continues across chunks).
  *   queries_h [n x 9], guided_h [n] (nullable), uniforms_h [n x 4]
  *   (nullable), wi_in_h / wi_out_h [n x 4] (may alias); page-locked host
