@@ -346,8 +346,10 @@ gdf_status alloc_ws(Context& c) {
                       static_cast<size_t>(c.net[0].features);
   const size_t dx = static_cast<size_t>(cap) * static_cast<size_t>(c.net[0].levels) *
                     static_cast<size_t>(c.net[0].features);
+  // dx[1] (the phi network's own dL/dfeatures) comes with the first
+  // training step that runs the two networks' second halves side by side
   if ((s = dalloc(&w.feat[0], feat)) || (s = dalloc(&w.feat[1], feat)) || (s = dalloc(&w.dx[0], dx)) ||
-      (s = dalloc(&w.dx[1], dx)) || (s = dalloc(&w.stat_part, gdf::kStatBlocks)))
+      (s = dalloc(&w.stat_part, gdf::kStatBlocks)))
     return s;
   if (!c.train_aux[0]) {
     for (cudaStream_t& ts : c.train_aux) GDF_CUDA(cudaStreamCreateWithFlags(&ts, cudaStreamNonBlocking));
@@ -659,7 +661,7 @@ gdf_status gdf_ctx_bytes(const gdf_ctx* ctx, int64_t* bytes) {
   b += c.feat_tiles * 128 * lf * 2 * 2;                       // inference feature tiles
   b += c.ws.capacity * 16 + 3 * static_cast<int64_t>(c.num_sms) * (c.net[0].n_mlp + c.net[1].n_mlp) +
        3 * gdf::kAdamBlocks * 8 + 64 + (c.ws.capacity + 127) / 128 * 128 * lf * 2 * 2 +
-       2 * c.ws.capacity * lf * 4 + gdf::kStatBlocks * 8;      // training workspace
+       (c.ws.dx[1] ? 2 : 1) * c.ws.capacity * lf * 4 + gdf::kStatBlocks * 8;  // training workspace
   b += (c.lr_table_n[0] + c.lr_table_n[1]) * 4;
   b += c.host_cap * (9 * 4 + 1 + 4 * 4 + 4 * 4) + c.tool_cap * (9 + 2 + 4) * 4;
   b += c.pw.pixels * 2 + c.pw.df_cap * 28 * 4 + c.pw.nrc_cap * (15 + 1 + 1 + 3 + 15 + 3) * 4;
@@ -1170,7 +1172,7 @@ gdf_status train_step_dev(Context& c, const float* in_theta, const float* in_phi
     b.blob_bytes = nt.blob_bytes;
     b.grid = nt.w16 + nt.n_mlp;
     b.feat = c.ws.feat[id];
-    b.dx = c.ws.dx[id];
+    b.dx = c.ws.dx[c.train_one_stream ? 0 : id];
     b.dx_rows = c.ws.capacity;
     b.grid_grad = nt.grad + nt.n_mlp;
     b.wgrad_partial = c.ws.partial[id];
@@ -1191,7 +1193,7 @@ gdf_status train_step_dev(Context& c, const float* in_theta, const float* in_phi
     g.fwd = c.ws.fwd;
     g.n = n;
     g.n_dev = n_dev;
-    g.dx = c.ws.dx[id];
+    g.dx = c.ws.dx[c.train_one_stream ? 0 : id];
     g.dx_rows = c.ws.capacity;
     g.grid_grad = nt.grad + nt.n_mlp;
     g.gl = nt.gl;
@@ -1207,6 +1209,12 @@ gdf_status train_step_dev(Context& c, const float* in_theta, const float* in_phi
   };
   gdf_status sg;
   if ((sg = backward(0, st))) return sg;
+  if (c.train_one_stream) {  // one stream: both networks share dx[0]
+    if ((sg = grid_and_optimizer(0, st)) || (sg = backward(1, st)) || (sg = grid_and_optimizer(1, st))) return sg;
+  } else {
+  if (!c.ws.dx[1] && (sg = dalloc(&c.ws.dx[1], static_cast<size_t>(c.ws.capacity) *
+                                                   static_cast<size_t>(c.net[0].levels * c.net[0].features))))
+    return sg;
   cudaStream_t s_phi = c.train_aux[0], s_theta = c.train_aux[1];
   GDF_CUDA(cudaEventRecord(c.train_ev[0], st));
   GDF_CUDA(cudaStreamWaitEvent(s_phi, c.train_ev[0], 0));
@@ -1217,6 +1225,7 @@ gdf_status train_step_dev(Context& c, const float* in_theta, const float* in_phi
   GDF_CUDA(cudaEventRecord(c.train_ev[2], s_theta));
   GDF_CUDA(cudaStreamWaitEvent(st, c.train_ev[1], 0));
   GDF_CUDA(cudaStreamWaitEvent(st, c.train_ev[2], 0));
+  }
   // 4. FP64 loss and gradient-norm reductions
   e = gdf::launch_train_stats_mb(c.ws.fwd, n, n_dev, c.ws.sq, 2 * gdf::kAdamBlocks, c.ws.stat_part, c.ws.stats,
                                  loss_acc, st);

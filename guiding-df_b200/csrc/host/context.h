@@ -96,6 +96,9 @@ struct Context {
   // CTAs of the training step's persistent kernels (0: one per SM). A server
   // that keeps SMs free for inference while training runs lowers it.
   int train_ctas = 0;
+  // the training step's second half on the caller's stream alone, not
+  // forked over train_aux (a server, whose other slots fill the device)
+  bool train_one_stream = false;
   Net net[3];  // theta, phi, nrc
   uint32_t* d_err = nullptr;  // device error word of bounded waits
   TrainWorkspace ws;

@@ -148,10 +148,15 @@ void admit(gdf_server* s) {
     Slot& sl = s->slots[free_slots[used_slots++]];
     q->slot = static_cast<int>(&sl - s->slots.data());
     gdf_ctx* inst = q->r.instance;
-    // training's persistent kernels leave train_sm_reserve SMs to inference
+    // training's persistent kernels leave train_sm_reserve SMs to inference;
+    // the step stays on its slot's stream (the other slots fill the device,
+    // and forking every instance's steps over more streams lengthened the
+    // latency tail: slowdown p99 127-654 against 74-138)
     inst->c.train_ctas = s->cfg.train_sm_reserve > 0 ? inst->c.num_sms - s->cfg.train_sm_reserve : 0;
+    inst->c.train_one_stream = true;
     q->status = gdf_train_step(inst, q->r.in_theta_dev, q->r.in_phi_dev, q->r.target_dev, q->r.n, nullptr, sl.stream);
     inst->c.train_ctas = 0;
+    inst->c.train_one_stream = false;
     if (q->status) q->msg = gdf_last_error();
     // the step's FP64 statistics and the instance's device error flag, read
     // back without blocking the scheduler

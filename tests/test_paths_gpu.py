@@ -300,6 +300,22 @@ def test_train_paths_async_captures_into_a_graph():
     ctx2.close()
 
 
+def test_train_paths_below_min_batch_trains_nothing():
+    """A frame with fewer records than min_train_batch: the batch loop breaks
+    at once (learnedDistribution.cpp:232-233), so the weights and the
+    optimizer step stay as they were and the loss is 0 / batches = 0."""
+    fields, depth = W.path_state(2000, 17)
+    cfg, ctx = _ctx()
+    _, _, st = _state_dev(fields, depth)
+    before = [ctx.get_params(k) for k in (0, 1)]
+    loss, n = ctx.train_paths(st, pygdf.Aabb.of(*AABB), _px(2000))
+    assert 0 < n < cfg.min_train_batch and loss == 0.0
+    for k in (0, 1):
+        np.testing.assert_array_equal(ctx.get_params(k), before[k])
+        assert ctx.get_optimizer_state(k)[3] == 0
+    ctx.close()
+
+
 def test_infer_ex_shading_equals_prepared_queries():
     cfg, ctx = _ctx(pygdf.PRESET_FULL)
     rng = np.random.default_rng(3)
