@@ -703,22 +703,35 @@ def time_serving(W, rank, dev, args):
     for rep in range(SERVE_RUNS):
         srv.stats(reset=True)
         reqs = draw(1000)
-        tickets = []
+        tickets, t_sub = [], []
         t0 = time.perf_counter()
         next_t = t0
         for i, r in enumerate(reqs):
             next_t += rng.exponential(1.0 / rate)
             while time.perf_counter() < next_t:
                 pass
+            t_sub.append(time.perf_counter())
             tickets.append(submit(*r, 10000 * (rep + 1) + i))
         lat = np.array([srv.wait(t)[1] for t in tickets])
         st = srv.stats(reset=True)
         slow = lat / np.array([iso_ms(k, n, tr) for k, n, tr in reqs])
         is_tr = np.array([tr for _, _, tr in reqs])
+        # requests that found an earlier request of their own instance still
+        # in flight (same networks: they run in submission order)
+        t_sub = np.array(t_sub)
+        t_done = t_sub + lat * 1e-3
+        queued = np.zeros(len(reqs), bool)
+        last_done = {}
+        for i, (k, _, _) in enumerate(reqs):
+            queued[i] = last_done.get(k, -1.0) > t_sub[i]
+            last_done[k] = max(last_done.get(k, -1.0), t_done[i])
         runs.append({"p50_ms": st.p50_ms, "p99_ms": st.p99_ms, "max_ms": st.max_ms,
                      "p99_over_p50": st.p99_ms / st.p50_ms if st.p50_ms > 0 else None,
                      "slowdown": {**pct(slow), "p99_over_p50": float(np.percentile(slow, 99) / np.percentile(slow, 50))},
                      "inference_ms": pct(lat[~is_tr]), "training_ms": pct(lat[is_tr]),
+                     "behind_own_instance": {"requests": int(queued.sum()),
+                                             "slowdown": pct(slow[queued]) if queued.any() else None,
+                                             "slowdown_of_the_rest": pct(slow[~queued])},
                      "throughput": st.queries_per_s, "frac_of_peak": st.queries_per_s / peak.queries_per_s,
                      "requests": st.requests})
 
