@@ -1212,19 +1212,20 @@ gdf_status train_step_dev(Context& c, const float* in_theta, const float* in_phi
   if (c.train_one_stream) {  // one stream: both networks share dx[0]
     if ((sg = grid_and_optimizer(0, st)) || (sg = backward(1, st)) || (sg = grid_and_optimizer(1, st))) return sg;
   } else {
-  if (!c.ws.dx[1] && (sg = dalloc(&c.ws.dx[1], static_cast<size_t>(c.ws.capacity) *
-                                                   static_cast<size_t>(c.net[0].levels * c.net[0].features))))
-    return sg;
-  cudaStream_t s_phi = c.train_aux[0], s_theta = c.train_aux[1];
-  GDF_CUDA(cudaEventRecord(c.train_ev[0], st));
-  GDF_CUDA(cudaStreamWaitEvent(s_phi, c.train_ev[0], 0));
-  GDF_CUDA(cudaStreamWaitEvent(s_theta, c.train_ev[0], 0));
-  if ((sg = backward(1, s_phi)) || (sg = grid_and_optimizer(0, s_theta)) || (sg = grid_and_optimizer(1, s_phi)))
-    return sg;
-  GDF_CUDA(cudaEventRecord(c.train_ev[1], s_phi));
-  GDF_CUDA(cudaEventRecord(c.train_ev[2], s_theta));
-  GDF_CUDA(cudaStreamWaitEvent(st, c.train_ev[1], 0));
-  GDF_CUDA(cudaStreamWaitEvent(st, c.train_ev[2], 0));
+    if (!c.ws.dx[1] && (sg = dalloc(&c.ws.dx[1], static_cast<size_t>(c.ws.capacity) *
+                                                     static_cast<size_t>(c.net[0].levels * c.net[0].features))))
+      return sg;
+    cudaStream_t s_phi = c.train_aux[0], s_theta = c.train_aux[1];
+    GDF_CUDA(cudaEventRecord(c.train_ev[0], st));
+    GDF_CUDA(cudaStreamWaitEvent(s_phi, c.train_ev[0], 0));
+    GDF_CUDA(cudaStreamWaitEvent(s_theta, c.train_ev[0], 0));
+    if (!(sg = backward(1, s_phi)) && !(sg = grid_and_optimizer(0, s_theta))) sg = grid_and_optimizer(1, s_phi);
+    // both streams join the caller's, also after a failed launch
+    GDF_CUDA(cudaEventRecord(c.train_ev[1], s_phi));
+    GDF_CUDA(cudaEventRecord(c.train_ev[2], s_theta));
+    GDF_CUDA(cudaStreamWaitEvent(st, c.train_ev[1], 0));
+    GDF_CUDA(cudaStreamWaitEvent(st, c.train_ev[2], 0));
+    if (sg) return sg;
   }
   // 4. FP64 loss and gradient-norm reductions
   e = gdf::launch_train_stats_mb(c.ws.fwd, n, n_dev, c.ws.sq, 2 * gdf::kAdamBlocks, c.ws.stat_part, c.ws.stats,
