@@ -402,10 +402,11 @@ def main():
         rec_times, n_rec, rec_bytes = time_records(ctx, W, n, rank, dev, stream, flush, args)
     form_times = {}
     if "forms" in stages:
-        # the same bounce with the bf16 and FP8 inference forms
+        # the same bounce with the bf16 and FP8 inference forms (and the bf16
+        # form's training step)
         import pygdf
         for name, prec in (("bf16", pygdf.PREC_BF16), ("fp8", pygdf.PREC_FP8)):
-            cb, _, _ = make_context(args.workload, seed=1234 + rank, precision=prec)
+            cb, cfg_b, _ = make_context(args.workload, seed=1234 + rank, precision=prec)
             for i in range(args.warmup):
                 wi.copy_(wi0)
                 cb.infer(q, wi, guided=guided, seed=7, offset=i, n=n, stream=stream)
@@ -420,6 +421,10 @@ def main():
                 e.synchronize()
                 ts.append(s.elapsed_time(e))
             form_times[name] = ts
+            if name == "bf16" and "train" in stages:
+                # the bf16 form trains in bf16 as well
+                tt, _ = time_train(cb, cfg_b, W, nb, rank, dev, stream, flush, args)
+                form_times["bf16_train"] = tt
             cb.sync(stream)
             cb.close()
     grouped = None
@@ -929,10 +934,17 @@ def _report(args, rank, world, dist, dev, n, cfg, params, times, e2e_times, trai
         what = {"bf16": "bf16 MLP operands (fp32 accumulation)",
                 "fp8": "e4m3 hidden matrices, per-matrix and per-row power-of-two scales (fp32 accumulation)"}
         for name, ts in form_times.items():
+            if name == "bf16_train":
+                continue
             mb = statistics.mean(ts)
             line[name] = {"metric": "guided queries/s, " + what[name],
                           "value": job_rate(n, world, mb), "unit": "queries/s", "ms_per_step": mb,
                           "vs_fp16": ms / mb}
+        if "bf16_train" in form_times and "bf16" in line:
+            mt = statistics.mean(form_times["bf16_train"])
+            line["bf16"]["train"] = {"metric": "train samples/s, bf16 training form", "batch": nb,
+                                     "value": job_rate(nb, world, mt), "unit": "records/s",
+                                     "ms_per_step": mt, "vs_fp16": ms_train / mt if train_times else None}
         if refgpu:
             line["reference_gpu"] = refgpu
         if grouped:

@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
 #include "df_tile.cuh"
@@ -26,7 +27,16 @@ __device__ __forceinline__ void mma_steps(uint32_t d, uint32_t a_s, uint32_t a_l
   }
 }
 
-// ReLU'(forward activation) * accumulator -> fp16 -> D tile (64 columns).
+// Two floats from a packed pair of the operand format (fp16, or bf16).
+template <bool BF16>
+__device__ __forceinline__ float2 unpack2(uint32_t w) {
+  if constexpr (BF16) return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&w));
+  else return __half22float2(*reinterpret_cast<const __half2*>(&w));
+}
+
+// ReLU'(forward activation) * accumulator -> operand format -> D tile (64
+// columns); BF16: the bf16 training form.
+template <bool BF16 = false>
 __device__ __forceinline__ void dgrad_relu_to_tile(const tile::Wg& c, uint32_t taddr,
                                                    const uint8_t* h_tile, uint8_t* d_tile) {
 #pragma unroll
@@ -37,14 +47,14 @@ __device__ __forceinline__ void dgrad_relu_to_tile(const tile::Wg& c, uint32_t t
 #pragma unroll
     for (int kc = 0; kc < 4; ++kc) {
       const uint4 hv = *reinterpret_cast<const uint4*>(h_tile + tile::chunk_off(c.row, h * 4 + kc, 64));
-      const __half2* hh = reinterpret_cast<const __half2*>(&hv);
-      __half2 out[4];
+      const uint32_t hw[4] = {hv.x, hv.y, hv.z, hv.w};
+      uint32_t out[4];
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        const float2 f = __half22float2(hh[j]);
+        const float2 f = unpack2<BF16>(hw[j]);
         const float a = f.x > 0.f ? __uint_as_float(r[kc * 8 + 2 * j]) : 0.f;
         const float b = f.y > 0.f ? __uint_as_float(r[kc * 8 + 2 * j + 1]) : 0.f;
-        out[j] = __floats2half2_rn(a, b);
+        out[j] = tile::pack2(a, b, BF16);
       }
       *reinterpret_cast<uint4*>(d_tile + tile::chunk_off(c.row, h * 4 + kc, 64)) =
           *reinterpret_cast<uint4*>(out);
@@ -53,6 +63,7 @@ __device__ __forceinline__ void dgrad_relu_to_tile(const tile::Wg& c, uint32_t t
   tc_fence_before();
 }
 
+template <bool BF16 = false>
 __device__ __forceinline__ void relu_to(const tile::Wg& c, uint32_t taddr, uint8_t* dst) {
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
@@ -61,11 +72,11 @@ __device__ __forceinline__ void relu_to(const tile::Wg& c, uint32_t taddr, uint8
     tmem_ld_wait();
 #pragma unroll
     for (int kc = 0; kc < 4; ++kc) {
-      __half2 v[4];
+      uint32_t v[4];
 #pragma unroll
       for (int j = 0; j < 4; ++j)
-        v[j] = __floats2half2_rn(fmaxf(__uint_as_float(r[kc * 8 + 2 * j]), 0.f),
-                                 fmaxf(__uint_as_float(r[kc * 8 + 2 * j + 1]), 0.f));
+        v[j] = tile::pack2(fmaxf(__uint_as_float(r[kc * 8 + 2 * j]), 0.f),
+                           fmaxf(__uint_as_float(r[kc * 8 + 2 * j + 1]), 0.f), BF16);
       *reinterpret_cast<uint4*>(dst + tile::chunk_off(c.row, h * 4 + kc, 64)) = *reinterpret_cast<uint4*>(v);
     }
   }

@@ -214,7 +214,7 @@ gdf_status repack(Net& n, cudaStream_t st) {
                                        static_cast<int>(n.rows.size()), st, n.infer_bf16);
   if (e != cudaSuccess) return cuda_fail(e, "pack ema");
   e = gdf::launch_pack_mlp(n.w16, n.blob_w16, n.rows.data(), n.cols.data(),
-                           static_cast<int>(n.rows.size()), st);
+                           static_cast<int>(n.rows.size()), st, n.train_bf16);
   if (e != cudaSuccess) return cuda_fail(e, "pack w16");
   if (n.infer_f8 && (e = gdf::launch_pack_fp8(n.f8_pack, st)) != cudaSuccess) return cuda_fail(e, "pack fp8");
   return GDF_OK;
@@ -591,6 +591,8 @@ gdf_status gdf_create(const gdf_config* cfg, gdf_ctx** out) {
   if ((s = layout_df_net(c.cfg, 0, c.net[0])) || (s = layout_df_net(c.cfg, 1, c.net[1])))
     return cleanup(s);
   c.net[0].infer_bf16 = c.net[1].infer_bf16 = c.cfg.precision == GDF_PREC_BF16;
+  // the bf16 form trains in bf16 too: the training blob is bf16(fp16 copy)
+  c.net[0].train_bf16 = c.net[1].train_bf16 = c.cfg.precision == GDF_PREC_BF16;
   c.net[0].infer_f8 = c.net[1].infer_f8 = c.cfg.precision == GDF_PREC_FP8;
   if (c.cfg.nrc_enable && (s = layout_nrc_net(c.cfg, c.net[2]))) return cleanup(s);
   for (Net& n : c.net)
@@ -1093,6 +1095,7 @@ static gdf::AdamParams adam_params(Context& c, int id, const gdf_adam_config& a,
   p.lr_table = c.lr_table[id < 2 ? 0 : 1];
   p.lr_table_n = c.lr_table_n[id < 2 ? 0 : 1];
   p.blob_ema_bf16 = n.infer_bf16;
+  p.blob_w16_bf16 = n.train_bf16;
   p.err = c.d_err;
   return p;
 }
@@ -1119,7 +1122,8 @@ gdf_status train_step_dev(Context& c, const float* in_theta, const float* in_phi
   p.blob_phi = c.net[1].blob_w16;
   p.blob_theta_bytes = c.net[0].blob_bytes;
   p.blob_phi_bytes = c.net[1].blob_bytes;
-  p.bf16 = p.fp8 = 0;
+  p.bf16 = c.net[0].train_bf16 ? 1 : 0;
+  p.fp8 = 0;
   p.feat_theta = c.ws.feat[0];
   p.feat_phi = c.ws.feat[1];
   p.queries = in_theta;
@@ -1145,6 +1149,7 @@ gdf_status train_step_dev(Context& c, const float* in_theta, const float* in_phi
   tf.gl_phi = c.net[1].gl;
   tf.feat_theta = c.ws.feat[0];
   tf.feat_phi = c.ws.feat[1];
+  tf.bf16 = p.bf16;
   cudaError_t e = gdf::launch_train_features(shape, tf, st);
   if (e != cudaSuccess) return cuda_fail(e, "train_features");
   e = gdf::launch_df_fused(shape, gdf::kModeTrainFeat, p, gdf::train_ctas(c), st);
@@ -1180,6 +1185,7 @@ gdf_status train_step_dev(Context& c, const float* in_theta, const float* in_phi
     b.hidden = nt.hidden;
     b.err = c.d_err;
     b.gl = nt.gl;
+    b.bf16 = nt.train_bf16 ? 1 : 0;
     const cudaError_t eb = gdf::launch_df_train_bwd(shape, id == 1, b, gdf::train_ctas(c), sb);
     if (eb != cudaSuccess) return cuda_fail(eb, "df_train_bwd");
     return GDF_OK;

@@ -37,6 +37,7 @@ struct Net {
   __half* blob_w16 = nullptr;  // n_mlp, canonical layout of w16
   uint32_t blob_bytes = 0;
   bool infer_bf16 = false;     // blob_ema holds bf16 (bf16 inference form, DF networks)
+  bool train_bf16 = false;     // blob_w16 holds bf16 (bf16 training form, DF networks)
   // FP8 inference form (DF networks): e4m3 hidden matrices, rebuilt from
   // ema16 after every optimizer step (launch_pack_fp8)
   bool infer_f8 = false;

@@ -414,7 +414,11 @@ cudaError_t launch_t(int mode, const DfKernelParams& p, size_t smem, int num_sms
   int64_t ctas = (n_tiles + kDfWarpgroups - 1) / kDfWarpgroups;
   if (ctas > num_sms) ctas = num_sms;
   if (ctas < 1) ctas = 1;
-  const int fmt = (mode == kModeTrainFwd || mode == kModeTrainFeat) ? 0 : (p.fp8 ? 2 : (p.bf16 ? 1 : 0));
+  // the training forward with feature tiles has an fp16 and a bf16 form;
+  // the one with in-kernel gathers (static-workspace loss) fp16 only
+  const int fmt = mode == kModeTrainFwd ? 0
+                  : mode == kModeTrainFeat ? (p.bf16 ? 1 : 0)
+                                           : (p.fp8 ? 2 : (p.bf16 ? 1 : 0));
   auto pick = [&](auto k16, auto kb16, auto k8) { return fmt == 2 ? k8 : (fmt == 1 ? kb16 : k16); };
   auto kern = mode == kModeInfer
                   ? pick(df_fused_kernel<L, F, NBT, NBP, LIN, kModeInfer, kDfWarpgroups, 0>,
@@ -424,8 +428,10 @@ cudaError_t launch_t(int mode, const DfKernelParams& p, size_t smem, int num_sms
                   ? pick(df_fused_kernel<L, F, NBT, NBP, LIN, kModeEval, kDfWarpgroups, 0>,
                          df_fused_kernel<L, F, NBT, NBP, LIN, kModeEval, kDfWarpgroups, 1>,
                          df_fused_kernel<L, F, NBT, NBP, LIN, kModeEval, kDfWarpgroups, 2>)
-              : mode == kModeTrainFeat ? df_fused_kernel<L, F, NBT, NBP, LIN, kModeTrainFeat, kDfWarpgroups, 0>
-                                       : df_fused_kernel<L, F, NBT, NBP, LIN, kModeTrainFwd, kDfWarpgroups, 0>;
+              : mode == kModeTrainFeat
+                  ? (fmt == 1 ? df_fused_kernel<L, F, NBT, NBP, LIN, kModeTrainFeat, kDfWarpgroups, 1>
+                              : df_fused_kernel<L, F, NBT, NBP, LIN, kModeTrainFeat, kDfWarpgroups, 0>)
+                  : df_fused_kernel<L, F, NBT, NBP, LIN, kModeTrainFwd, kDfWarpgroups, 0>;
   cudaError_t e = allow_dynamic_smem(kern);
   if (e != cudaSuccess) return e;
   kern<<<static_cast<unsigned>(ctas), kDfThreads, smem, st>>>(p);

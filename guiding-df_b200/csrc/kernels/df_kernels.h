@@ -72,6 +72,7 @@ struct TrainFeatParams {
   GridLevels gl_theta, gl_phi;
   __half* feat_theta;        // [n_tiles][128 x L*F] canonical
   __half* feat_phi;
+  int32_t bf16;              // features rounded to bf16 (the bf16 training form)
 };
 
 struct GridFeatParams {

@@ -45,7 +45,7 @@ __host__ __device__ constexpr int pad16t(int v) { return (v + 15) / 16 * 16; }
 
 // dL/dlogits of one row into the D tile (fp16, 64 columns; first NB used).
 // compute_gradients_specialized_linear_interpolation / _nearest (AR.h:51-104).
-template <int NB, bool LINEAR>
+template <int NB, bool LINEAR, bool BF16>
 __device__ __noinline__ void dlogits_to_tile(uint32_t taddr, float u, float pdf_other, float prefix,
                                             bool ok, uint8_t* d_tile, uint32_t row) {
   float v[NB];
@@ -85,7 +85,7 @@ __device__ __noinline__ void dlogits_to_tile(uint32_t taddr, float u, float pdf_
   const float p1 = select_bin<NB>(v, cidx) * inv_res;
 #pragma unroll
   for (int kc = 0; kc < NB / 8; ++kc) {
-    __half2 out[4];
+    uint32_t out[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       float g[2];
@@ -103,9 +103,9 @@ __device__ __noinline__ void dlogits_to_tile(uint32_t taddr, float u, float pdf_
         }
         g[e] = ok ? multiplier * jj : 0.f;
       }
-      out[j] = __floats2half2_rn(g[0], g[1]);
+      out[j] = tile::pack2(g[0], g[1], BF16);
     }
-    *reinterpret_cast<uint4*>(d_tile + tile::chunk_off(row, kc, 64)) = *reinterpret_cast<uint4*>(out);
+    *reinterpret_cast<uint4*>(d_tile + tile::chunk_off(row, kc, 64)) = make_uint4(out[0], out[1], out[2], out[3]);
   }
 }
 
@@ -176,7 +176,9 @@ __global__ void __launch_bounds__(256) grid_scatter_kernel(const __grid_constant
   grid_backward_level<F>(p.gl, l, pos, dl, p.grid_grad);
 }
 
-template <int L, int F, int NB, bool LINEAR, bool PHI>
+// BF16: the bf16 training form (weights, grid features, encodings,
+// activations and gradients in bf16; fp32 accumulation).
+template <int L, int F, int NB, bool LINEAR, bool PHI, bool BF16>
 __global__ void __launch_bounds__(128, 1) df_train_bwd_kernel(const __grid_constant__ DfBwdParams p) {
   constexpr int LF = L * F;
   constexpr int K0 = PHI ? pad16t(LF + 40) : pad16t(LF + 28);
@@ -253,14 +255,15 @@ __global__ void __launch_bounds__(128, 1) df_train_bwd_kernel(const __grid_const
   auto t_g = [&](int l) { return tmem + (l == 0 ? 96u : 192u + 64u * static_cast<uint32_t>(l - 1)); };
   const uint32_t lane = c.lane_base;
 
-  constexpr uint32_t kIdFwd64 = idesc_f16(128, 64, 0, 0, 0);
-  constexpr uint32_t kIdFwdNB = idesc_f16(128, NB, 0, 0, 0);
-  constexpr uint32_t kIdDgrad = idesc_f16(128, 64, 0, 0, 1);    // B = W^T read MN-major
-  constexpr uint32_t kIdDx = idesc_f16(128, LF, 0, 0, 1);
-  constexpr uint32_t kIdWg64 = idesc_f16(64, 64, 0, 1, 1);      // A, B MN-major
-  constexpr uint32_t kIdWgF = idesc_f16(64, LF, 0, 1, 1);
-  constexpr uint32_t kIdWgR = idesc_f16(64, KR0, 0, 1, 1);
-  constexpr uint32_t kIdWgOut = idesc_f16(64, NB, 0, 1, 1);
+  constexpr uint32_t kFmt = BF16 ? 1u : 0u;  // A and B share one type
+  constexpr uint32_t kIdFwd64 = idesc_f16(128, 64, kFmt, 0, 0);
+  constexpr uint32_t kIdFwdNB = idesc_f16(128, NB, kFmt, 0, 0);
+  constexpr uint32_t kIdDgrad = idesc_f16(128, 64, kFmt, 0, 1);    // B = W^T read MN-major
+  constexpr uint32_t kIdDx = idesc_f16(128, LF, kFmt, 0, 1);
+  constexpr uint32_t kIdWg64 = idesc_f16(64, 64, kFmt, 1, 1);      // A, B MN-major
+  constexpr uint32_t kIdWgF = idesc_f16(64, LF, kFmt, 1, 1);
+  constexpr uint32_t kIdWgR = idesc_f16(64, KR0, kFmt, 1, 1);
+  constexpr uint32_t kIdWgOut = idesc_f16(64, NB, kFmt, 1, 1);
 
   bool first = true;
   for (int64_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
@@ -282,13 +285,13 @@ __global__ void __launch_bounds__(128, 1) df_train_bwd_kernel(const __grid_const
 
     // ---- forward: X = [XF | XR] | H_1 .. H_H | logits
     if constexpr (PHI) {
-      tile::sh_ob_to_tile(q, x_tile, c.row, 0, KR0);
+      tile::sh_ob_to_tile(q, x_tile, c.row, 0, KR0, BF16);
       float tw[12];
       triangle_wave_encode<12>(q[9], tw);
-      tile::store_run(x_tile, c.row, 28, KR0, tw, 12);
-      tile::ones_to_tile(x_tile, c.row, 40, KR0, KR0);
+      tile::store_run(x_tile, c.row, 28, KR0, tw, 12, BF16);
+      tile::ones_to_tile(x_tile, c.row, 40, KR0, KR0, BF16);
     } else {
-      tile::theta_rest_to_tile(q, x_tile, c.row, 0, KR0);
+      tile::theta_rest_to_tile(q, x_tile, c.row, 0, KR0, BF16);
     }
     mbar_wait(&bars[2], fphase, p.err, kErrMbarTimeout);
     fphase ^= 1u;
@@ -307,10 +310,10 @@ __global__ void __launch_bounds__(128, 1) df_train_bwd_kernel(const __grid_const
         mma_commit(c.bar);
       }
       tile::wait_mma(c);
-      if (l < H) relu_to(c, t_work + lane, h_tile(l + 1));
+      if (l < H) relu_to<BF16>(c, t_work + lane, h_tile(l + 1));
     }
     // ---- dL/dlogits -> D tile
-    dlogits_to_tile<NB, LINEAR>(t_work + lane, u_own, fabsf(PHI ? fw.x : fw.y), fw.z, ok, d_tile, c.row);
+    dlogits_to_tile<NB, LINEAR, BF16>(t_work + lane, u_own, fabsf(PHI ? fw.x : fw.y), fw.z, ok, d_tile, c.row);
 
     // ---- backward: output layer, hidden layers, first layer
     for (int l = H; l >= 0; --l) {
@@ -343,7 +346,7 @@ __global__ void __launch_bounds__(128, 1) df_train_bwd_kernel(const __grid_const
         mma_commit(c.bar);
       }
       tile::wait_mma(c);
-      if (l > 0) dgrad_relu_to_tile(c, t_work + lane, h_tile(l), d_tile);
+      if (l > 0) dgrad_relu_to_tile<BF16>(c, t_work + lane, h_tile(l), d_tile);
     }
     // every MMA reading XF has completed: the next tile's features
     if (c.leader && t + gridDim.x < n_tiles) fetch_features(t + gridDim.x);
@@ -407,18 +410,24 @@ __global__ void __launch_bounds__(128, 1) df_train_bwd_kernel(const __grid_const
   if (warp == 0) tmem_dealloc(tmem, 512);
 }
 
-template <int L, int F, int NB, bool LIN, bool PHI>
-cudaError_t launch_bwd_t(const DfBwdParams& p, int ctas, cudaStream_t st) {
+template <int L, int F, int NB, bool LIN, bool PHI, bool BF16>
+cudaError_t launch_bwd_f(const DfBwdParams& p, int ctas, cudaStream_t st) {
   constexpr int LF = L * F;
   constexpr int K0 = PHI ? pad16t(LF + 40) : pad16t(LF + 28);
   if (p.feat == nullptr) return cudaErrorInvalidValue;
   const size_t smem = ((p.blob_bytes + 127u) & ~127u) + 128u * K0 * 2u +
                       static_cast<size_t>(p.hidden + 1) * 128u * 64u * 2u + 64u;
-  auto k = df_train_bwd_kernel<L, F, NB, LIN, PHI>;
+  auto k = df_train_bwd_kernel<L, F, NB, LIN, PHI, BF16>;
   cudaError_t e = allow_dynamic_smem(k);
   if (e != cudaSuccess) return e;
   k<<<ctas, 128, smem, st>>>(p);
   return cudaGetLastError();
+}
+
+template <int L, int F, int NB, bool LIN, bool PHI>
+cudaError_t launch_bwd_t(const DfBwdParams& p, int ctas, cudaStream_t st) {
+  if (p.bf16) return launch_bwd_f<L, F, NB, LIN, PHI, true>(p, ctas, st);
+  return launch_bwd_f<L, F, NB, LIN, PHI, false>(p, ctas, st);
 }
 
 // ----------------------------------------------------------------- Adam
@@ -514,7 +523,12 @@ __global__ void __launch_bounds__(256) adam_ema_kernel(const __grid_constant__ A
     const uint32_t k = static_cast<uint32_t>(i - p.layer_off[l]);
     const uint32_t cols = static_cast<uint32_t>(p.layer_cols[l]);
     const uint32_t off = static_cast<uint32_t>(p.layer_off[l]) + canon_offset(k / cols, k % cols, cols);
-    p.blob_w16[off] = w16h;
+    if (p.blob_w16_bf16) {
+      const __nv_bfloat16 b = __float2bfloat16_rn(__half2float(w16h));
+      p.blob_w16[off] = *reinterpret_cast<const __half*>(&b);
+    } else {
+      p.blob_w16[off] = w16h;
+    }
     if (p.blob_ema_bf16) {
       const __nv_bfloat16 b = __float2bfloat16_rn(__half2float(emah));
       p.blob_ema[off] = *reinterpret_cast<const __half*>(&b);

@@ -114,8 +114,8 @@ __global__ void __launch_bounds__(256, 4) train_features_kernel(const __grid_con
     tile::grid_level<F>(p.gl_phi, l, p.gl_phi.interp, p.grid_phi, pp[0], pp[1], pp[2], fp);
 #pragma unroll
     for (int k = 0; k < F; k += 2) {
-      ot[(j * F + k) / 2] = tile::pack2(ft[k], ft[k + 1], false);
-      op[(j * F + k) / 2] = tile::pack2(fp[k], fp[k + 1], false);
+      ot[(j * F + k) / 2] = tile::pack2(ft[k], ft[k + 1], p.bf16 != 0);
+      op[(j * F + k) / 2] = tile::pack2(fp[k], fp[k + 1], p.bf16 != 0);
     }
   }
   const int64_t off = (row >> 7) * (128 * LF) +

@@ -90,6 +90,12 @@ extern "C" gdf_status gdf_train_loss_static(gdf_ctx* ctx, const float* in_theta,
                        .c_str());
     return GDF_ERR_INVALID_ARG;
   }
+  // its forward gathers the grid itself and runs fp16 operands only: the
+  // bf16 form's training weights are bf16
+  if (c.net[0].train_bf16) {
+    set_last_error("gdf_train_loss_static: not available for the bf16 precision form");
+    return GDF_ERR_UNSUPPORTED;
+  }
   void* base = nullptr;
   e = scratch_address(&base);
   if (e != cudaSuccess) {

@@ -30,6 +30,7 @@ struct DfBwdParams {
   int32_t hidden;           // tcnn n_hidden_layers
   uint32_t* err;
   GridLevels gl;
+  int32_t bf16;             // bf16 training form: bf16 weight blob, features and activations
 };
 
 // Grid backward of a batch (grid_scatter_kernel): dx from the backward.
@@ -85,6 +86,7 @@ struct AdamParams {
   const float* lr_table;
   int32_t lr_table_n;
   bool blob_ema_bf16;       // the inference blob holds bf16 (bf16 inference form)
+  bool blob_w16_bf16;       // the training blob holds bf16 (bf16 training form)
   uint32_t* err;            // device error word (bounded waits of the staged grid part)
 };
 

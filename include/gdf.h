@@ -104,7 +104,9 @@ typedef struct gdf_config {
   gdf_mlp_config mlp_nrc;
   gdf_adam_config adam_nrc; /* base_hashgrid_nrc_df.json optimizer          */
   float nrc_loss_scale;     /* TRAIN_LOSS_SCALE_NRC (parameters.h:62) = 1024 */
-  int32_t precision;        /* gdf_precision of the inference MLP layers     */
+  int32_t precision;        /* gdf_precision of the DF MLP layers: FP16 (the
+                               reference), BF16 (inference and training),
+                               FP8 (inference; training stays fp16)         */
   uint32_t seed;            /* parameter initialisation seed (7272)          */
   int64_t max_queries;      /* capacity of one inference call                */
   int64_t max_train_batch;  /* capacity of one training call                 */
@@ -342,6 +344,7 @@ gdf_status gdf_set_optimizer_state(gdf_ctx* ctx, int32_t net, const float* m_hos
  *     that first call before any stream capture, and do not reset the
  *     device (cudaDeviceReset) while the library is loaded;
  *   - the current device must be the context's (else GDF_ERR_INVALID_ARG);
+ *   - not for the BF16 precision form (GDF_ERR_UNSUPPORTED);
  *   - all calls share the one array: calls whose work overlaps on the GPU
  *     (other streams, other threads) race; order them on one stream. */
 gdf_status gdf_train_loss_static(gdf_ctx* ctx, const float* in_theta_dev, const float* in_phi_dev,

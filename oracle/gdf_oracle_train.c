@@ -28,6 +28,9 @@
 
 static int32_t pad16i(int32_t v) { return (v + 15) / 16 * 16; }
 static float h16(float x) { return go_round_f16(x); }
+/* a backward storage point of the MLP operand format (go_set_storage: fp16,
+ * the reference's; bf16 for the bf16 training form) */
+static float hst(float x) { return go_store(x); }
 
 /* fp16 pdf table of one network from its fp32 logits: logits stored as fp16
  * (tcnn output precision), softmax2 in float stored as fp16, times N in fp16
@@ -61,7 +64,7 @@ static void dlogits(const float* table, int n, int linear, float u, float pdf_ot
       const float pi = table[i] * inv_res;
       const float j0 = f == i ? p0 * (1.0f - p0) : -p0 * pi;
       const float j1 = c == i ? p1 * (1.0f - p1) : -p1 * pi;
-      out[i] = h16(multiplier * ((1.0f - w) * j0 + w * j1));
+      out[i] = hst(multiplier * ((1.0f - w) * j0 + w * j1));
     }
   } else {
     int f = (int)(u * (float)n);
@@ -69,7 +72,7 @@ static void dlogits(const float* table, int n, int linear, float u, float pdf_ot
     const float p0 = table[f] * inv_res;
     for (int i = 0; i < n; ++i) {
       const float pi = table[i] * inv_res;
-      out[i] = h16(multiplier * (f == i ? p0 * (1.0f - p0) : -p0 * pi));
+      out[i] = hst(multiplier * (f == i ? p0 * (1.0f - p0) : -p0 * pi));
     }
   }
 }
@@ -132,7 +135,7 @@ static void mlp_bwd_row(const float* w16, int k0, int width, int n_hidden, int n
   for (int c = 0; c < width; ++c) {
     double acc = 0.0;
     for (int r = 0; r < n_out_pad; ++r) acc += (double)dy[r] * w16[off[n_hidden] + (int64_t)r * width + c];
-    d[c] = hl[c] > 0.0f ? (double)h16(acc) : 0.0; /* backward activations stored as fp16 */
+    d[c] = hl[c] > 0.0f ? (double)hst(acc) : 0.0; /* backward activations stored as fp16 (bf16) */
   }
   for (int l = n_hidden - 1; l >= 1; --l) {
     const float* hp = hidden + (size_t)(l - 1) * width;
@@ -141,7 +144,7 @@ static void mlp_bwd_row(const float* w16, int k0, int width, int n_hidden, int n
     for (int c = 0; c < width; ++c) {
       double acc = 0.0;
       for (int r = 0; r < width; ++r) acc += d[r] * w16[off[l] + (int64_t)r * width + c];
-      dn[c] = hp[c] > 0.0f ? (double)h16(acc) : 0.0;
+      dn[c] = hp[c] > 0.0f ? (double)hst(acc) : 0.0;
     }
     memcpy(d, dn, sizeof(double) * (size_t)width);
   }

@@ -356,10 +356,14 @@ def pdf_tables(d: DfCfg, p_theta, p_phi, queries, u_theta, storage: str = "fp16"
     return a, b
 
 
-def df_train_grads(d: DfCfg, w_theta, w_phi, in_theta, in_phi, target, loss_scale=1024.0):
+def df_train_grads(d: DfCfg, w_theta, w_phi, in_theta, in_phi, target, loss_scale=1024.0,
+                   storage: str = "fp16"):
     """Gradients (scaled by loss_scale, FP64) of one DF training batch; the
-    weights are the fp32 masters, rounded here to the fp16 training copies."""
-    wt, wp = round_f16(w_theta), round_f16(w_phi)
+    weights are the fp32 masters, rounded here to the fp16 training copies.
+    storage "bf16": the bf16 training form's storage points (MLP matrices
+    bf16(fp16 copy), encoded inputs, activations, dL/dlogits and backward
+    activations in bf16; the pdf tables stay fp16)."""
+    wt, wp = df_weights(d, 0, w_theta, storage), df_weights(d, 1, w_phi, storage)
     a, b, t = f32(in_theta), f32(in_phi), f32(target)
     n = a.shape[0]
     gt = np.zeros(wt.size, np.float64)
@@ -368,8 +372,9 @@ def df_train_grads(d: DfCfg, w_theta, w_phi, in_theta, in_phi, target, loss_scal
     pdf = np.empty((n, 2), np.float32)
     dlt = np.empty((n, d.n_bins_theta), np.float32)
     dlp = np.empty((n, d.n_bins_phi), np.float32)
-    dropped = lib().go_df_train_grads(C.byref(d), _p(wt), _p(wp), _p(a), _p(b), _p(t), n, loss_scale,
-                                      _p(gt), _p(gp), _p(lik), _p(pdf), _p(dlt), _p(dlp))
+    with _storage(storage):
+        dropped = lib().go_df_train_grads(C.byref(d), _p(wt), _p(wp), _p(a), _p(b), _p(t), n, loss_scale,
+                                          _p(gt), _p(gp), _p(lik), _p(pdf), _p(dlt), _p(dlp))
     return dict(grad_theta=gt, grad_phi=gp, likelihood=lik, pdf=pdf, dlog_theta=dlt, dlog_phi=dlp,
                 dropped=int(dropped))
 

@@ -10,6 +10,9 @@
   activations; the fp16 EMA weights are the network): the pdf, sampled
   direction and divergence-loss error each format carries, reported and
   bounded.
+* The BF16 form also trains in bf16 (MLP weights, encoded inputs,
+  activations and gradients; fp32 accumulation and optimizer): one step's
+  loss and gradients against the FP64 oracle, next to the FP16 form's.
 """
 import numpy as np
 import pytest
@@ -155,4 +158,83 @@ def test_form_compensated_scans(form):
     e = float(err.cpu().item())
     print(storage, "max |1 - sum p / N| with compensated sums:", e)
     assert 0.0 <= e <= 4 * 2.0 ** -24, e
+    ctx.close()
+
+
+def _step_gradients(preset, prec, seed=3, n=8192):
+    from gdf_testutil import gen_weights
+    cfg = pygdf.default_config(preset)
+    cfg.precision = prec
+    ctx = pygdf.Context(cfg)
+    pt, pp = gen_weights(cfg, 0, seed, 1.2, 0.2), gen_weights(cfg, 1, seed + 1, 1.2, 0.2)
+    ctx.set_params(0, pt)
+    ctx.set_params(1, pp)
+    a, b, t = W.training_batch(n, seed + 7, cfg.n_bins_theta, cfg.pdf_interp == 0)
+    st = ctx.train_step(dev(a), dev(b), dev(t))
+    ctx.sync()
+    d = O.df_cfg_from(cfg)
+    beta1 = np.float64(np.float32(cfg.adam_df.beta1))
+    grads = []
+    for net, w0 in ((0, pt), (1, pp)):
+        m = ctx.get_optimizer_state(net)[0].astype(np.float64)
+        g = m / (1.0 - beta1)
+        n_mlp = O.df_mlp_params(d, net)
+        g[:n_mlp] -= np.float64(cfg.adam_df.l2_reg) * w0[:n_mlp]
+        grads.append((g, n_mlp))
+    ctx.close()
+    return cfg, st, grads, (pt, pp, a, b, t)
+
+
+@pytest.mark.parametrize("preset", [pygdf.PRESET_SMALL, pygdf.PRESET_FULL])
+def test_bf16_training_step(preset):
+    """One training step of the BF16 form: loss and gradients (recovered from
+    Adam's first moment) against the oracle run with the same storage points
+    (bf16 MLP matrices, encoded inputs, activations, dL/dlogits and backward
+    activations; fp16 pdf tables), as tight as the FP16 form against its
+    own; and, reported beside the FP16 form's, against the FP16 oracle (the
+    reference's storage points): the error the format carries. The weight
+    gradient sums records of both signs, so bf16's coarser storage (8
+    significand bits to fp16's 11) shows up there several times larger than
+    in any one term."""
+    cfg, st16, g16, data = _step_gradients(preset, pygdf.PREC_FP16)
+    _, stbf, gbf, _ = _step_gradients(preset, pygdf.PREC_BF16)
+    pt, pp, a, b, t = data
+    d = O.df_cfg_from(cfg)
+    ref16 = O.df_train_grads(d, pt, pp, a, b, t, cfg.loss_scale)
+    refbf = O.df_train_grads(d, pt, pp, a, b, t, cfg.loss_scale, storage="bf16")
+
+    def rel(x, y):
+        return float(np.linalg.norm(x - y) / (np.linalg.norm(y) + 1e-30))
+
+    def loss_err(st, ref):
+        lr = float(np.mean(ref["likelihood"].astype(np.float64)))
+        return abs(st.loss - lr) / abs(lr)
+
+    e16, ebf, ebf_fmt = loss_err(st16, ref16), loss_err(stbf, refbf), loss_err(stbf, ref16)
+    print(f"loss rel error: fp16 form vs its oracle {e16:.2e}; bf16 form vs its oracle {ebf:.2e}, "
+          f"vs the fp16 oracle {ebf_fmt:.2e}")
+    assert e16 < 1e-4 and ebf < 1e-4, (e16, ebf)
+    for net, key in ((0, "grad_theta"), (1, "grad_phi")):
+        (x16, n_mlp), (xbf, _) = g16[net], gbf[net]
+        r16g, rbfg = ref16[key] / cfg.loss_scale, refbf[key] / cfg.loss_scale
+        for part, name in ((slice(0, n_mlp), "mlp"), (slice(n_mlp, None), "grid")):
+            a16, abf, fmt = rel(x16[part], r16g[part]), rel(xbf[part], rbfg[part]), rel(xbf[part], r16g[part])
+            print(f"net {net} {name} gradient rel error: fp16 form {a16:.2e}, bf16 form {abf:.2e} "
+                  f"(vs the fp16 oracle {fmt:.2e})")
+            assert a16 < 5e-3 and abf < 5e-3, (net, name, a16, abf)
+    assert stbf.n_records == st16.n_records and stbf.n_dropped == st16.n_dropped
+
+
+def test_bf16_training_reduces_loss():
+    """Steps of the BF16 form on one batch lower its loss, as the FP16 form's do."""
+    from gdf_testutil import gen_weights
+    cfg = pygdf.default_config(pygdf.PRESET_SMALL)
+    cfg.precision = pygdf.PREC_BF16
+    ctx = pygdf.Context(cfg)
+    ctx.set_params(0, gen_weights(cfg, 0, 5, 1.2, 0.2))
+    ctx.set_params(1, gen_weights(cfg, 1, 6, 1.2, 0.2))
+    a, b, t = (dev(x) for x in W.training_batch(8192, 9, cfg.n_bins_theta, cfg.pdf_interp == 0))
+    losses = [ctx.train_step(a, b, t).loss for _ in range(30)]
+    print("bf16 losses:", losses[0], losses[-1])
+    assert np.all(np.isfinite(losses)) and losses[-1] < losses[0]
     ctx.close()
