@@ -386,6 +386,8 @@ class Context:
         a.n = n
         a.cdf_norm_err_dev = _ptr(norm_err)
         if stage_events is not None:
+            if any(not e.cuda_event for e in stage_events):
+                raise ValueError("stage_events must be recorded once before use (torch creates them lazily)")
             evs = (C.c_void_p * 2)(*[e.cuda_event for e in stage_events])
             a.stage_events = C.cast(evs, C.c_void_p)
             a._keep_events = evs

@@ -213,3 +213,31 @@ def test_sync_status_clean_after_runs():
     ctx, _, _ = make_ctx(pygdf.PRESET_SMALL)
     ctx.sync()
     ctx.close()
+
+
+def test_stage_events_time_the_two_launches_and_change_nothing():
+    """gdf_infer_args.stage_events: the call records the two events after its
+    grid-feature and fused launches; the guiding data is the same as without
+    them, and the two stage times add up to the call."""
+    import torch
+    ctx, _, _ = make_ctx(pygdf.PRESET_FULL, seed=8)
+    n = 200000
+    q = dev(W.queries(n, 4))
+    wi0, guided = W.wi_init(n, 4, 0.7, 0.1)
+    g = dev(guided)
+    wa, wb = dev(wi0), dev(wi0)
+    ctx.infer_ex(wa, queries=q, guided=g, seed=2, offset=3)
+    stream = torch.cuda.current_stream()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    mid = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    for m in mid:
+        m.record(stream)
+    s.record(stream)
+    ctx.infer_ex(wb, queries=q, guided=g, seed=2, offset=3, stream=stream, stage_events=mid)
+    e.record(stream)
+    e.synchronize()
+    np.testing.assert_array_equal(wa.cpu().numpy(), wb.cpu().numpy())
+    t_feat, t_fused, t_all = s.elapsed_time(mid[0]), mid[0].elapsed_time(mid[1]), s.elapsed_time(e)
+    print(f"grid features {t_feat:.3f} ms, fused {t_fused:.3f} ms, call {t_all:.3f} ms")
+    assert t_feat > 0 and t_fused > 0 and t_feat + t_fused <= t_all * 1.001 + 1e-3
+    ctx.close()
