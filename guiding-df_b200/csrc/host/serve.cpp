@@ -6,10 +6,12 @@
 // many jobs share one GPU. One scheduler thread owns all CUDA work:
 //   * instances (gdf_ctx, registered by the caller) stay resident; their
 //     device footprint counts against the budget;
-//   * requests wait in arrival order; a request is admitted when its
-//     instance has no request on the device (requests of one instance run
-//     in submission order, as they read and write the same networks), a
-//     stream slot is free and its transient device memory fits the budget;
+//   * requests wait in arrival order; per instance, a training step (it
+//     writes the networks) is admitted once every earlier request of that
+//     instance is done, an inference request (it only reads) once no
+//     earlier training step of the instance is pending or running, so the
+//     inference requests between two steps may run together; each also
+//     needs a free stream slot and transient memory within the budget;
 //   * all inference requests admitted in one round run as one grouped
 //     launch (gdf_group_infer); each training request runs on its own
 //     stream, overlapping the inference;
@@ -77,7 +79,8 @@ struct gdf_server {
   std::thread worker;
   bool stop = false;
   std::vector<gdf_ctx*> instances;
-  std::unordered_map<gdf_ctx*, int> busy;  // requests of the instance on the device
+  std::unordered_map<gdf_ctx*, int> busy;        // requests of the instance on the device
+  std::unordered_map<gdf_ctx*, int> busy_train;  // ... of which training steps
   int64_t resident = 0, transient = 0;
   int max_train = 1, train_busy = 0;  // slots training may hold / holds
   std::deque<Request*> pending;
@@ -114,22 +117,36 @@ void admit(gdf_server* s) {
   if (free_slots.empty()) return;
   size_t slots_needed = 0;
   int64_t mem = s->resident + s->transient;
-  std::vector<gdf_ctx*> taken;  // instances whose next request must wait this round
+  // Per instance, in arrival order: a training step (it writes the
+  // networks) runs alone, after every earlier request and before every
+  // later one; inference requests (they only read) between two training
+  // steps may run together, in one grouped launch or beside each other.
+  struct Round {
+    bool blocked = false;  // an earlier request of the instance waits: so do the later ones
+    bool train = false;    // a training step of the instance was admitted this round
+    bool infer = false;    // an inference request of the instance was admitted this round
+  };
+  std::unordered_map<gdf_ctx*, Round> round;
   for (auto it = s->pending.begin(); it != s->pending.end();) {
     Request* q = *it;
     gdf_ctx* inst = q->r.instance;
-    const bool inst_busy = s->busy[inst] > 0 || std::find(taken.begin(), taken.end(), inst) != taken.end();
+    Round& ri = round[inst];
+    const bool is_infer = q->r.kind == GDF_REQ_INFER;
+    const bool inst_free = !ri.blocked && !ri.train &&
+                           (is_infer ? s->busy_train[inst] == 0 : (s->busy[inst] == 0 && !ri.infer));
     const bool mem_ok = mem + q->transient <= s->cfg.hbm_budget_bytes;
-    bool ok = !inst_busy && mem_ok;
-    if (ok && q->r.kind == GDF_REQ_INFER)
+    bool ok = inst_free && mem_ok;
+    if (ok && is_infer)
       ok = static_cast<int>(infer.size()) < s->cfg.max_batch && (!infer.empty() || slots_needed < free_slots.size());
-    if (ok && q->r.kind == GDF_REQ_TRAIN)
+    if (ok && !is_infer)
       ok = slots_needed < free_slots.size() && s->train_busy + static_cast<int>(train.size()) < s->max_train;
-    taken.push_back(inst);  // keeps arrival order per instance
     if (!ok) {
+      ri.blocked = true;  // keeps arrival order per instance
       ++it;
       continue;
     }
+    if (is_infer) ri.infer = true;
+    else ri.train = true;
     if (q->r.kind == GDF_REQ_INFER) {
       if (infer.empty()) ++slots_needed;
       infer.push_back(q);
@@ -141,6 +158,7 @@ void admit(gdf_server* s) {
     mem += q->transient;
     s->transient += q->transient;
     s->busy[inst] += 1;
+    if (!is_infer) s->busy_train[inst] += 1;
     it = s->pending.erase(it);
   }
   size_t used_slots = 0;
@@ -221,6 +239,7 @@ bool complete(gdf_server* s) {
       q->t_done = now;
       s->transient -= q->transient;
       s->busy[q->r.instance] -= 1;
+      if (q->r.kind == GDF_REQ_TRAIN) s->busy_train[q->r.instance] -= 1;
       s->latency_ms.push_back(std::chrono::duration<double, std::milli>(now - q->t_submit).count());
       s->queries_done += q->r.n;
       s->requests_done += 1;

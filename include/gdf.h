@@ -453,8 +453,11 @@ typedef struct gdf_server gdf_server;
 
 /* A request server over resident instances (no counterpart in the
  * reference, which guides one job per process). A scheduler thread admits
- * requests in arrival order as stream slots and budget allow -- requests
- * of one instance run in submission order, one at a time -- batches all
+ * requests in arrival order as stream slots and budget allow -- per
+ * instance, a training request runs after every earlier request and
+ * before every later one, while the inference requests between two
+ * training requests may run together (they only read the networks; give
+ * them distinct output buffers) -- batches all
  * inference requests admitted together into one grouped launch
  * (gdf_group_infer) and runs training requests on streams of their own, so
  * their work overlaps on the device. Instances must share the grid

@@ -178,3 +178,58 @@ def test_sm_reserve_is_validated():
         with pytest.raises(pygdf.GdfError):
             pygdf.Server(1 << 30, slots=2, max_batch=4, train_sm_reserve=bad)
     pygdf.Server(1 << 30, slots=2, max_batch=4, train_sm_reserve=sms - 1).close()
+
+
+def test_training_orders_the_inference_of_its_instance():
+    """Per instance: inference requests before a training request see the
+    weights before it, those after see the weights after it, and inference
+    requests between two training requests may run together. Before the
+    first step the results equal the same sequence run directly bit for
+    bit; after it the weights carry the step's float-atomic grid sums, so
+    at least 99 % of the rows must agree; and the last request, a repeat of
+    the first, must see other weights than the first."""
+    insts = _instances()[:1]
+    c = insts[0]
+    srv = pygdf.Server(pygdf.ctx_bytes(c) + (1 << 30), slots=4, max_batch=8)
+    srv.add_instance(c)
+    reqs = _infer_requests()[:4]
+    batch = _train_batches(c.cfg)[1][:2]
+    seq = [("i", 0), ("i", 1), ("t", 0), ("i", 2), ("i", 3), ("t", 1), ("i", 0)]
+    outs, tickets, keep = [], [], []
+    for kind, k in seq:
+        if kind == "i":
+            r = reqs[k]
+            wi_d, q_d, g_d = dev(r["wi"]), dev(r["q"]), dev(r["guided"])
+            keep += [q_d, g_d]
+            outs.append(wi_d)
+            tickets.append(srv.submit_infer(c, q_d, wi_d, guided=g_d, seed=r["seed"], offset=r["offset"]))
+        else:
+            a, b, t = (dev(x) for x in batch[k])
+            keep += [a, b, t]
+            outs.append(None)
+            tickets.append(srv.submit_train(c, a, b, t))
+    for t in tickets:
+        srv.wait(t)
+    srv.close()
+    alone = _instances()[0]
+    trained = False
+    for (kind, k), got in zip(seq, outs):
+        if kind == "i":
+            r = reqs[k]
+            wi_d = dev(r["wi"])
+            alone.infer(dev(r["q"]), wi_d, guided=dev(r["guided"]), seed=r["seed"], offset=r["offset"])
+            torch.cuda.synchronize()
+            x, y = got.cpu().numpy(), wi_d.cpu().numpy()
+            if not trained:
+                np.testing.assert_array_equal(x, y)
+            else:
+                same = np.all(x == y, axis=1).mean()
+                assert same >= 0.99, same
+        else:
+            alone.train_step(*(dev(x) for x in batch[k]))
+            trained = True
+    first, last = outs[0].cpu().numpy(), outs[-1].cpu().numpy()
+    guided = reqs[0]["guided"].astype(bool)
+    assert np.all(first[guided] == last[guided], axis=1).mean() < 0.5
+    c.close()
+    alone.close()
