@@ -68,6 +68,13 @@ struct gdf_group {
   cudaEvent_t last_launch = nullptr;  // after the group's last replay
   bool launched = false;
   uint32_t* d_err = nullptr;
+  // per-job completion: tiles done per job (device), and per job the
+  // sequence number of the last call that finished it (host-mapped)
+  uint32_t* d_job_tiles_done = nullptr;
+  uint32_t* h_job_flag = nullptr;
+  uint32_t* d_job_flag = nullptr;
+  uint32_t seq = 0;               // sequence number of the last call
+  std::vector<int64_t> job_n;     // the last call's job sizes
   cudaStream_t cap_stream = nullptr;
   std::vector<Plan> plans;
   // (levels, features, jobs, log2 tiles) -> (warpgroups, feature block)
@@ -116,6 +123,7 @@ gdf_status ensure_feat(gdf_group* g, int64_t tiles, int lf, cudaStream_t st) {
 }
 
 struct JobSet {
+  int32_t n_jobs = 0;
   int levels, features;
   bool linear, bf16;
   uint32_t bt = 0, bp = 0;
@@ -161,7 +169,7 @@ gdf_status check_jobs(const gdf_job* jobs, int32_t n, JobSet* js) {
 // queues its copy to the device; wi_override (nullable) redirects every
 // job's guiding data to one scratch buffer (tuning runs).
 gdf_status upload_table(gdf_group* g, const gdf_job* jobs, int32_t n, int wgs, float* wi_override,
-                        cudaStream_t st) {
+                        uint32_t seq, cudaStream_t st) {
   const int k = g->slot;
   g->slot ^= 1;
   GDF_GCUDA(cudaEventSynchronize(g->copied[k]));
@@ -196,7 +204,7 @@ gdf_status upload_table(gdf_group* g, const gdf_job* jobs, int32_t n, int wgs, f
     wi_off += (j.n + 3) / 4 * 4;
   }
   hdr->n_jobs = n;
-  hdr->pad = 0;
+  hdr->seq = seq;
   hdr->total_tiles = tile;
   hdr->n_super = super;
   GDF_GCUDA(cudaMemcpyAsync(g->d_hdr, hdr, sizeof(gdf::GroupHeader), cudaMemcpyHostToDevice, st));
@@ -231,6 +239,8 @@ gdf_status get_plan(gdf_group* g, const JobSet& js, int wgs, int fblock, size_t*
   prm.max_blob_theta = js.bt;
   prm.max_blob_phi = js.bp;
   prm.err = g->d_err;
+  prm.job_tiles_done = g->d_job_tiles_done;
+  prm.job_flag = g->d_job_flag;
   const size_t smem = gdf::group_fused_smem_bytes(shape, wgs, js.bt, js.bp);
   if (smem > 227u * 1024u) return gfail(GDF_ERR_UNSUPPORTED, "grouped kernel shared memory exceeds 227 KB");
   cudaGraph_t graph = nullptr;
@@ -282,6 +292,7 @@ gdf_status launch_plan(gdf_group* g, size_t plan, const JobSet& js, cudaStream_t
   Plan& p = g->plans[plan];
   p.feat_params.gridDim = dim3(static_cast<unsigned>(feature_blocks(js, p.fblock)));
   GDF_GCUDA(cudaGraphExecKernelNodeSetParams(p.exec, p.feat_node, &p.feat_params));
+  GDF_GCUDA(cudaMemsetAsync(g->d_job_tiles_done, 0, static_cast<size_t>(js.n_jobs) * 4, st));
   const unsigned grid = g->sm_cap > 0 ? std::min(p.fused_grid, static_cast<unsigned>(g->sm_cap)) : p.fused_grid;
   if (p.fused_params.gridDim.x != grid) {
     p.fused_params.gridDim = dim3(grid);
@@ -332,7 +343,8 @@ gdf_status autotune(gdf_group* g, const gdf_job* jobs, int32_t n, const JobSet& 
       off += (jobs[i].n + 3) / 4 * 4;
     }
     size_t plan = 0;
-    if ((s = upload_table(g, jobs, n, cand[k].first, g->tune_wi, st))) break;
+    // sequence number 0: a timing run marks no job done
+    if ((s = upload_table(g, jobs, n, cand[k].first, g->tune_wi, 0u, st))) break;
     if ((s = get_plan(g, js, cand[k].first, cand[k].second, &plan))) break;
     if ((s = launch_plan(g, plan, js, st))) break;  // warm-up
     GDF_GCUDA(cudaEventRecord(a, st));
@@ -370,10 +382,14 @@ gdf_status gdf_group_create(int32_t max_jobs, gdf_group** out) {
   cudaDeviceGetAttribute(&g->num_sms, cudaDevAttrMultiProcessorCount, g->device);
   if (cudaMalloc(&g->d_hdr, sizeof(gdf::GroupHeader)) != cudaSuccess ||
       cudaMalloc(&g->d_jobs, static_cast<size_t>(max_jobs) * sizeof(gdf::GroupJobDev)) != cudaSuccess ||
-      cudaMalloc(&g->d_err, 4) != cudaSuccess) {
+      cudaMalloc(&g->d_err, 4) != cudaSuccess ||
+      cudaMalloc(&g->d_job_tiles_done, static_cast<size_t>(max_jobs) * 4) != cudaSuccess ||
+      cudaHostAlloc(&g->h_job_flag, static_cast<size_t>(max_jobs) * 4, cudaHostAllocMapped) != cudaSuccess ||
+      cudaHostGetDevicePointer(&g->d_job_flag, g->h_job_flag, 0) != cudaSuccess) {
     cudaGetLastError();
     return bail(gfail(GDF_ERR_OOM_BUDGET, "grouped job table"));
   }
+  std::memset(g->h_job_flag, 0, static_cast<size_t>(max_jobs) * 4);
   for (int k = 0; k < 2; ++k) {
     if (cudaMallocHost(&g->h_stage[k], stage_bytes(max_jobs)) != cudaSuccess ||
         cudaEventCreateWithFlags(&g->copied[k], cudaEventDisableTiming) != cudaSuccess) {
@@ -396,6 +412,8 @@ gdf_status gdf_group_destroy(gdf_group* g) {
   cudaFree(g->d_hdr);
   cudaFree(g->d_jobs);
   cudaFree(g->d_err);
+  cudaFree(g->d_job_tiles_done);
+  if (g->h_job_flag) cudaFreeHost(g->h_job_flag);
   if (g->feat) cudaFreeAsync(g->feat, nullptr);
   cudaFree(g->tune_wi);
   if (g->last_launch) cudaEventDestroy(g->last_launch);
@@ -414,6 +432,10 @@ gdf_status gdf_group_infer(gdf_group* g, const gdf_job* jobs, int32_t n_jobs, vo
   JobSet js{};
   gdf_status s = check_jobs(jobs, n_jobs, &js);
   if (s) return s;
+  js.n_jobs = n_jobs;
+  if (++g->seq == 0u) g->seq = 1u;  // 0 is the timing runs' number
+  g->job_n.assign(static_cast<size_t>(n_jobs), 0);
+  for (int32_t i = 0; i < n_jobs; ++i) g->job_n[static_cast<size_t>(i)] = jobs[i].n;
   if (js.total_tiles == 0) return GDF_OK;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if ((s = ensure_feat(g, js.total_tiles, js.levels * js.features, st))) return s;
@@ -432,7 +454,7 @@ gdf_status gdf_group_infer(gdf_group* g, const gdf_job* jobs, int32_t n_jobs, vo
   g->last_wgs = cfg.first;
   g->last_fblock = cfg.second;
   size_t plan = 0;
-  if ((s = upload_table(g, jobs, n_jobs, cfg.first, nullptr, st))) return s;
+  if ((s = upload_table(g, jobs, n_jobs, cfg.first, nullptr, g->seq, st))) return s;
   if ((s = get_plan(g, js, cfg.first, cfg.second, &plan))) return s;
   return launch_plan(g, plan, js, st);
 }
@@ -457,6 +479,12 @@ gdf_status gdf_group_tuning(const gdf_group* g, int32_t* warpgroups, int32_t* fe
   if (tuned_ms)
     for (int k = 0; k < 4; ++k) tuned_ms[k] = g->last_tune_ms[k];
   return GDF_OK;
+}
+
+int32_t gdf_group_job_done(const gdf_group* g, int32_t job) {
+  if (!g || job < 0 || static_cast<size_t>(job) >= g->job_n.size()) return 0;
+  if (g->job_n[static_cast<size_t>(job)] == 0) return 1;
+  return *reinterpret_cast<const volatile uint32_t*>(g->h_job_flag + job) == g->seq ? 1 : 0;
 }
 
 gdf_status gdf_group_set_sm_cap(gdf_group* g, int32_t ctas) {

@@ -48,6 +48,7 @@ struct Request {
   Clock::time_point t_submit{}, t_done{};
   int state = 0;  // 0 pending, 1 on the device, 2 done
   int slot = -1;
+  int job = -1;  // index in its slot's grouped launch (inference)
   int64_t transient = 0;
   gdf_status status = GDF_OK;
   std::string msg;  // what failed, when status is not GDF_OK
@@ -67,6 +68,7 @@ struct Slot {
   SlotOut* out = nullptr;      // read back when the slot's work ends
   gdf_group* group = nullptr;  // grouped inference launches on this slot
   std::vector<Request*> reqs;  // requests whose work ends at `done`
+  int64_t held_transient = 0;  // of requests done before `done`: freed with it
   bool busy = false;
 };
 
@@ -189,11 +191,15 @@ void admit(gdf_server* s) {
   }
   if (!infer.empty()) {
     Slot& sl = s->slots[free_slots[used_slots++]];
+    // smallest first: a grouped launch finishes its jobs roughly in table
+    // order, and each request is returned as soon as its job is done
+    std::stable_sort(infer.begin(), infer.end(), [](const Request* a, const Request* b) { return a->r.n < b->r.n; });
     std::vector<gdf_job> jobs(infer.size());
     for (size_t k = 0; k < infer.size(); ++k) {
       const gdf_request& r = infer[k]->r;
       jobs[k] = gdf_job{r.instance, r.queries_dev, r.guided_dev, r.uniforms_dev, r.philox_seed,
                         r.philox_offset, r.wi_dev, r.n};
+      infer[k]->job = static_cast<int>(k);
     }
     // while training runs, inference takes the SMs training leaves free;
     // a grouped launch keeps its CTA count to the end, so later requests get
@@ -212,14 +218,46 @@ void admit(gdf_server* s) {
   }
 }
 
-// Completion of slots whose work has ended. Holds the lock.
+// Marks a request done at `now` (latency and statistics); its transient
+// memory is released by the caller.
+void finish(gdf_server* s, Request* q, Clock::time_point now) {
+  q->state = 2;
+  q->t_done = now;
+  s->busy[q->r.instance] -= 1;
+  if (q->r.kind == GDF_REQ_TRAIN) s->busy_train[q->r.instance] -= 1;
+  s->latency_ms.push_back(std::chrono::duration<double, std::milli>(now - q->t_submit).count());
+  s->queries_done += q->r.n;
+  s->requests_done += 1;
+  s->t_last = now;
+}
+
+// Completion of requests whose work has ended: inference requests whose
+// job in a still-running grouped launch is done (gdf_group_job_done), then
+// whole slots. Holds the lock.
 bool complete(gdf_server* s) {
   bool any = false;
   for (Slot& sl : s->slots) {
     if (!sl.busy) continue;
     const cudaError_t e = cudaEventQuery(sl.done);
-    if (e == cudaErrorNotReady) continue;
+    if (e == cudaErrorNotReady) {
+      if (sl.reqs.empty() || sl.reqs[0]->r.kind != GDF_REQ_INFER) continue;
+      const Clock::time_point now = Clock::now();
+      std::vector<Request*> rest;
+      for (Request* q : sl.reqs) {
+        if (q->status == GDF_OK && gdf_group_job_done(sl.group, q->job)) {
+          finish(s, q, now);
+          sl.held_transient += q->transient;
+          any = true;
+        } else {
+          rest.push_back(q);
+        }
+      }
+      sl.reqs.swap(rest);
+      continue;
+    }
     const Clock::time_point now = Clock::now();
+    s->transient -= sl.held_transient;
+    sl.held_transient = 0;
     for (Request* q : sl.reqs) {
       if (e != cudaSuccess && q->status == GDF_OK) {
         q->status = GDF_ERR_CUDA;
@@ -235,15 +273,8 @@ bool complete(gdf_server* s) {
         q->stats.n_records = q->r.n;
         q->stats.n_dropped = static_cast<int64_t>(sl.out->dropped);
       }
-      q->state = 2;
-      q->t_done = now;
       s->transient -= q->transient;
-      s->busy[q->r.instance] -= 1;
-      if (q->r.kind == GDF_REQ_TRAIN) s->busy_train[q->r.instance] -= 1;
-      s->latency_ms.push_back(std::chrono::duration<double, std::milli>(now - q->t_submit).count());
-      s->queries_done += q->r.n;
-      s->requests_done += 1;
-      s->t_last = now;
+      finish(s, q, now);
     }
     sl.reqs.clear();
     sl.busy = false;

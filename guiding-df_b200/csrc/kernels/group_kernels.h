@@ -32,7 +32,7 @@ struct GroupJobDev {
 
 struct GroupHeader {
   int32_t n_jobs;
-  int32_t pad;
+  uint32_t seq;              // this call's sequence number (job completion flags)
   int64_t total_tiles;
   int64_t n_super;
 };
@@ -47,6 +47,11 @@ struct GroupParams {
   GridLevels gl;                     // the grid configuration all jobs share
   uint32_t max_blob_theta, max_blob_phi;
   uint32_t* err;
+  // per-job completion: tiles done (device, zeroed before each launch) and
+  // the call's sequence number stored when a job's last tile is written
+  // (host-mapped, so the host sees a job finish before the launch ends)
+  uint32_t* job_tiles_done;
+  uint32_t* job_flag;
 };
 
 struct GroupShape {

@@ -398,6 +398,14 @@ gdf_status gdf_group_tuning(const gdf_group* g, int32_t* warpgroups, int32_t* fe
  * and skips tuning; warpgroups = 0 returns to tuning. */
 gdf_status gdf_group_set_shape(gdf_group* g, int32_t warpgroups, int32_t feature_block);
 
+/* 1 once job `job` of the group's last gdf_group_infer call has all its
+ * guiding data written (visible to the host and to later work on any
+ * stream), 0 while it has not, or for a job index outside that call. Jobs
+ * early in the table finish first, so small jobs listed first come back before the
+ * launch ends; polls host memory, never synchronises. No counterpart in
+ * the reference. */
+int32_t gdf_group_job_done(const gdf_group* g, int32_t job);
+
 /* Caps the CTAs of the group's persistent fused launches at `ctas` (0: one
  * per SM, the default), so that later calls leave the other SMs to work on
  * other streams; results do not depend on the cap. */

@@ -97,3 +97,26 @@ def test_sm_cap_keeps_results_across_plans():
     g.close()
     for c in ctxs:
         c.close()
+
+
+def test_job_done_flags():
+    """gdf_group_job_done: after a call has finished every job reports done;
+    a new call's jobs start over (its flags carry the new call's number), an
+    empty job is done at once, and indexes outside the last call are not."""
+    ctxs = _contexts()
+    g = pygdf.Group(max_jobs=16)
+    g.set_shape(4, 256)
+    jobs = _jobs(ctxs, [1000, 30000, 0, 5000], seed=120)
+    g.infer(jobs)
+    g.sync()
+    assert all(g.job_done(k) for k in range(4))
+    assert not g.job_done(4) and not g.job_done(-1)
+    again = _jobs(ctxs[:2], [70000, 2000], seed=130)
+    g.infer(again)
+    g.sync()
+    assert g.job_done(0) and g.job_done(1) and not g.job_done(2)
+    _check(jobs)
+    _check(again)
+    g.close()
+    for c in ctxs:
+        c.close()
