@@ -68,7 +68,7 @@ struct gdf_group {
   cudaEvent_t last_launch = nullptr;  // after the group's last replay
   bool launched = false;
   uint32_t* d_err = nullptr;
-  // per-job completion: tiles done per job (device), and per job the
+  // per-job completion: warps done per job (device), and per job the
   // sequence number of the last call that finished it (host-mapped)
   uint32_t* d_job_tiles_done = nullptr;
   uint32_t* h_job_flag = nullptr;

@@ -47,8 +47,9 @@ struct GroupParams {
   GridLevels gl;                     // the grid configuration all jobs share
   uint32_t max_blob_theta, max_blob_phi;
   uint32_t* err;
-  // per-job completion: tiles done (device, zeroed before each launch) and
-  // the call's sequence number stored when a job's last tile is written
+  // per-job completion: warps of 32 rows done (device, zeroed before each
+  // launch) and the call's sequence number stored when a job's last one is
+  // written
   // (host-mapped, so the host sees a job finish before the launch ends)
   uint32_t* job_tiles_done;
   uint32_t* job_flag;

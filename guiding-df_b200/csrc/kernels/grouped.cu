@@ -275,13 +275,13 @@ __global__ void __launch_bounds__(128 * WGS, 1) group_fused_kernel(const __grid_
     const tile::RowResult rp = epilogue_bins<LINEAR, BF16>(J.bins_phi, c.tmem + c.lane_base, guided, wi.y, u[2], u[3]);
     if (valid)
       *reinterpret_cast<float4*>(J.wi + row * 4) = make_float4(rt.u, rp.u, wi.z * rt.pdf, wi.w * rp.pdf);
-    // the job's last tile: its rows are visible device-wide, then to the
-    // host through the flag (unless a bounded wait has failed)
-    __threadfence();
-    named_bar_sync(c.bar_id, 128);
-    if (c.leader) {
-      const uint32_t tiles = static_cast<uint32_t>((J.n + 127) / 128);
-      if (atomicAdd(g.job_tiles_done + j, 1u) + 1u == tiles &&
+    // each warp counts its 32 rows; the job's last warp makes them visible
+    // to the host through the flag (unless a bounded wait has failed)
+    __syncwarp();
+    if ((tid & 31u) == 0u) {
+      __threadfence();
+      const uint32_t warps = 4u * static_cast<uint32_t>((J.n + 127) / 128);
+      if (atomicAdd(g.job_tiles_done + j, 1u) + 1u == warps &&
           *reinterpret_cast<volatile uint32_t*>(g.err) == 0u) {
         __threadfence_system();
         *reinterpret_cast<volatile uint32_t*>(g.job_flag + j) = g.hdr->seq;
