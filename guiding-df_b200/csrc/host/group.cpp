@@ -74,6 +74,7 @@ struct gdf_group {
   uint32_t* h_job_flag = nullptr;
   uint32_t* d_job_flag = nullptr;
   uint32_t seq = 0;               // sequence number of the last call
+  bool track = false;             // job completion reported (gdf_group_track_jobs)
   std::vector<int64_t> job_n;     // the last call's job sizes
   cudaStream_t cap_stream = nullptr;
   std::vector<Plan> plans;
@@ -205,6 +206,8 @@ gdf_status upload_table(gdf_group* g, const gdf_job* jobs, int32_t n, int wgs, f
   }
   hdr->n_jobs = n;
   hdr->seq = seq;
+  hdr->track = g->track ? 1u : 0u;
+  hdr->pad = 0u;
   hdr->total_tiles = tile;
   hdr->n_super = super;
   GDF_GCUDA(cudaMemcpyAsync(g->d_hdr, hdr, sizeof(gdf::GroupHeader), cudaMemcpyHostToDevice, st));
@@ -481,8 +484,14 @@ gdf_status gdf_group_tuning(const gdf_group* g, int32_t* warpgroups, int32_t* fe
   return GDF_OK;
 }
 
+gdf_status gdf_group_track_jobs(gdf_group* g, int32_t on) {
+  if (!g) return gfail(GDF_ERR_INVALID_ARG, "null group");
+  g->track = on != 0;
+  return GDF_OK;
+}
+
 int32_t gdf_group_job_done(const gdf_group* g, int32_t job) {
-  if (!g || job < 0 || static_cast<size_t>(job) >= g->job_n.size()) return 0;
+  if (!g || !g->track || job < 0 || static_cast<size_t>(job) >= g->job_n.size()) return 0;
   if (g->job_n[static_cast<size_t>(job)] == 0) return 1;
   return *reinterpret_cast<const volatile uint32_t*>(g->h_job_flag + job) == g->seq ? 1 : 0;
 }

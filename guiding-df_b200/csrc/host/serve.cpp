@@ -333,7 +333,8 @@ gdf_status gdf_server_create(const gdf_server_config* cfg, gdf_server** out) {
       gdf_server_destroy(s);
       return sfail(GDF_ERR_CUDA, "server streams");
     }
-    if ((st = gdf_group_create(cfg->max_batch, &sl.group)) || (st = gdf_group_set_shape(sl.group, 4, 256))) {
+    if ((st = gdf_group_create(cfg->max_batch, &sl.group)) || (st = gdf_group_set_shape(sl.group, 4, 256)) ||
+        (st = gdf_group_track_jobs(sl.group, 1))) {
       gdf_server_destroy(s);
       return st;
     }

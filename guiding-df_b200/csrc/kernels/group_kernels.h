@@ -35,6 +35,8 @@ struct GroupHeader {
   uint32_t seq;              // this call's sequence number (job completion flags)
   int64_t total_tiles;
   int64_t n_super;
+  uint32_t track;            // report each job's completion (job_flag)
+  uint32_t pad;
 };
 
 // Kernel parameters: fixed for a captured graph; the job set is read from

@@ -277,6 +277,7 @@ __global__ void __launch_bounds__(128 * WGS, 1) group_fused_kernel(const __grid_
       *reinterpret_cast<float4*>(J.wi + row * 4) = make_float4(rt.u, rp.u, wi.z * rt.pdf, wi.w * rp.pdf);
     // each warp counts its 32 rows; the job's last warp makes them visible
     // to the host through the flag (unless a bounded wait has failed)
+    if (g.hdr->track == 0u) continue;
     __syncwarp();
     if ((tid & 31u) == 0u) {
       __threadfence();

@@ -190,6 +190,7 @@ def lib() -> C.CDLL:
             "gdf_group_set_shape": [P, C.c_int32, C.c_int32],
             "gdf_group_set_sm_cap": [P, C.c_int32],
             "gdf_group_job_done": [P, C.c_int32],
+            "gdf_group_track_jobs": [P, C.c_int32],
             "gdf_ctx_bytes": [P, C.POINTER(C.c_int64)],
             "gdf_server_create": [C.POINTER(ServerConfig), C.POINTER(C.c_void_p)],
             "gdf_server_destroy": [P],
@@ -493,6 +494,9 @@ class Group:
 
     def set_shape(self, warpgroups: int, feature_block: int):
         check(lib().gdf_group_set_shape(self.h, warpgroups, feature_block))
+
+    def track_jobs(self, on: bool = True):
+        check(lib().gdf_group_track_jobs(self.h, int(on)))
 
     def job_done(self, job: int) -> bool:
         return bool(lib().gdf_group_job_done(self.h, job))

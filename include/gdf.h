@@ -398,9 +398,16 @@ gdf_status gdf_group_tuning(const gdf_group* g, int32_t* warpgroups, int32_t* fe
  * and skips tuning; warpgroups = 0 returns to tuning. */
 gdf_status gdf_group_set_shape(gdf_group* g, int32_t warpgroups, int32_t feature_block);
 
-/* 1 once job `job` of the group's last gdf_group_infer call has all its
- * guiding data written (visible to the host and to later work on any
- * stream), 0 while it has not, or for a job index outside that call. Jobs
+/* Turns per-job completion reports on (1) or off (0, the default) for the
+ * group's later calls: each warp of the fused kernel then counts its rows
+ * with an atomic after a memory fence (about 4 % of a launch's time). No
+ * counterpart in the reference. */
+gdf_status gdf_group_track_jobs(gdf_group* g, int32_t on);
+
+/* With tracking on: 1 once job `job` of the group's last gdf_group_infer
+ * call has all its guiding data written (visible to the host and to later
+ * work on any stream), 0 while it has not, or for a job index outside that
+ * call; always 0 with tracking off. Jobs
  * early in the table finish first, so small jobs listed first come back before the
  * launch ends; polls host memory, never synchronises. No counterpart in
  * the reference. */

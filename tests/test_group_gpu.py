@@ -100,12 +100,17 @@ def test_sm_cap_keeps_results_across_plans():
 
 
 def test_job_done_flags():
-    """gdf_group_job_done: after a call has finished every job reports done;
-    a new call's jobs start over (its flags carry the new call's number), an
-    empty job is done at once, and indexes outside the last call are not."""
+    """gdf_group_job_done: off by default; with tracking on, after a call
+    has finished every job reports done; a new call's jobs start over (its
+    flags carry the new call's number), an empty job is done at once, and
+    indexes outside the last call are not."""
     ctxs = _contexts()
     g = pygdf.Group(max_jobs=16)
     g.set_shape(4, 256)
+    g.infer(_jobs(ctxs[:1], [1000], seed=110))
+    g.sync()
+    assert not g.job_done(0)
+    g.track_jobs(True)
     jobs = _jobs(ctxs, [1000, 30000, 0, 5000], seed=120)
     g.infer(jobs)
     g.sync()
