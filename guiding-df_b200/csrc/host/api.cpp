@@ -887,44 +887,49 @@ gdf_status gdf_infer_host(gdf_ctx* ctx, const float* queries_h, const uint8_t* g
   // guided flags (1 B per query) go in one copy ahead of the chunks.
   cudaStream_t s_in = c.pipe[0], s_run = c.pipe[1], s_out = c.pipe[2];
   constexpr int64_t kChunk = 4096 * 128, kMinChunk = 1024 * 128;
-  if (guided_h) GDF_CUDA(cudaMemcpyAsync(c.host_g, guided_h, static_cast<size_t>(n), cudaMemcpyHostToDevice, s_in));
-  int64_t m = 0;
-  for (int64_t b = 0; b < n; b += m) {
-    const int64_t rest = n - b;
-    m = std::min(kChunk, (rest / 2 + 127) / 128 * 128);
-    if (m < kMinChunk) m = std::min(rest, kMinChunk);
-    GDF_CUDA(cudaMemcpyAsync(c.host_q + b * 9, queries_h + b * 9, static_cast<size_t>(m) * 36,
-                             cudaMemcpyHostToDevice, s_in));
-    GDF_CUDA(cudaMemcpyAsync(c.host_wi + b * 4, wi_in_h + b * 4, static_cast<size_t>(m) * 16,
-                             cudaMemcpyHostToDevice, s_in));
-    if (uniforms_h)
-      GDF_CUDA(cudaMemcpyAsync(c.host_u + b * 4, uniforms_h + b * 4, static_cast<size_t>(m) * 16,
+  auto issue = [&]() -> gdf_status {
+    if (guided_h) GDF_CUDA(cudaMemcpyAsync(c.host_g, guided_h, static_cast<size_t>(n), cudaMemcpyHostToDevice, s_in));
+    int64_t m = 0;
+    for (int64_t b = 0; b < n; b += m) {
+      const int64_t rest = n - b;
+      m = std::min(kChunk, (rest / 2 + 127) / 128 * 128);
+      if (m < kMinChunk) m = std::min(rest, kMinChunk);
+      GDF_CUDA(cudaMemcpyAsync(c.host_q + b * 9, queries_h + b * 9, static_cast<size_t>(m) * 36,
                                cudaMemcpyHostToDevice, s_in));
-    // one event object per hand-over: each wait takes the record before it
-    GDF_CUDA(cudaEventRecord(c.pipe_ev[4], s_in));
-    GDF_CUDA(cudaStreamWaitEvent(s_run, c.pipe_ev[4], 0));
-    gdf::DfKernelParams p = df_params(c);
-    p.queries = c.host_q + b * 9;
-    p.guided = guided_h ? c.host_g + b : nullptr;
-    p.uniforms = uniforms_h ? c.host_u + b * 4 : nullptr;
-    p.wi = c.host_wi + b * 4;
-    p.n = m;
-    p.philox_seed = philox_seed;
-    p.philox_offset = philox_offset;
-    p.philox_row_base = b;
-    if ((s = grid_features(c, p.queries, nullptr, gdf_aabb{}, m, p, s_run, b / 128))) return s;
-    cudaError_t e = gdf::launch_df_fused(df_shape(c), gdf::kModeInfer, p, c.num_sms, s_run);
-    if (e != cudaSuccess) return cuda_fail(e, "df_fused (infer_host)");
-    GDF_CUDA(cudaEventRecord(c.pipe_ev[5], s_run));
-    GDF_CUDA(cudaStreamWaitEvent(s_out, c.pipe_ev[5], 0));
-    GDF_CUDA(cudaMemcpyAsync(wi_out_h + b * 4, c.host_wi + b * 4, static_cast<size_t>(m) * 16,
-                             cudaMemcpyDeviceToHost, s_out));
-  }
+      GDF_CUDA(cudaMemcpyAsync(c.host_wi + b * 4, wi_in_h + b * 4, static_cast<size_t>(m) * 16,
+                               cudaMemcpyHostToDevice, s_in));
+      if (uniforms_h)
+        GDF_CUDA(cudaMemcpyAsync(c.host_u + b * 4, uniforms_h + b * 4, static_cast<size_t>(m) * 16,
+                                 cudaMemcpyHostToDevice, s_in));
+      // one event object per hand-over: each wait takes the record before it
+      GDF_CUDA(cudaEventRecord(c.pipe_ev[4], s_in));
+      GDF_CUDA(cudaStreamWaitEvent(s_run, c.pipe_ev[4], 0));
+      gdf::DfKernelParams p = df_params(c);
+      p.queries = c.host_q + b * 9;
+      p.guided = guided_h ? c.host_g + b : nullptr;
+      p.uniforms = uniforms_h ? c.host_u + b * 4 : nullptr;
+      p.wi = c.host_wi + b * 4;
+      p.n = m;
+      p.philox_seed = philox_seed;
+      p.philox_offset = philox_offset;
+      p.philox_row_base = b;
+      if ((s = grid_features(c, p.queries, nullptr, gdf_aabb{}, m, p, s_run, b / 128))) return s;
+      cudaError_t e = gdf::launch_df_fused(df_shape(c), gdf::kModeInfer, p, c.num_sms, s_run);
+      if (e != cudaSuccess) return cuda_fail(e, "df_fused (infer_host)");
+      GDF_CUDA(cudaEventRecord(c.pipe_ev[5], s_run));
+      GDF_CUDA(cudaStreamWaitEvent(s_out, c.pipe_ev[5], 0));
+      GDF_CUDA(cudaMemcpyAsync(wi_out_h + b * 4, c.host_wi + b * 4, static_cast<size_t>(m) * 16,
+                               cudaMemcpyDeviceToHost, s_out));
+    }
+    return GDF_OK;
+  };
+  const gdf_status issued = issue();
+  // the three streams join the caller's, also after a failed launch
   for (int i = 0; i < 3; ++i) {
     GDF_CUDA(cudaEventRecord(c.pipe_ev[i], c.pipe[i]));
     GDF_CUDA(cudaStreamWaitEvent(user, c.pipe_ev[i], 0));
   }
-  return GDF_OK;
+  return issued;
 }
 
 }  // extern "C"
