@@ -26,3 +26,25 @@ def test_round_bf16_matches_torch():
     L = O.lib()
     got = np.array([L.go_round_bf16(float(v)) for v in x], dtype=np.float32)
     assert np.array_equal(got, ref)
+
+
+def test_training_oracle_storage_switch():
+    """The training oracle's storage switch (the bf16 training form's storage
+    points): it changes the gradients by the format's error -- more than
+    fp32 noise, much less than the gradients -- is deterministic, and leaves
+    the default fp16 model untouched afterwards."""
+    import pygdf
+    from gdf_testutil import gen_weights
+    from pygdf import workload as W
+    cfg = pygdf.default_config(pygdf.PRESET_SMALL)
+    d = O.df_cfg_from(cfg)
+    pt, pp = gen_weights(cfg, 0, 3), gen_weights(cfg, 1, 4)
+    a, b, t = W.training_batch(1024, 10, cfg.n_bins_theta, cfg.pdf_interp == 0)
+    g16 = O.df_train_grads(d, pt, pp, a, b, t, cfg.loss_scale)
+    gbf = O.df_train_grads(d, pt, pp, a, b, t, cfg.loss_scale, storage="bf16")
+    gbf2 = O.df_train_grads(d, pt, pp, a, b, t, cfg.loss_scale, storage="bf16")
+    g16b = O.df_train_grads(d, pt, pp, a, b, t, cfg.loss_scale)
+    for key in ("grad_theta", "grad_phi"):
+        assert np.array_equal(gbf[key], gbf2[key]) and np.array_equal(g16[key], g16b[key])
+        rel = np.linalg.norm(gbf[key] - g16[key]) / np.linalg.norm(g16[key])
+        assert 1e-4 < rel < 0.3, (key, rel)
